@@ -1,0 +1,97 @@
+/*
+ * photonoxide_sim.h: the host side of the B200 FDTD engine, photonoxide's `Simulation` API
+ * (src/fdtd.rs:469-1590) over the device engine of photonoxide_fdtd.h.
+ *
+ * It builds what the reference's Simulation builds on the CPU (the cell-averaged permittivity,
+ * the time step, the walls, the CPML's tables, conductivity, dispersive media, sources, probes and
+ * monitors), then steps on the GPU: the fields go to the device at the first run and stay there,
+ * coming back when read. It is the C ABI the Python package binds; a Rust caller keeps its own
+ * Simulation and binds photonoxide_fdtd.h instead.
+ *
+ * Conventions as photonoxide_fdtd.h. Errors: 0 or a negative FDTD_E_* status, the message in
+ * pxs_last_error(sim); construction errors in the caller's buffer.
+ */
+#ifndef PHOTONOXIDE_SIM_H
+#define PHOTONOXIDE_SIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pxs_sim pxs_sim;
+
+/* A box geometry (the value of the reference's eps(x, y, z) closures): boxes of 7 doubles
+ * {xlo, xhi, ylo, yhi, zlo, zhi, value}, a point inside when lo < p < hi on each axis, later
+ * boxes over earlier ones, `background` elsewhere. */
+typedef struct {
+  double background;
+  int32_t nboxes;
+  const double *boxes;
+} pxs_geometry;
+
+/* FDFD's cell average (src/fdfd/three.rs:563-588) of a geometry at every value of E (3 x
+ * cells); only values whose cell crosses a box's face take the 8^3-sample average. */
+int pxs_average(const int64_t n[3], const double d[3], const double o[3], const pxs_geometry *g,
+                double *out);
+
+/* Simulation::new / with_permittivity (src/fdtd.rs:570-796): grid n, d, origin o; kind[a] 0 a
+ * CPML of low/high cells (0 = wall), 1 periodic; cpml = {reflection, sigma (NaN: from
+ * reflection), order, kappa, alpha}; the per-value permittivity `eps` (3 x cells) or, if NULL,
+ * the geometry averaged. precision 32 or 64 on the device. NULL on error, message in err. */
+pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], const int32_t kind[3],
+                    const int64_t low[3], const int64_t high[3], const double cpml[5],
+                    double courant, const double *eps, const pxs_geometry *geometry,
+                    int32_t precision, size_t hbm_budget, char *err, int32_t errlen);
+void pxs_destroy(pxs_sim *s);
+const char *pxs_last_error(const pxs_sim *s);
+
+/* Simulation::with_conductivity (src/fdtd.rs:945-992): sampled at each value of E, from a
+ * per-value array (3 x cells) or, if NULL, the geometry. */
+int pxs_conductivity(pxs_sim *s, const double *sigma, const pxs_geometry *geometry);
+/* Simulation::conductor (src/fdtd.rs:995-1008) */
+int pxs_conductor(pxs_sim *s, int32_t comp, int64_t i, int64_t j, int64_t k);
+/* Simulation::with_medium (src/fdtd/media.rs:741-825): poles of 4 doubles {kind (0 Lorentz,
+ * 1 Drude), strength|plasma, resonance|damping, damping|0}; where: a 3 x cells mask, or if
+ * NULL the geometry's nonzero places. */
+int pxs_medium(pxs_sim *s, double eps_inf, int32_t npoles, const double *poles,
+               const uint8_t *inside, const pxs_geometry *geometry);
+
+/* Waveforms as 6 doubles {kind, p1..p5} (photonoxide_fdtd.h's fdtd_waveform). */
+int pxs_add_source(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j, int64_t k,
+                   const double wave[6]);
+int pxs_add_current(pxs_sim *s, int32_t field, int64_t count, const int32_t *comps,
+                    const int64_t *at, const double *amps, const double wave[6]);
+int pxs_add_dipole(pxs_sim *s, int32_t field, int32_t comp, const double pos[3], double are,
+                   double aim, const double wave[6]);
+int pxs_add_probe(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j, int64_t k);
+int pxs_add_dft(pxs_sim *s, const int64_t low[3], const int64_t high[3], int32_t nf,
+                const double *freqs);
+/* window = {blo, bhi, clo, chi} along axis.others(); -1 for the whole axis */
+int pxs_add_flux(pxs_sim *s, int32_t axis, int64_t plane, const int64_t window[4], int32_t nf,
+                 const double *freqs);
+int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const double *freqs);
+
+/* Simulation::run (src/fdtd.rs:1142-1158) on the device. */
+int pxs_run(pxs_sim *s, int64_t steps);
+double pxs_dt(const pxs_sim *s);
+int64_t pxs_steps(const pxs_sim *s);
+int pxs_get_field(pxs_sim *s, int32_t field, int32_t comp, double *out);
+int pxs_set_field(pxs_sim *s, int32_t field, int32_t comp, const double *in);
+/* probe n's values, one per step since it was added; returns the count (out may be NULL) */
+int64_t pxs_probe(pxs_sim *s, int32_t n, double *out);
+/* every transform's sums (Monitors::layout order), complex interleaved; returns the count */
+int64_t pxs_transforms(pxs_sim *s, double *out);
+/* Simulation::flux (src/fdtd/monitors.rs:539-552): returns the frequencies' count */
+int pxs_flux(pxs_sim *s, int32_t n, double *out);
+/* the setup tables, as orc_tables: 0 ca, 1 cb, 2 kappa/h nodes, 3 halves, 4 slabs */
+int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out);
+/* The device engine under it (created at the first run), or NULL. */
+struct fdtd_ctx *pxs_engine(pxs_sim *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

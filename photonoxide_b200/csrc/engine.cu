@@ -1,0 +1,1396 @@
+// The B200 FDTD engine: photonoxide's time step (src/fdtd.rs:1319-1419) as CUDA kernels for
+// sm_100a, behind the C ABI of include/photonoxide_fdtd.h.
+//
+// One step is ONE pass over the grid (kernel `step`): each CTA owns a tile of TX x TY values in
+// every plane of a run of planes along z and marches up through them. At plane k it stages the
+// old E of plane k+1 (with the row and column of neighbours the curl needs) in shared memory,
+// computes the new H~ of plane k over its tile and the low row and column around it (E's back
+// differences need them; the neighbours' CTAs compute the same values), adds the magnetic
+// currents, then updates E of plane k on its tile with the CPML's psi recursions, the electric
+// currents and the dispersive media's ADE currents fused in. Each value is computed with the
+// same operations in the same order as the reference's CPU kernel (src/fdtd/kernel.rs,
+// src/fdtd/kernel/reference.rs): in f64 the engine gives the reference's bits, and in f32 the
+// reference's f32 arithmetic (`Yee<f32>`) on problems without sources. Fields, psi and the
+// step's old/new copies are ping-ponged (the step reads one copy and writes the other), so
+// CTAs never wait on one another.
+//
+// The probes and transforms are read after each step by a gather kernel into a ring of K steps
+// of values; every K steps a contraction kernel adds sum_n F(t_n) e^{i w t_n} dt into f64 sums,
+// in time order per value (src/fdtd/monitors.rs:185-206), phases taken in f64 on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "photonoxide_fdtd.h"
+#include "portable.h"
+
+namespace pxf {
+
+constexpr int TX = 32;  // a tile's values along x
+constexpr int TY = 8;   // and along y
+constexpr int NT = 256; // threads per CTA
+constexpr int RX = TX + 2, RY = TY + 2;  // E's staged region: x0-1 .. x0+TX, y0-1 .. y0+TY
+constexpr int HX = TX + 1, HY = TY + 1;  // H's computed region: x0-1 .. x0+TX-1, y0-1 ..
+constexpr double TAU = 6.283185307179586476925286766559;
+
+struct SlabEntry {
+  int from, count;  // count 0: no slab
+  long long psi;    // where its psi starts
+  int coef;         // where its b starts (a follows after count)
+};
+
+// A value the sources add to, with its entries (emitter, amplitude) in CPU order.
+struct Group {
+  int local;  // index in the CTA's staged region: H's (HX x HY) or E's tile (TX x TY), x fastest
+  int comp;
+  int first, count;
+};
+struct Entry {
+  double are, aim;
+  int emitter;
+  int pad;
+};
+
+struct Pole3 {
+  double alpha, xi, gamma;
+};
+
+template <typename T>
+struct MediaArgs {
+  const int *member;  // 3N: index into the compact state, or -1
+  const int *group;   // per member: its group
+  const T *scale;     // per member: p_m
+  T *before;          // per member: E^{n-1}
+  T *current;         // per member x maxpoles: J_p^n
+  T *previous;        // per member x maxpoles: J_p^{n-1}
+  int maxpoles;
+  int ngroups;
+  const T *gchi;      // per group: chi
+  const int *gpoles;  // per group: its pole count
+  const T *gpole;     // per group x maxpoles x 3: alpha, xi, gamma
+  T two_dt;
+};
+
+template <typename T>
+struct StepArgs {
+  int n[3];
+  long long N;
+  int periodic[3];
+  int low[3], high[3];
+  T dt;
+  T step[3];
+  const T *fe;  // kappa/h at the nodes: x | y | z
+  const T *fh;  // at the halves
+  const T *e_in;
+  const T *h_in;
+  T *e_out;
+  T *h_out;
+  const T *ca;  // NULL: lossless
+  const T *cb;
+  SlabEntry slab[2][3][3][2];
+  const T *coefs;
+  const T *psi_h_in;
+  T *psi_h_out;
+  T *psi_e;
+  // sources: per (tile, k) the groups on H (over the H region) and on E (over the tile)
+  const int *hbucket;
+  const int *ebucket;
+  const Group *hgroups;
+  const Group *egroups;
+  const Entry *entries;
+  const double *waves_h;  // this step's w at H's time: 2 per emitter
+  const double *waves_e;  // at E's time
+  int tiles_x, tiles_y, zchunk;
+  MediaArgs<T> media;
+};
+
+__host__ __device__ inline int wrap_index(int g, int n, int periodic) {
+  if (g >= 0 && g < n) return g;
+  if (periodic) {
+    if (g == n) return 0;
+    if (g == -1) return n - 1;
+  }
+  return -1;
+}
+
+// Whether value m along axis w is in a CPML slab there, and which.
+template <typename T>
+__device__ inline const SlabEntry *slab_at(const StepArgs<T> &A, int field, int c, int w, int m) {
+  if (A.periodic[w]) return nullptr;
+  int side;
+  if (m < A.low[w]) side = 0;
+  else if (m >= A.n[w] - A.high[w]) side = 1;
+  else return nullptr;
+  const SlabEntry *s = &A.slab[field][c][w][side];
+  return s->count > 0 ? s : nullptr;
+}
+
+// One slab's share of a value's update (src/fdtd/kernel/reference.rs:102-180): psi <- b psi + a
+// (dF / h), then H -= dt (sign psi) or E += cb (sign psi). `diff` is the other field's raw
+// difference along w (forward for H, back for E), as the curl took it.
+template <typename T, int FIELD>
+__device__ inline T slab_update(const StepArgs<T> &A, const SlabEntry *s, int c, int w, int i,
+                                int j, int k, T diff, T v, T cbv, bool own) {
+  int m = w == 0 ? i : (w == 1 ? j : k);
+  int q = m - s->from;
+  int li = i, lj = j, lk = k;
+  int dx = A.n[0], dy = A.n[1];
+  if (w == 0) { li = q; dx = s->count; }
+  else if (w == 1) { lj = q; dy = s->count; }
+  else lk = q;
+  long long p = s->psi + ((long long)lk * dy + lj) * dx + li;
+  T d = diff / A.step[w];
+  T b = A.coefs[s->coef + q], a = A.coefs[s->coef + s->count + q];
+  T old = FIELD == 1 ? A.psi_h_in[p] : A.psi_e[p];
+  T psi = b * old + a * d;
+  if (own) {
+    if (FIELD == 1) A.psi_h_out[p] = psi;
+    else A.psi_e[p] = psi;
+  }
+  T sign = (w == (c + 1) % 3) ? T(1) : T(-1);
+  T u = sign * psi;
+  if (FIELD == 1) return v - A.dt * u;
+  return v + cbv * u;
+}
+
+// The fused step over one tile column and a run of planes.
+template <typename T, bool LOSSY, bool MEDIA>
+__global__ void __launch_bounds__(NT) step_kernel(StepArgs<T> A) {
+  __shared__ T sE[2][3][RY][RX];
+  __shared__ T sH[2][3][HY][HX];
+  __shared__ T sEn[3][TY][TX];
+  const int tid = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int x0 = (tile % A.tiles_x) * TX, y0 = (tile / A.tiles_x) * TY;
+  const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
+  const int kbeg = blockIdx.y * A.zchunk;
+  const int kend = min(kbeg + A.zchunk, nz);
+  if (kbeg >= nz) return;
+  const long long N = A.N;
+
+  auto load_e = [&](int buf, int kk) {  // E's plane kk (already wrapped; -1 = beyond a wall)
+    for (int q = tid; q < 3 * RY * RX; q += NT) {
+      int c = q / (RY * RX), rem = q % (RY * RX);
+      int ly = rem / RX, lx = rem % RX;
+      int gi = wrap_index(x0 - 1 + lx, nx, A.periodic[0]);
+      int gj = wrap_index(y0 - 1 + ly, ny, A.periodic[1]);
+      T v = T(0);
+      if (gi >= 0 && gj >= 0 && kk >= 0) v = A.e_in[c * N + ((long long)kk * ny + gj) * nx + gi];
+      sE[buf][c][ly][lx] = v;
+    }
+  };
+
+  // H's new plane kk over the region, from E's planes kk (buffer ec) and kk+1 (buffer en):
+  // H <- H - dt curl E with forward differences (reference.rs:14-50), then the slabs in axis
+  // order (kernel.rs:525-579 takes the slabs along x, then y, then z).
+  auto compute_h = [&](int hb, int ec, int en, int kk, bool write) {
+    int kn = wrap_index(kk + 1, nz, A.periodic[2]);
+    for (int q = tid; q < HY * HX; q += NT) {
+      int ly = q / HX, lx = q % HX;  // region cell; E region index (ly, lx) is the same place
+      int gi = wrap_index(x0 - 1 + lx, nx, A.periodic[0]);
+      int gj = wrap_index(y0 - 1 + ly, ny, A.periodic[1]);
+      if (gi < 0 || gj < 0 || x0 - 1 + lx >= nx || y0 - 1 + ly >= ny) {
+        sH[hb][0][ly][lx] = sH[hb][1][ly][lx] = sH[hb][2][ly][lx] = T(0);
+        continue;
+      }
+      bool own = write && lx >= 1 && ly >= 1;
+      // E at this value, its +x and +y neighbours (plane kk), and +z (plane kk+1); beyond a wall
+      // the neighbour is zero (the staged region holds zeros there)
+      T ex = sE[ec][0][ly][lx], ey = sE[ec][1][ly][lx], ez = sE[ec][2][ly][lx];
+      T ey_xp = sE[ec][1][ly][lx + 1], ez_xp = sE[ec][2][ly][lx + 1];
+      T ex_yp = sE[ec][0][ly + 1][lx], ez_yp = sE[ec][2][ly + 1][lx];
+      T ex_zp = kn >= 0 ? sE[en][0][ly][lx] : T(0), ey_zp = kn >= 0 ? sE[en][1][ly][lx] : T(0);
+      T fx = A.fh[gi], fy = A.fh[nx + gj], fz = A.fh[nx + ny + kk];
+      long long r = ((long long)kk * ny + gj) * nx + gi;
+      // x: dy(Ez) fy - dz(Ey) fz ; y: dz(Ex) fz - dx(Ez) fx ; z: dx(Ey) fx - dy(Ex) fy
+      T dyEz = ez_yp - ez, dzEy = ey_zp - ey, dzEx = ex_zp - ex, dxEz = ez_xp - ez;
+      T dxEy = ey_xp - ey, dyEx = ex_yp - ex;
+      T hx = A.h_in[r] - A.dt * (dyEz * fy - dzEy * fz);
+      T hy = A.h_in[N + r] - A.dt * (dzEx * fz - dxEz * fx);
+      T hz = A.h_in[2 * N + r] - A.dt * (dxEy * fx - dyEx * fy);
+      const SlabEntry *s;
+      // H_x: slabs along y (d/dy of Ez, sign +), then z (d/dz of Ey, sign -)
+      if ((s = slab_at(A, 1, 0, 1, gj))) hx = slab_update<T, 1>(A, s, 0, 1, gi, gj, kk, dyEz, hx, T(0), own);
+      if ((s = slab_at(A, 1, 0, 2, kk))) hx = slab_update<T, 1>(A, s, 0, 2, gi, gj, kk, dzEy, hx, T(0), own);
+      // H_y: slabs along x (d/dx of Ez, sign -), then z (d/dz of Ex, sign +)
+      if ((s = slab_at(A, 1, 1, 0, gi))) hy = slab_update<T, 1>(A, s, 1, 0, gi, gj, kk, dxEz, hy, T(0), own);
+      if ((s = slab_at(A, 1, 1, 2, kk))) hy = slab_update<T, 1>(A, s, 1, 2, gi, gj, kk, dzEx, hy, T(0), own);
+      // H_z: slabs along x (d/dx of Ey, sign +), then y (d/dy of Ex, sign -)
+      if ((s = slab_at(A, 1, 2, 0, gi))) hz = slab_update<T, 1>(A, s, 2, 0, gi, gj, kk, dxEy, hz, T(0), own);
+      if ((s = slab_at(A, 1, 2, 1, gj))) hz = slab_update<T, 1>(A, s, 2, 1, gi, gj, kk, dyEx, hz, T(0), own);
+      sH[hb][0][ly][lx] = hx;
+      sH[hb][1][ly][lx] = hy;
+      sH[hb][2][ly][lx] = hz;
+    }
+  };
+
+  // The magnetic currents of plane kk on the region (src/fdtd.rs:1348-1359): each value's
+  // entries in CPU order by one thread, H -= dt Re(a w(t)).
+  auto inject_h = [&](int hb, int kk) {
+    int bucket = tile * nz + kk;
+    int g0 = A.hbucket[bucket], g1 = A.hbucket[bucket + 1];
+    for (int g = g0 + tid; g < g1; g += NT) {
+      Group gr = A.hgroups[g];
+      T *v = &sH[hb][gr.comp][0][0] + gr.local;
+      for (int q = gr.first; q < gr.first + gr.count; q++) {
+        Entry en = A.entries[q];
+        double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
+        if (sizeof(T) == 8) *v = *v - (T)((double)A.dt * amount);
+        else *v = *v - A.dt * (T)amount;
+      }
+    }
+  };
+
+  int ec = 0, en = 1, hp = 0, hc = 1;
+  // Prologue: H's new plane kbeg-1 (wrapped on a periodic z), which E's plane kbeg needs.
+  int km = wrap_index(kbeg - 1, nz, A.periodic[2]);
+  if (km >= 0) {
+    load_e(ec, km);
+    load_e(en, kbeg);
+    __syncthreads();
+    compute_h(hp, ec, en, km, false);
+    __syncthreads();
+    inject_h(hp, km);
+    ec = 1; en = 0;
+  } else {
+    for (int q = tid; q < 3 * HY * HX; q += NT) (&sH[hp][0][0][0])[q] = T(0);
+    load_e(ec, kbeg);
+    ec = 0; en = 1;
+  }
+  __syncthreads();
+
+  for (int k = kbeg; k < kend; k++) {
+    load_e(en, wrap_index(k + 1, nz, A.periodic[2]));
+    __syncthreads();
+    compute_h(hc, ec, en, k, true);
+    __syncthreads();
+    inject_h(hc, k);
+    __syncthreads();
+    // H's tile to memory; E's update on the tile (back differences of the new H)
+    for (int q = tid; q < TY * TX; q += NT) {
+      int ly = q / TX, lx = q % TX;
+      int gi = x0 + lx, gj = y0 + ly;
+      if (gi >= nx || gj >= ny) continue;
+      long long r = ((long long)k * ny + gj) * nx + gi;
+      int hy_ = ly + 1, hx_ = lx + 1;  // this value in H's region
+      A.h_out[r] = sH[hc][0][hy_][hx_];
+      A.h_out[N + r] = sH[hc][1][hy_][hx_];
+      A.h_out[2 * N + r] = sH[hc][2][hy_][hx_];
+      // back differences: the neighbour before, zero beyond a wall (wrap_index gave -1 there and
+      // compute_h stored zeros), and along z the previous plane (zero beyond a wall)
+      bool zb = wrap_index(k - 1, nz, A.periodic[2]) >= 0;
+      T hxv = sH[hc][0][hy_][hx_], hyv = sH[hc][1][hy_][hx_], hzv = sH[hc][2][hy_][hx_];
+      T hz_xm = sH[hc][2][hy_][hx_ - 1], hy_xm = sH[hc][1][hy_][hx_ - 1];
+      T hz_ym = sH[hc][2][hy_ - 1][hx_], hx_ym = sH[hc][0][hy_ - 1][hx_];
+      T hy_zm = zb ? sH[hp][1][hy_][hx_] : T(0), hx_zm = zb ? sH[hp][0][hy_][hx_] : T(0);
+      T fx = A.fe[gi], fy = A.fe[nx + gj], fz = A.fe[nx + ny + k];
+      // x: dy(Hz) fy - dz(Hy) fz ; y: dz(Hx) fz - dx(Hz) fx ; z: dx(Hy) fx - dy(Hx) fy
+      T dyHz = hzv - hz_ym, dzHy = hyv - hy_zm, dzHx = hxv - hx_zm, dxHz = hzv - hz_xm;
+      T dxHy = hyv - hy_xm, dyHx = hxv - hx_ym;
+      T curl[3] = {dyHz * fy - dzHy * fz, dzHx * fz - dxHz * fx, dxHy * fx - dyHx * fy};
+      T diffs[3][3] = {{T(0), dyHz, dzHy}, {dxHz, T(0), dzHx}, {dxHy, dyHx, T(0)}};
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T eo = sE[ec][c][ly + 1][lx + 1];
+        T cbv = A.cb[c * N + r];
+        T cav;
+        if (LOSSY) cav = A.ca[c * N + r];
+        else cav = cbv == T(0) ? T(0) : T(1);
+        T v = cav * eo + cbv * curl[c];
+        int w0 = (c + 1) % 3, w1 = (c + 2) % 3;
+        int wa = min(w0, w1), wb = max(w0, w1);
+        int m[3] = {gi, gj, k};
+        const SlabEntry *s;
+        if ((s = slab_at(A, 0, c, wa, m[wa]))) v = slab_update<T, 0>(A, s, c, wa, gi, gj, k, diffs[c][wa], v, cbv, true);
+        if ((s = slab_at(A, 0, c, wb, m[wb]))) v = slab_update<T, 0>(A, s, c, wb, gi, gj, k, diffs[c][wb], v, cbv, true);
+        sEn[c][ly][lx] = v;
+      }
+    }
+    __syncthreads();
+    // The electric currents (src/fdtd.rs:1375-1387): E -= cb Re(a w(t + dt/2)).
+    {
+      int bucket = tile * nz + k;
+      int g0 = A.ebucket[bucket], g1 = A.ebucket[bucket + 1];
+      for (int g = g0 + tid; g < g1; g += NT) {
+        Group gr = A.egroups[g];
+        int ly = gr.local / TX, lx = gr.local % TX;
+        long long r = ((long long)k * ny + (y0 + ly)) * nx + (x0 + lx);
+        T cbv = A.cb[gr.comp * N + r];
+        T *v = &sEn[gr.comp][ly][lx];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          Entry en2 = A.entries[q];
+          double amount =
+              en2.are * A.waves_e[2 * en2.emitter] - en2.aim * A.waves_e[2 * en2.emitter + 1];
+          if (sizeof(T) == 8) *v = *v - (T)((double)cbv * amount);
+          else *v = *v - cbv * (T)amount;
+        }
+      }
+    }
+    __syncthreads();
+    for (int q = tid; q < TY * TX; q += NT) {
+      int ly = q / TX, lx = q % TX;
+      int gi = x0 + lx, gj = y0 + ly;
+      if (gi >= nx || gj >= ny) continue;
+      long long r = ((long long)k * ny + gj) * nx + gi;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T v = sEn[c][ly][lx];
+        if (MEDIA) {
+          // Media::update (src/fdtd/media.rs:670-705): the rest of E's update, then the currents
+          int mi = A.media.member[c * N + r];
+          if (mi >= 0) {
+            const MediaArgs<T> &M = A.media;
+            int g = M.group[mi];
+            int np = M.gpoles[g];
+            T before = M.before[mi];
+            T rest = M.gchi[g] * before;
+            const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+            T *cur = M.current + (long long)mi * M.maxpoles;
+            T *prev = M.previous + (long long)mi * M.maxpoles;
+            for (int p = 0; p < np; p++)
+              rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
+            T next = v + M.scale[mi] * rest;
+            T slope = (next - before) / M.two_dt;
+            for (int p = 0; p < np; p++) {
+              T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
+              prev[p] = cur[p];
+              cur[p] = jn;
+            }
+            M.before[mi] = sE[ec][c][ly + 1][lx + 1];  // E^n, saved before the update
+            v = next;
+          }
+        }
+        A.e_out[c * N + r] = v;
+      }
+    }
+    // this plane's E becomes the staged "plane k" of the next step; H's new plane becomes k-1
+    int t = ec; ec = en; en = t;
+    t = hp; hp = hc; hc = t;
+    __syncthreads();
+  }
+}
+
+// The waveforms of a batch of steps, in f64 (src/fdtd.rs:329-423): for step m of the batch, w
+// at H's time t = (first+m) dt and at E's t + dt/2, 2 doubles each per emitter.
+struct Wave {
+  int kind;
+  double p[5];
+};
+// The waveforms with the reference's exp and sincos (portable.h), so the sources' values are
+// its bits: w.at(t) for a point source, the analytic form w(t) for a current.
+__device__ inline void wave_eval(const Wave &w, double t, double *re, double *im, int point) {
+  if (w.kind == 0) {
+    double u = (t - w.p[2]) / w.p[1];
+    double g = pxp::exp(-u * u);
+    double s, c;
+    if (point) {  // e^{-u^2} sin(omega (t - delay))
+      pxp::sincos((TAU * w.p[0]) * (t - w.p[2]), &s, &c);
+      *re = g * s;
+      *im = 0.0;
+    } else {  // (i e^{-u^2}) e^{-i omega (t - delay)}, as num-complex multiplies
+      pxp::sincos(-(TAU * w.p[0]) * (t - w.p[2]), &s, &c);
+      *re = 0.0 * c - g * s;
+      *im = 0.0 * s + g * c;
+    }
+  } else if (w.kind == 1) {
+    double u = (t - w.p[1]) / w.p[0];
+    *re = -u * pxp::exp(-u * u) * sqrt(2.0 * 2.718281828459045235);
+    *im = 0.0;
+  } else {
+    double ss = 1.0;
+    if (w.p[3] > 0.0) {
+      double r = fmin(fmax(t / w.p[3], 0.0), 1.0);
+      ss = r * r * (3.0 - 2.0 * r);
+    }
+    double s, c;
+    pxp::sincos(-(TAU * w.p[0]) * t, &s, &c);
+    if (point) {  // smoothstep * Re(amplitude e^{-i omega t})
+      *re = ss * (w.p[1] * c - w.p[2] * s);
+      *im = 0.0;
+    } else {  // (smoothstep amplitude) e^{-i omega t}
+      double ar = ss * w.p[1], ai = ss * w.p[2];
+      *re = ar * c - ai * s;
+      *im = ar * s + ai * c;
+    }
+  }
+}
+// point[e]: 1 if emitter e is a point source (w.at), else 0 (complex_at)
+__global__ void waves_kernel(const Wave *waves, const int *point, int nw, long long first,
+                             int batch, double dt, double *out_h, double *out_e) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nw * batch) return;
+  int m = q / nw, e = q % nw;
+  double t = (double)(first + m) * dt;
+  double half = t + 0.5 * dt;
+  double re, im;
+  wave_eval(waves[e], t, &re, &im, point[e]);
+  out_h[2 * ((long long)m * nw + e)] = re;
+  out_h[2 * ((long long)m * nw + e) + 1] = im;
+  wave_eval(waves[e], half, &re, &im, point[e]);
+  out_e[2 * ((long long)m * nw + e)] = re;
+  out_e[2 * ((long long)m * nw + e) + 1] = im;
+}
+
+// After a step: the probes' values into the record, the transformed values into the ring.
+template <typename T>
+__global__ void gather_kernel(const T *e, const T *h, const long long *where, int count,
+                              T *ring_row, const long long *probes, int nprobes, double *record_row) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < count) {
+    long long w = where[q];  // field bit 62, then component * N + r
+    const T *f = (w >> 62) ? h : e;
+    ring_row[q] = f[w & ((1LL << 62) - 1)];
+  } else if (q < count + nprobes) {
+    long long w = probes[q - count];
+    const T *f = (w >> 62) ? h : e;
+    record_row[q - count] = (double)f[w & ((1LL << 62) - 1)];
+  }
+}
+
+// e^{i w t} dt for each step of the batch and each (monitor, field, frequency) slot
+// (src/fdtd/monitors.rs:178-183): E at te = (first+m+1) dt, H at te - dt/2.
+__global__ void phase_kernel(const double *omega, const int *slot_field, int nslots,
+                             long long first, int batch, double dt, double *out) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nslots * batch) return;
+  int m = q / nslots, s = q % nslots;
+  double te = (double)(first + m + 1) * dt;
+  double t = slot_field[s] ? te - 0.5 * dt : te;
+  double sn, cs;
+  pxp::sincos(omega[s] * t, &sn, &cs);
+  out[2 * (long long)q] = cs * dt;
+  out[2 * (long long)q + 1] = sn * dt;
+}
+
+// sums[f][v] += sum_m ring[m][v] * phase[m][slot(f)], m in time order, f64 (monitors.rs:185-206).
+struct SeriesDev {
+  long long value0;  // first value in the ring
+  long long volume;
+  long long sum0;    // first sum (complex)
+  int nf;
+  int slot0;         // its phases' slot for frequency 0
+};
+template <typename T>
+__global__ void dft_kernel(const SeriesDev *series, int nseries, const long long *value_series,
+                           long long nvalues, const T *ring, int batch, const double *phase,
+                           int nslots, double *sums) {
+  long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nvalues) return;
+  SeriesDev s = series[value_series[v]];
+  long long o = v - s.value0;
+  for (int f = 0; f < s.nf; f++) {
+    double *acc = sums + 2 * (s.sum0 + (long long)f * s.volume + o);
+    double re = acc[0], im = acc[1];
+    const double *ph = phase + 2 * (long long)(s.slot0 + f);
+    for (int m = 0; m < batch; m++) {
+      double x = (double)ring[(long long)m * nvalues + v];
+      re = re + x * ph[2 * (long long)m * nslots];
+      im = im + x * ph[2 * (long long)m * nslots + 1];
+    }
+    acc[0] = re;
+    acc[1] = im;
+  }
+}
+
+template <typename T>
+__global__ void convert_kernel(const double *in, T *out, long long n) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) out[q] = (T)in[q];
+}
+template <typename T>
+__global__ void widen_kernel(const T *in, double *out, long long n) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) out[q] = (double)in[q];
+}
+
+}  // namespace pxf
+
+using namespace pxf;
+
+// ------------------------------------------------------------------------------------------
+// The context: the device state of one simulation.
+
+struct DeviceSlab {
+  int field, comp, axis;
+  long long from, count, psi, coef, size;
+};
+
+struct fdtd_ctx {
+  std::string error;
+  int precision = 32;
+  size_t elem = 4;
+  int n[3];
+  long long N;
+  int periodic[3], low[3], high[3];
+  double dt;
+  double step[3];
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> allocations;
+  // fields: two copies each, 3N values
+  void *e[2] = {nullptr, nullptr}, *h[2] = {nullptr, nullptr};
+  int parity = 0;
+  void *ca = nullptr, *cb = nullptr;
+  bool lossless = true, coeffs_set = false, fields_set = false;
+  void *fe = nullptr, *fh = nullptr, *coefs = nullptr;
+  void *psi_h[2] = {nullptr, nullptr}, *psi_e = nullptr;
+  long long psi_h_len = 0, psi_e_len = 0;
+  std::vector<DeviceSlab> slabs;
+  SlabEntry table[2][3][3][2];
+  // launch shape
+  int tiles_x, tiles_y, zchunk, zchunks;
+  // sources
+  int nwaves = 0;
+  Wave *d_waves = nullptr;
+  int *d_point = nullptr;
+  int *hbucket = nullptr, *ebucket = nullptr;
+  Group *hgroups = nullptr, *egroups = nullptr;
+  Entry *entries = nullptr;
+  double *waves_h = nullptr, *waves_e = nullptr;  // batch x nwaves x 2
+  int wave_batch = 0;
+  // probes and transforms
+  int nprobes = 0;
+  long long *d_probes = nullptr;
+  double *record = nullptr;
+  long long record_cap = 0, recorded = 0;
+  long long nvalues = 0;
+  long long *d_where = nullptr, *d_value_series = nullptr;
+  SeriesDev *d_series = nullptr;
+  int nseries = 0, nslots = 0;
+  double *d_omega = nullptr;
+  int *d_slot_field = nullptr;
+  long long nsums = 0;
+  double *sums = nullptr;
+  void *ring = nullptr;
+  double *phase = nullptr;
+  int ring_k = 0;
+  // media
+  bool media = false;
+  MediaArgs<float> mf;
+  MediaArgs<double> md;
+  long long launches = 0;
+  // step-kernel timing: pairs of events around each launch while profiling
+  bool profiling = false;
+  std::vector<cudaEvent_t> events;
+  size_t events_used = 0;
+};
+
+namespace {
+
+int fail(fdtd_ctx *c, int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->error = buf;
+  return code;
+}
+
+#define CUDA_TRY(c, call)                                                                      \
+  do {                                                                                         \
+    cudaError_t err_ = (call);                                                                 \
+    if (err_ != cudaSuccess)                                                                   \
+      return fail((c), FDTD_E_GPU, "%s: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, \
+                  __LINE__);                                                                   \
+  } while (0)
+
+int alloc(fdtd_ctx *c, void **p, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 16);
+  if (c->budget && c->used + bytes > c->budget)
+    return fail(c, FDTD_E_BUDGET, "%zu MB more would exceed the HBM budget of %zu MB",
+                bytes >> 20, c->budget >> 20);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, FDTD_E_GPU, "cudaMalloc of %zu MB: %s", bytes >> 20, cudaGetErrorString(e));
+  }
+  c->used += bytes;
+  c->allocations.push_back(*p);
+  return 0;
+}
+void release(fdtd_ctx *c, void *p) {
+  if (!p) return;
+  auto it = std::find(c->allocations.begin(), c->allocations.end(), p);
+  if (it != c->allocations.end()) c->allocations.erase(it);
+  cudaFree(p);
+}
+
+template <typename T>
+int upload_as(fdtd_ctx *c, void *dst, const double *src, long long n) {
+  // through a staging copy of f64 on the device, converted there
+  if (n == 0) return 0;
+  if (sizeof(T) == 8) {
+    CUDA_TRY(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+  }
+  double *stage = nullptr;
+  long long chunk = std::min<long long>(n, 1LL << 24);
+  CUDA_TRY(c, cudaMallocAsync((void **)&stage, chunk * 8, c->stream));
+  for (long long at = 0; at < n; at += chunk) {
+    long long m = std::min(chunk, n - at);
+    cudaMemcpyAsync(stage, src + at, m * 8, cudaMemcpyHostToDevice, c->stream);
+    convert_kernel<T><<<(unsigned)((m + 255) / 256), 256, 0, c->stream>>>(stage, (T *)dst + at, m);
+  }
+  cudaFreeAsync(stage, c->stream);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaGetLastError());
+  return 0;
+}
+int upload(fdtd_ctx *c, void *dst, const double *src, long long n) {
+  return c->precision == 64 ? upload_as<double>(c, dst, src, n) : upload_as<float>(c, dst, src, n);
+}
+template <typename T>
+int download_as(fdtd_ctx *c, double *dst, const void *src, long long n) {
+  if (n == 0) return 0;
+  if (sizeof(T) == 8) {
+    CUDA_TRY(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return 0;
+  }
+  double *stage = nullptr;
+  long long chunk = std::min<long long>(n, 1LL << 24);
+  CUDA_TRY(c, cudaMallocAsync((void **)&stage, chunk * 8, c->stream));
+  for (long long at = 0; at < n; at += chunk) {
+    long long m = std::min(chunk, n - at);
+    widen_kernel<T><<<(unsigned)((m + 255) / 256), 256, 0, c->stream>>>((const T *)src + at, stage, m);
+    cudaMemcpyAsync(dst + at, stage, m * 8, cudaMemcpyDeviceToHost, c->stream);
+  }
+  cudaFreeAsync(stage, c->stream);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaGetLastError());
+  return 0;
+}
+int download(fdtd_ctx *c, double *dst, const void *src, long long n) {
+  return c->precision == 64 ? download_as<double>(c, dst, src, n)
+                            : download_as<float>(c, dst, src, n);
+}
+
+template <typename T>
+StepArgs<T> step_args(fdtd_ctx *c) {
+  StepArgs<T> A;
+  for (int a = 0; a < 3; a++) {
+    A.n[a] = c->n[a];
+    A.periodic[a] = c->periodic[a];
+    A.low[a] = c->low[a];
+    A.high[a] = c->high[a];
+    A.step[a] = (T)c->step[a];
+  }
+  A.N = c->N;
+  A.dt = (T)c->dt;
+  A.fe = (const T *)c->fe;
+  A.fh = (const T *)c->fh;
+  A.e_in = (const T *)c->e[c->parity];
+  A.h_in = (const T *)c->h[c->parity];
+  A.e_out = (T *)c->e[1 - c->parity];
+  A.h_out = (T *)c->h[1 - c->parity];
+  A.ca = c->lossless ? nullptr : (const T *)c->ca;
+  A.cb = (const T *)c->cb;
+  memcpy(A.slab, c->table, sizeof A.slab);
+  A.coefs = (const T *)c->coefs;
+  A.psi_h_in = (const T *)c->psi_h[c->parity];
+  A.psi_h_out = (T *)c->psi_h[1 - c->parity];
+  A.psi_e = (T *)c->psi_e;
+  A.hbucket = c->hbucket;
+  A.ebucket = c->ebucket;
+  A.hgroups = c->hgroups;
+  A.egroups = c->egroups;
+  A.entries = c->entries;
+  A.tiles_x = c->tiles_x;
+  A.tiles_y = c->tiles_y;
+  A.zchunk = c->zchunk;
+  if (sizeof(T) == 8) memcpy(&A.media, &c->md, sizeof A.media);
+  else memcpy(&A.media, &c->mf, sizeof A.media);
+  return A;
+}
+
+template <typename T>
+void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
+  dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
+  if (c->media) {
+    if (c->lossless) step_kernel<T, false, true><<<grid, NT, 0, c->stream>>>(A);
+    else step_kernel<T, true, true><<<grid, NT, 0, c->stream>>>(A);
+  } else {
+    if (c->lossless) step_kernel<T, false, false><<<grid, NT, 0, c->stream>>>(A);
+    else step_kernel<T, true, false><<<grid, NT, 0, c->stream>>>(A);
+  }
+}
+
+// Empty source tables: every bucket empty.
+int empty_sources(fdtd_ctx *c) {
+  long long nb = (long long)c->tiles_x * c->tiles_y * c->n[2] + 1;
+  std::vector<int> zero(nb, 0);
+  release(c, c->hbucket);
+  release(c, c->ebucket);
+  c->hbucket = c->ebucket = nullptr;
+  if (int r = alloc(c, (void **)&c->hbucket, nb * 4)) return r;
+  if (int r = alloc(c, (void **)&c->ebucket, nb * 4)) return r;
+  CUDA_TRY(c, cudaMemcpy(c->hbucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->ebucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+template <typename T>
+int run_impl(fdtd_ctx *c, long long steps, long long first) {
+  if (!c->coeffs_set || !c->fields_set)
+    return fail(c, FDTD_E_STATE, "upload the coefficients and the fields before a run");
+  const int K = c->ring_k > 0 ? c->ring_k : 64;
+  // the probes' record: grow to the run's steps
+  if (c->nprobes > 0 && c->recorded + steps > c->record_cap) {
+    long long cap = std::max<long long>(c->recorded + steps, 2 * c->record_cap);
+    double *nr = nullptr;
+    if (int r = alloc(c, (void **)&nr, (size_t)cap * c->nprobes * 8)) return r;
+    if (c->record && c->recorded)
+      CUDA_TRY(c, cudaMemcpyAsync(nr, c->record, (size_t)c->recorded * c->nprobes * 8,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    release(c, c->record);
+    c->record = nr;
+    c->record_cap = cap;
+  }
+  long long done = 0;
+  while (done < steps) {
+    int batch = (int)std::min<long long>(K, steps - done);
+    if (c->nwaves > 0) {
+      int total = c->nwaves * batch;
+      waves_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(
+          c->d_waves, c->d_point, c->nwaves, first + done, batch, c->dt, c->waves_h, c->waves_e);
+      c->launches++;
+    }
+    for (int m = 0; m < batch; m++) {
+      StepArgs<T> A = step_args<T>(c);
+      A.waves_h = c->waves_h + 2LL * m * c->nwaves;
+      A.waves_e = c->waves_e + 2LL * m * c->nwaves;
+      if (c->profiling) {
+        if (c->events_used + 2 > c->events.size()) {
+          for (int q = 0; q < 256; q++) {
+            cudaEvent_t ev;
+            cudaEventCreate(&ev);
+            c->events.push_back(ev);
+          }
+        }
+        cudaEventRecord(c->events[c->events_used++], c->stream);
+        launch_step<T>(c, A);
+        cudaEventRecord(c->events[c->events_used++], c->stream);
+      } else {
+        launch_step<T>(c, A);
+      }
+      c->launches++;
+      c->parity = 1 - c->parity;
+      long long gathered = c->nvalues + c->nprobes;
+      if (gathered > 0) {
+        T *row = c->nvalues ? (T *)c->ring + (long long)m * c->nvalues : nullptr;
+        double *rec = c->nprobes ? c->record + (c->recorded + done + m) * c->nprobes : nullptr;
+        gather_kernel<T><<<(unsigned)((gathered + 255) / 256), 256, 0, c->stream>>>(
+            (const T *)c->e[c->parity], (const T *)c->h[c->parity], c->d_where, (int)c->nvalues,
+            row, c->d_probes, c->nprobes, rec);
+        c->launches++;
+      }
+    }
+    if (c->nvalues > 0) {
+      int total = c->nslots * batch;
+      phase_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(c->d_omega, c->d_slot_field,
+                                                                c->nslots, first + done, batch,
+                                                                c->dt, c->phase);
+      dft_kernel<T><<<(unsigned)((c->nvalues + 127) / 128), 128, 0, c->stream>>>(
+          c->d_series, c->nseries, c->d_value_series, c->nvalues, (const T *)c->ring, batch,
+          c->phase, c->nslots, c->sums);
+      c->launches += 2;
+    }
+    done += batch;
+  }
+  c->recorded += steps;
+  CUDA_TRY(c, cudaGetLastError());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fdtd_last_error(const fdtd_ctx *ctx) { return ctx ? ctx->error.c_str() : "no context"; }
+
+int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const double *factor_e,
+                const double *factor_h, const fdtd_slab *slabs, int32_t nslabs, int32_t precision,
+                size_t hbm_budget, fdtd_ctx **out) {
+  if (!out || !grid || !step || !factor_e || !factor_h) return FDTD_E_INVALID;
+  *out = nullptr;
+  fdtd_ctx *c = new fdtd_ctx();
+  c->precision = precision == 64 ? 64 : 32;
+  c->elem = c->precision == 64 ? 8 : 4;
+  c->budget = hbm_budget;
+  c->dt = dt;
+  long long N = 1;
+  for (int a = 0; a < 3; a++) {
+    if (grid->n[a] <= 0 || grid->n[a] > (1 << 30)) {
+      fail(c, FDTD_E_INVALID, "the grid needs cells along every axis, got %lld along axis %d",
+           (long long)grid->n[a], a);
+      *out = c;
+      return FDTD_E_INVALID;
+    }
+    c->n[a] = (int)grid->n[a];
+    c->periodic[a] = grid->periodic[a] ? 1 : 0;
+    c->low[a] = c->periodic[a] ? 0 : (int)grid->low[a];
+    c->high[a] = c->periodic[a] ? 0 : (int)grid->high[a];
+    if (!c->periodic[a] && (c->low[a] < 0 || c->high[a] < 0 || c->low[a] + c->high[a] >= c->n[a])) {
+      fail(c, FDTD_E_INVALID, "CPMLs of %d and %d cells leave nothing of %d cells", c->low[a],
+           c->high[a], c->n[a]);
+      *out = c;
+      return FDTD_E_INVALID;
+    }
+    c->step[a] = step[a];
+    N *= c->n[a];
+  }
+  c->N = N;
+  *out = c;
+  if (!(dt > 0.0 && std::isfinite(dt)))
+    return fail(c, FDTD_E_INVALID, "the time step must be positive, got %g", dt);
+  CUDA_TRY(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  size_t E = c->elem;
+  for (int p = 0; p < 2; p++) {
+    if (int r = alloc(c, &c->e[p], 3 * N * E)) return r;
+    if (int r = alloc(c, &c->h[p], 3 * N * E)) return r;
+  }
+  if (int r = alloc(c, &c->cb, 3 * N * E)) return r;
+  long long nf = (long long)c->n[0] + c->n[1] + c->n[2];
+  if (int r = alloc(c, &c->fe, nf * E)) return r;
+  if (int r = alloc(c, &c->fh, nf * E)) return r;
+  if (int r = upload(c, c->fe, factor_e, nf)) return r;
+  if (int r = upload(c, c->fh, factor_h, nf)) return r;
+  // the slabs: psi for E in place, for H in two copies; their coefficients in one table
+  memset(c->table, 0, sizeof c->table);
+  std::vector<double> coefs;
+  for (int s = 0; s < nslabs; s++) {
+    const fdtd_slab &sl = slabs[s];
+    int w = sl.axis, comp = sl.component, field = sl.field;
+    if (w < 0 || w > 2 || comp < 0 || comp > 2 || field < 0 || field > 1 || comp == w ||
+        c->periodic[w] || sl.count <= 0 || sl.from < 0 || sl.from + sl.count > c->n[w])
+      return fail(c, FDTD_E_INVALID, "slab %d is not a CPML slab of this grid", s);
+    int side;
+    if (sl.from == 0 && sl.count == c->low[w]) side = 0;
+    else if (sl.from + sl.count == c->n[w] && sl.count == c->high[w]) side = 1;
+    else return fail(c, FDTD_E_INVALID, "slab %d does not match the grid's CPML cells", s);
+    DeviceSlab d;
+    d.field = field;
+    d.comp = comp;
+    d.axis = w;
+    d.from = sl.from;
+    d.count = sl.count;
+    d.size = sl.count * (N / c->n[w]);
+    d.coef = (long long)coefs.size();
+    d.psi = field == 1 ? c->psi_h_len : c->psi_e_len;
+    (field == 1 ? c->psi_h_len : c->psi_e_len) += d.size;
+    for (long long q = 0; q < sl.count; q++) coefs.push_back(sl.b[q]);
+    for (long long q = 0; q < sl.count; q++) coefs.push_back(sl.a[q]);
+    c->slabs.push_back(d);
+    SlabEntry &t = c->table[field][comp][w][side];
+    t.from = (int)sl.from;
+    t.count = (int)sl.count;
+    t.psi = d.psi;
+    t.coef = (int)d.coef;
+  }
+  if (int r = alloc(c, &c->coefs, coefs.size() * E)) return r;
+  if (int r = upload(c, c->coefs, coefs.data(), (long long)coefs.size())) return r;
+  for (int p = 0; p < 2; p++)
+    if (int r = alloc(c, &c->psi_h[p], c->psi_h_len * E)) return r;
+  if (int r = alloc(c, &c->psi_e, c->psi_e_len * E)) return r;
+  CUDA_TRY(c, cudaMemsetAsync(c->psi_h[0], 0, c->psi_h_len * E, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->psi_h[1], 0, c->psi_h_len * E, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->psi_e, 0, c->psi_e_len * E, c->stream));
+  // launch shape: tiles of TX x TY, and the z planes cut into runs so that the grid holds
+  // several CTAs per SM
+  c->tiles_x = (c->n[0] + TX - 1) / TX;
+  c->tiles_y = (c->n[1] + TY - 1) / TY;
+  int sms = 148;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  long long tiles = (long long)c->tiles_x * c->tiles_y;
+  long long want = 8LL * sms;
+  int chunks = (int)std::min<long long>(c->n[2], std::max<long long>(1, (want + tiles - 1) / tiles));
+  c->zchunk = (c->n[2] + chunks - 1) / chunks;
+  c->zchunks = (c->n[2] + c->zchunk - 1) / c->zchunk;
+  if (int r = empty_sources(c)) return r;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+void fdtd_destroy(fdtd_ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (cudaEvent_t ev : c->events) cudaEventDestroy(ev);
+  for (void *p : c->allocations) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int fdtd_upload_coeffs(fdtd_ctx *c, const double *ca, const double *cb) {
+  if (!c || !cb) return fail(c, FDTD_E_INVALID, "cb is needed");
+  c->lossless = ca == nullptr;
+  if (ca) {
+    if (!c->ca)
+      if (int r = alloc(c, &c->ca, 3 * c->N * c->elem)) return r;
+    if (int r = upload(c, c->ca, ca, 3 * c->N)) return r;
+  }
+  if (int r = upload(c, c->cb, cb, 3 * c->N)) return r;
+  c->coeffs_set = true;
+  return 0;
+}
+
+int fdtd_upload_fields(fdtd_ctx *c, const double *e, const double *h, const double *const *psi) {
+  if (!c) return FDTD_E_INVALID;
+  c->parity = 0;
+  size_t E = c->elem;
+  if (e) { if (int r = upload(c, c->e[0], e, 3 * c->N)) return r; }
+  else CUDA_TRY(c, cudaMemsetAsync(c->e[0], 0, 3 * c->N * E, c->stream));
+  if (h) { if (int r = upload(c, c->h[0], h, 3 * c->N)) return r; }
+  else CUDA_TRY(c, cudaMemsetAsync(c->h[0], 0, 3 * c->N * E, c->stream));
+  for (size_t s = 0; s < c->slabs.size(); s++) {
+    const DeviceSlab &d = c->slabs[s];
+    void *base = d.field == 1 ? c->psi_h[0] : c->psi_e;
+    void *dst = (char *)base + d.psi * E;
+    if (psi && psi[s]) { if (int r = upload(c, dst, psi[s], d.size)) return r; }
+    else CUDA_TRY(c, cudaMemsetAsync(dst, 0, d.size * E, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->fields_set = true;
+  return 0;
+}
+
+int fdtd_download_fields(fdtd_ctx *c, double *e, double *h, double *const *psi) {
+  if (!c) return FDTD_E_INVALID;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (e) if (int r = download(c, e, c->e[c->parity], 3 * c->N)) return r;
+  if (h) if (int r = download(c, h, c->h[c->parity], 3 * c->N)) return r;
+  if (psi)
+    for (size_t s = 0; s < c->slabs.size(); s++) {
+      if (!psi[s]) continue;
+      const DeviceSlab &d = c->slabs[s];
+      const void *base = d.field == 1 ? c->psi_h[c->parity] : c->psi_e;
+      if (int r = download(c, psi[s], (const char *)base + d.psi * c->elem, d.size)) return r;
+    }
+  return 0;
+}
+
+int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, int64_t ninj,
+                     const fdtd_injection *inj) {
+  if (!c) return FDTD_E_INVALID;
+  int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+  std::vector<int> point(std::max(nwaves, 1), -1);
+  for (int64_t q = 0; q < ninj; q++) {
+    const fdtd_injection &x = inj[q];
+    if (x.field < 0 || x.field > 1 || x.component < 0 || x.component > 2 || x.r < 0 ||
+        x.r >= c->N || x.emitter < 0 || x.emitter >= nwaves || !std::isfinite(x.a_re) ||
+        !std::isfinite(x.a_im))
+      return fail(c, FDTD_E_INVALID, "injection %lld is outside the grid or not finite",
+                  (long long)q);
+    int want = x.point ? 1 : 0;
+    if (point[x.emitter] >= 0 && point[x.emitter] != want)
+      return fail(c, FDTD_E_INVALID, "emitter %d is both a point source and a current", x.emitter);
+    point[x.emitter] = want;
+  }
+  for (int w = 0; w < nwaves; w++)
+    if (waves[w].kind < 0 || waves[w].kind > 2)
+      return fail(c, FDTD_E_INVALID, "waveform %d has no kind %d", w, waves[w].kind);
+  // Group by value in CPU order (Resident::plan, resident.rs:546-590), then by (tile, plane):
+  // an H value also goes to the tiles whose low halo row or column it is.
+  struct Item { long long key; int local; int comp; std::vector<int> entries; };
+  std::vector<Entry> entries;
+  std::vector<std::vector<Item>> per_field(2);
+  for (int f = 0; f < 2; f++) {
+    std::vector<long long> order;
+    std::vector<std::vector<int>> lists;
+    std::vector<long long> places;
+    // value -> position in order
+    std::unordered_map<long long, int> index;
+    for (int64_t q = 0; q < ninj; q++) {
+      const fdtd_injection &x = inj[q];
+      if (x.field != f) continue;
+      long long place = (long long)x.component * c->N + x.r;
+      int at = -1;
+      auto found = index.find(place);
+      if (found != index.end()) at = found->second;
+      if (at < 0) {
+        at = (int)places.size();
+        index[place] = at;
+        places.push_back(place);
+        lists.emplace_back();
+      }
+      Entry en;
+      en.are = x.a_re;
+      en.aim = x.a_im;
+      en.emitter = x.emitter;
+      en.pad = 0;
+      lists[at].push_back((int)entries.size());
+      entries.push_back(en);
+    }
+    for (size_t g = 0; g < places.size(); g++) {
+      int comp = (int)(places[g] / c->N);
+      long long r = places[g] % c->N;
+      int i = (int)(r % nx), j = (int)((r / nx) % ny), k = (int)(r / ((long long)nx * ny));
+      int tx = i / TX, ty = j / TY;
+      auto push = [&](int ttx, int tty, int lx, int ly, int width) {
+        Item it;
+        it.key = ((long long)(tty * c->tiles_x + ttx)) * nz + k;
+        it.local = ly * width + lx;
+        it.comp = comp;
+        it.entries = lists[g];
+        per_field[f].push_back(it);
+      };
+      if (f == 0) {
+        push(tx, ty, i - tx * TX, j - ty * TY, TX);
+      } else {
+        push(tx, ty, i - tx * TX + 1, j - ty * TY + 1, HX);
+        // the tiles whose low halo this value is: next along x, next along y (wrapping on a
+        // periodic axis), and the diagonal one
+        int txn = -1, tyn = -1, lxn = 0, lyn = 0;
+        if (i == (tx + 1) * TX - 1 && (tx + 1) < c->tiles_x) { txn = tx + 1; lxn = 0; }
+        if (c->periodic[0] && i == nx - 1 && c->tiles_x > 0) { txn = 0; lxn = 0; }
+        if (j == (ty + 1) * TY - 1 && (ty + 1) < c->tiles_y) { tyn = ty + 1; lyn = 0; }
+        if (c->periodic[1] && j == ny - 1 && c->tiles_y > 0) { tyn = 0; lyn = 0; }
+        if (txn >= 0) push(txn, ty, lxn, j - ty * TY + 1, HX);
+        if (tyn >= 0) push(tx, tyn, i - tx * TX + 1, lyn, HX);
+        if (txn >= 0 && tyn >= 0) push(txn, tyn, lxn, lyn, HX);
+      }
+    }
+  }
+  long long nb = (long long)c->tiles_x * c->tiles_y * nz + 1;
+  std::vector<Entry> ordered_entries;
+  std::vector<Group> groups[2];
+  std::vector<int> buckets[2];
+  for (int f = 0; f < 2; f++) {
+    auto &items = per_field[f];
+    std::stable_sort(items.begin(), items.end(),
+                     [](const Item &a, const Item &b) { return a.key < b.key; });
+    buckets[f].assign(nb, 0);
+    for (auto &it : items) {
+      Group g;
+      g.local = it.local;
+      g.comp = it.comp;
+      g.first = (int)ordered_entries.size();
+      g.count = (int)it.entries.size();
+      for (int e : it.entries) ordered_entries.push_back(entries[e]);
+      groups[f].push_back(g);
+      buckets[f][it.key + 1]++;
+    }
+    for (long long b = 1; b < nb; b++) buckets[f][b] += buckets[f][b - 1];
+  }
+  release(c, c->hbucket); release(c, c->ebucket); release(c, c->hgroups); release(c, c->egroups);
+  release(c, c->entries); release(c, c->d_waves); release(c, c->d_point);
+  release(c, c->waves_h); release(c, c->waves_e);
+  c->hbucket = c->ebucket = nullptr;
+  c->hgroups = c->egroups = nullptr;
+  c->entries = nullptr;
+  c->d_waves = nullptr;
+  c->d_point = nullptr;
+  c->waves_h = c->waves_e = nullptr;
+  if (int r = alloc(c, (void **)&c->hbucket, nb * 4)) return r;
+  if (int r = alloc(c, (void **)&c->ebucket, nb * 4)) return r;
+  if (int r = alloc(c, (void **)&c->hgroups, groups[1].size() * sizeof(Group))) return r;
+  if (int r = alloc(c, (void **)&c->egroups, groups[0].size() * sizeof(Group))) return r;
+  if (int r = alloc(c, (void **)&c->entries, ordered_entries.size() * sizeof(Entry))) return r;
+  CUDA_TRY(c, cudaMemcpy(c->hbucket, buckets[1].data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->ebucket, buckets[0].data(), nb * 4, cudaMemcpyHostToDevice));
+  if (!groups[1].empty())
+    CUDA_TRY(c, cudaMemcpy(c->hgroups, groups[1].data(), groups[1].size() * sizeof(Group), cudaMemcpyHostToDevice));
+  if (!groups[0].empty())
+    CUDA_TRY(c, cudaMemcpy(c->egroups, groups[0].data(), groups[0].size() * sizeof(Group), cudaMemcpyHostToDevice));
+  if (!ordered_entries.empty())
+    CUDA_TRY(c, cudaMemcpy(c->entries, ordered_entries.data(), ordered_entries.size() * sizeof(Entry), cudaMemcpyHostToDevice));
+  c->nwaves = nwaves;
+  if (nwaves > 0) {
+    std::vector<Wave> w(nwaves);
+    for (int q = 0; q < nwaves; q++) {
+      w[q].kind = waves[q].kind;
+      for (int p = 0; p < 5; p++) w[q].p[p] = waves[q].p[p];
+      if (point[q] < 0) point[q] = 0;
+    }
+    const int K = c->ring_k > 0 ? c->ring_k : 64;
+    if (int r = alloc(c, (void **)&c->d_waves, nwaves * sizeof(Wave))) return r;
+    if (int r = alloc(c, (void **)&c->d_point, nwaves * sizeof(int))) return r;
+    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * nwaves * 16)) return r;
+    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * nwaves * 16)) return r;
+    c->wave_batch = K;
+    CUDA_TRY(c, cudaMemcpy(c->d_waves, w.data(), nwaves * sizeof(Wave), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(c->d_point, point.data(), nwaves * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+int fdtd_set_probes(fdtd_ctx *c, int32_t n, const int32_t *field, const int32_t *component,
+                    const int64_t *r) {
+  if (!c) return FDTD_E_INVALID;
+  std::vector<long long> w(std::max(n, 1));
+  for (int p = 0; p < n; p++) {
+    if (field[p] < 0 || field[p] > 1 || component[p] < 0 || component[p] > 2 || r[p] < 0 ||
+        r[p] >= c->N)
+      return fail(c, FDTD_E_INVALID, "probe %d is outside the grid", p);
+    w[p] = ((long long)field[p] << 62) | ((long long)component[p] * c->N + r[p]);
+  }
+  release(c, c->d_probes);
+  release(c, c->record);
+  c->d_probes = nullptr;
+  c->record = nullptr;
+  c->record_cap = c->recorded = 0;
+  c->nprobes = n;
+  if (n > 0) {
+    if (int rr = alloc(c, (void **)&c->d_probes, n * 8)) return rr;
+    CUDA_TRY(c, cudaMemcpy(c->d_probes, w.data(), n * 8, cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+int fdtd_set_dft(fdtd_ctx *c, int32_t nseries, const fdtd_series *series, int32_t nmonitors,
+                 const int32_t *freqs_per_monitor, const double *freqs) {
+  if (!c) return FDTD_E_INVALID;
+  // phase slots: per monitor, its frequencies at E's times then at H's (resident.rs:714-730)
+  std::vector<int> slot0(nmonitors + 1, 0), fcount(nmonitors, 0), fstart(nmonitors, 0);
+  std::vector<double> omega;
+  std::vector<int> slot_field;
+  int at = 0;
+  for (int m = 0; m < nmonitors; m++) {
+    fstart[m] = at;
+    fcount[m] = freqs_per_monitor[m];
+    slot0[m] = (int)omega.size();
+    for (int fld = 0; fld < 2; fld++)
+      for (int f = 0; f < fcount[m]; f++) {
+        double fr = freqs[at + f];
+        if (!(fr > 0 && std::isfinite(fr) && TAU * fr * c->dt < M_PI))
+          return fail(c, FDTD_E_INVALID, "frequency %g is at or beyond the Nyquist frequency", fr);
+        omega.push_back(TAU * fr);
+        slot_field.push_back(fld);
+      }
+    at += fcount[m];
+  }
+  std::vector<SeriesDev> sd(nseries);
+  std::vector<long long> where, value_series;
+  long long values = 0, sums = 0;
+  for (int s = 0; s < nseries; s++) {
+    const fdtd_series &x = series[s];
+    if (x.monitor < 0 || x.monitor >= nmonitors || x.field < 0 || x.field > 1 ||
+        x.component < 0 || x.component > 2)
+      return fail(c, FDTD_E_INVALID, "series %d is malformed", s);
+    long long vol = 1;
+    for (int a = 0; a < 3; a++) {
+      if (x.lo[a] < 0 || x.len[a] <= 0 || x.lo[a] + x.len[a] > c->n[a])
+        return fail(c, FDTD_E_INVALID, "series %d's box is not on the grid", s);
+      vol *= x.len[a];
+    }
+    sd[s].value0 = values;
+    sd[s].volume = vol;
+    sd[s].sum0 = sums;
+    sd[s].nf = fcount[x.monitor];
+    sd[s].slot0 = slot0[x.monitor] + (x.field == 1 ? fcount[x.monitor] : 0);
+    for (long long k = 0; k < x.len[2]; k++)
+      for (long long j = 0; j < x.len[1]; j++)
+        for (long long i = 0; i < x.len[0]; i++) {
+          long long r = ((x.lo[2] + k) * c->n[1] + (x.lo[1] + j)) * c->n[0] + (x.lo[0] + i);
+          where.push_back(((long long)x.field << 62) | ((long long)x.component * c->N + r));
+          value_series.push_back(s);
+        }
+    values += vol;
+    sums += vol * sd[s].nf;
+  }
+  for (void *p : {(void *)c->d_where, (void *)c->d_value_series, (void *)c->d_series,
+                  (void *)c->d_omega, (void *)c->d_slot_field, (void *)c->sums, c->ring,
+                  (void *)c->phase})
+    release(c, p);
+  c->d_where = c->d_value_series = nullptr;
+  c->d_series = nullptr;
+  c->d_omega = nullptr;
+  c->d_slot_field = nullptr;
+  c->sums = nullptr;
+  c->ring = nullptr;
+  c->phase = nullptr;
+  c->nvalues = values;
+  c->nseries = nseries;
+  c->nslots = (int)omega.size();
+  c->nsums = sums;
+  if (values == 0) return 0;
+  // the ring: K steps of the values, K as large as 64 while it stays within 1 GB
+  long long K = 64;
+  while (K > 4 && (size_t)K * values * c->elem > (1ULL << 30)) K /= 2;
+  c->ring_k = (int)K;
+  if (int r = alloc(c, (void **)&c->d_where, values * 8)) return r;
+  if (int r = alloc(c, (void **)&c->d_value_series, values * 8)) return r;
+  if (int r = alloc(c, (void **)&c->d_series, nseries * sizeof(SeriesDev))) return r;
+  if (int r = alloc(c, (void **)&c->d_omega, omega.size() * 8)) return r;
+  if (int r = alloc(c, (void **)&c->d_slot_field, slot_field.size() * 4)) return r;
+  if (int r = alloc(c, (void **)&c->sums, sums * 16)) return r;
+  if (int r = alloc(c, &c->ring, K * values * c->elem)) return r;
+  if (int r = alloc(c, (void **)&c->phase, K * omega.size() * 16)) return r;
+  CUDA_TRY(c, cudaMemcpy(c->d_where, where.data(), values * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->d_value_series, value_series.data(), values * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->d_series, sd.data(), nseries * sizeof(SeriesDev), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->d_omega, omega.data(), omega.size() * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(c->d_slot_field, slot_field.data(), slot_field.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemset(c->sums, 0, sums * 16));
+  // the source waves' batch must match the ring's
+  if (c->nwaves > 0 && c->wave_batch < K) {
+    release(c, c->waves_h);
+    release(c, c->waves_e);
+    c->waves_h = c->waves_e = nullptr;
+    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * c->nwaves * 16)) return r;
+    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * c->nwaves * 16)) return r;
+    c->wave_batch = (int)K;
+  }
+  return 0;
+}
+
+int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups) {
+  if (!c) return FDTD_E_INVALID;
+  long long members = 0;
+  int maxp = 1;
+  for (int g = 0; g < ngroups; g++) {
+    members += groups[g].count;
+    maxp = std::max(maxp, (int)groups[g].npoles);
+  }
+  c->media = members > 0;
+  if (!c->media) return 0;
+  std::vector<int> member(3 * c->N, -1), group(members);
+  std::vector<double> scale(members), gchi(ngroups), gpole((size_t)ngroups * maxp * 3, 0.0);
+  std::vector<int> gpoles(ngroups);
+  long long m = 0;
+  for (int g = 0; g < ngroups; g++) {
+    const fdtd_media_group &G = groups[g];
+    gchi[g] = G.chi;
+    gpoles[g] = G.npoles;
+    for (int p = 0; p < G.npoles; p++)
+      for (int q = 0; q < 3; q++) gpole[((size_t)g * maxp + p) * 3 + q] = G.poles[3 * p + q];
+    for (long long v = 0; v < G.count; v++, m++) {
+      if (G.component[v] < 0 || G.component[v] > 2 || G.r[v] < 0 || G.r[v] >= c->N)
+        return fail(c, FDTD_E_INVALID, "a medium's value is outside the grid");
+      long long at = G.component[v] * c->N + G.r[v];
+      if (member[at] >= 0) return fail(c, FDTD_E_INVALID, "a value is in two media");
+      member[at] = (int)m;
+      group[m] = g;
+      scale[m] = G.scale[v];
+    }
+  }
+  size_t E = c->elem;
+  void *d_member, *d_group, *d_scale, *d_before, *d_cur, *d_prev, *d_gchi, *d_gpoles, *d_gpole;
+  if (int r = alloc(c, &d_member, member.size() * 4)) return r;
+  if (int r = alloc(c, &d_group, members * 4)) return r;
+  if (int r = alloc(c, &d_scale, members * E)) return r;
+  if (int r = alloc(c, &d_before, members * E)) return r;
+  if (int r = alloc(c, &d_cur, members * maxp * E)) return r;
+  if (int r = alloc(c, &d_prev, members * maxp * E)) return r;
+  if (int r = alloc(c, &d_gchi, ngroups * E)) return r;
+  if (int r = alloc(c, &d_gpoles, ngroups * 4)) return r;
+  if (int r = alloc(c, &d_gpole, gpole.size() * E)) return r;
+  CUDA_TRY(c, cudaMemcpy(d_member, member.data(), member.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(d_group, group.data(), members * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(d_gpoles, gpoles.data(), ngroups * 4, cudaMemcpyHostToDevice));
+  if (int r = upload(c, d_scale, scale.data(), members)) return r;
+  if (int r = upload(c, d_gchi, gchi.data(), ngroups)) return r;
+  if (int r = upload(c, d_gpole, gpole.data(), (long long)gpole.size())) return r;
+  CUDA_TRY(c, cudaMemset(d_before, 0, members * E));
+  CUDA_TRY(c, cudaMemset(d_cur, 0, members * maxp * E));
+  CUDA_TRY(c, cudaMemset(d_prev, 0, members * maxp * E));
+  auto fillm = [&](auto &M) {
+    using T = typename std::remove_pointer<decltype(M.scale)>::type;
+    using TT = typename std::remove_const<T>::type;
+    M.member = (const int *)d_member;
+    M.group = (const int *)d_group;
+    M.scale = (const TT *)d_scale;
+    M.before = (TT *)d_before;
+    M.current = (TT *)d_cur;
+    M.previous = (TT *)d_prev;
+    M.maxpoles = maxp;
+    M.ngroups = ngroups;
+    M.gchi = (const TT *)d_gchi;
+    M.gpoles = (const int *)d_gpoles;
+    M.gpole = (const TT *)d_gpole;
+    M.two_dt = (TT)(2.0 * c->dt);
+  };
+  if (c->precision == 64) fillm(c->md);
+  else fillm(c->mf);
+  return 0;
+}
+
+int fdtd_run_async(fdtd_ctx *c, int64_t steps, int64_t first_step) {
+  if (!c) return FDTD_E_INVALID;
+  if (steps < 0) return fail(c, FDTD_E_INVALID, "a negative number of steps");
+  if (steps == 0) return 0;
+  c->launches = 0;
+  return c->precision == 64 ? run_impl<double>(c, steps, first_step)
+                            : run_impl<float>(c, steps, first_step);
+}
+
+int fdtd_synchronize(fdtd_ctx *c) {
+  if (!c) return FDTD_E_INVALID;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaGetLastError());
+  return 0;
+}
+
+int fdtd_run(fdtd_ctx *c, int64_t steps, int64_t first_step) {
+  if (int r = fdtd_run_async(c, steps, first_step)) return r;
+  return fdtd_synchronize(c);
+}
+
+int fdtd_read_probes(fdtd_ctx *c, double *out, int64_t capacity, int64_t *steps) {
+  if (!c) return FDTD_E_INVALID;
+  if (steps) *steps = c->nprobes > 0 ? c->recorded : 0;
+  if (!out || c->nprobes == 0) return 0;
+  long long n = c->recorded * c->nprobes;
+  if (capacity < n) return fail(c, FDTD_E_INVALID, "%lld values need room for %lld", n, (long long)capacity);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaMemcpy(out, c->record, n * 8, cudaMemcpyDeviceToHost));
+  c->recorded = 0;
+  return 0;
+}
+
+int fdtd_read_dft(fdtd_ctx *c, double *sums, int64_t count) {
+  if (!c) return FDTD_E_INVALID;
+  if (count != c->nsums)
+    return fail(c, FDTD_E_INVALID, "the transforms hold %lld sums, not %lld", c->nsums, (long long)count);
+  if (c->nsums == 0) return 0;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  std::vector<double> tmp(2 * c->nsums);
+  CUDA_TRY(c, cudaMemcpy(tmp.data(), c->sums, c->nsums * 16, cudaMemcpyDeviceToHost));
+  for (long long q = 0; q < 2 * c->nsums; q++) sums[q] += tmp[q];
+  CUDA_TRY(c, cudaMemset(c->sums, 0, c->nsums * 16));
+  return 0;
+}
+
+int fdtd_device_fields(fdtd_ctx *c, void **e, void **h) {
+  if (!c) return FDTD_E_INVALID;
+  if (e) *e = c->e[c->parity];
+  if (h) *h = c->h[c->parity];
+  return 0;
+}
+
+void *fdtd_stream(fdtd_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int fdtd_profile(fdtd_ctx *c, int32_t on) {
+  if (!c) return FDTD_E_INVALID;
+  c->profiling = on != 0;
+  c->events_used = 0;
+  return 0;
+}
+
+int fdtd_profile_read(fdtd_ctx *c, double *ms, int64_t *launches) {
+  if (!c) return FDTD_E_INVALID;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  double total = 0.0;
+  for (size_t q = 0; q + 1 < c->events_used; q += 2) {
+    float t = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&t, c->events[q], c->events[q + 1]));
+    total += t;
+  }
+  if (ms) *ms = total;
+  if (launches) *launches = (int64_t)(c->events_used / 2);
+  return 0;
+}
+int64_t fdtd_launches(const fdtd_ctx *c) { return c ? c->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,1170 @@
+// The host side of the B200 FDTD engine: photonoxide's `Simulation` (src/fdtd.rs:469-1590),
+// building on the CPU what the reference builds (the averaged permittivity, the time step, the
+// walls, the CPML's tables, conductivity, media, sources and monitors) and stepping on the device
+// through the engine's C ABI (photonoxide_fdtd.h). Compiled without floating-point contraction,
+// so every table is the reference's bits.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "photonoxide_fdtd.h"
+#include "photonoxide_sim.h"
+#include "portable.h"
+
+namespace {
+
+constexpr double kTau = 6.283185307179586476925286766559;
+constexpr double kPi = 3.141592653589793238462643383279;
+
+inline int first_of(int c) { return (c + 1) % 3; }
+inline int second_of(int c) { return (c + 2) % 3; }
+
+struct Grid {  // Grid3d (src/fdfd/three.rs:70-157)
+  int64_t n[3];
+  double d[3], o[3];
+  int64_t cells() const { return n[0] * n[1] * n[2]; }
+  double node(int a, int64_t m) const { return o[a] + (double)m * d[a]; }
+  void e_position(int c, int64_t r, double p[3]) const {
+    int64_t i = r % n[0], j = (r / n[0]) % n[1], k = r / (n[0] * n[1]);
+    p[0] = node(0, i);
+    p[1] = node(1, j);
+    p[2] = node(2, k);
+    p[c] += 0.5 * d[c];
+  }
+};
+
+struct Geometry {
+  double background = 1.0;
+  std::vector<double> boxes;  // 7 per box
+  explicit Geometry(const pxs_geometry *g) {
+    if (!g) return;
+    background = g->background;
+    boxes.assign(g->boxes, g->boxes + 7 * (size_t)g->nboxes);
+  }
+  size_t count() const { return boxes.size() / 7; }
+  double at(const double p[3]) const {
+    double v = background;
+    for (size_t b = 0; b < count(); b++) {
+      const double *x = &boxes[7 * b];
+      if (x[0] < p[0] && p[0] < x[1] && x[2] < p[1] && p[1] < x[3] && x[4] < p[2] && p[2] < x[5])
+        v = x[6];
+    }
+    return v;
+  }
+};
+
+// The cell average of one value (src/fdfd/three.rs:563-588), in num-complex's arithmetic on a
+// zero imaginary part: 1/eps = eps/(eps eps), n/inverse = n inverse/(inverse inverse).
+double average_cell(const Geometry &geo, const double centre[3], const double h[3], int along) {
+  const int samples = 8;
+  const double n = 8.0;
+  int a = along, b = first_of(along), c = second_of(along);
+  double sum = 0.0, p[3] = {centre[0], centre[1], centre[2]};
+  for (int sb = 0; sb < samples; sb++) {
+    p[b] = centre[b] + (((double)sb + 0.5) / n - 0.5) * h[b];
+    for (int sc = 0; sc < samples; sc++) {
+      p[c] = centre[c] + (((double)sc + 0.5) / n - 0.5) * h[c];
+      double inverse = 0.0;
+      for (int sa = 0; sa < samples; sa++) {
+        p[a] = centre[a] + (((double)sa + 0.5) / n - 0.5) * h[a];
+        double e = geo.at(p);
+        inverse += (1.0 * e) / (e * e);
+      }
+      sum += (n * inverse) / (inverse * inverse);
+    }
+  }
+  return sum / (n * n);
+}
+
+// The same average of a uniform value: what every cell away from the boxes' faces gives.
+double average_uniform(double e) {
+  const double n = 8.0;
+  double sum = 0.0;
+  for (int q = 0; q < 64; q++) {
+    double inverse = 0.0;
+    for (int s = 0; s < 8; s++) inverse += (1.0 * e) / (e * e);
+    sum += (n * inverse) / (inverse * inverse);
+  }
+  return sum / (n * n);
+}
+
+// Whether every sample of the cell around `centre` sees the same boxes: along each axis the
+// samples run from centre + offset(0) h to centre + offset(7) h, and a box holds all of them or
+// none when, on some axis, both ends are outside on the same side, or on every axis both are in.
+bool uniform_cell(const Geometry &geo, const double centre[3], const double h[3], double *value) {
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; a++) {
+    lo[a] = centre[a] + ((0.0 + 0.5) / 8.0 - 0.5) * h[a];
+    hi[a] = centre[a] + ((7.0 + 0.5) / 8.0 - 0.5) * h[a];
+  }
+  double v = geo.background;
+  for (size_t b = 0; b < geo.count(); b++) {
+    const double *x = &geo.boxes[7 * b];
+    bool none = false, all = true;
+    for (int a = 0; a < 3; a++) {
+      double blo = x[2 * a], bhi = x[2 * a + 1];
+      bool lo_in = blo < lo[a] && lo[a] < bhi, hi_in = blo < hi[a] && hi[a] < bhi;
+      if (!(lo_in && hi_in)) all = false;
+      if ((hi[a] <= blo) || (lo[a] >= bhi)) none = true;  // both ends on one side, outside
+      else if (!(lo_in && hi_in)) {
+        // the box's face crosses the samples along this axis: the samples differ unless another
+        // axis puts them all outside
+      }
+    }
+    if (none) continue;
+    if (!all) return false;
+    v = x[6];
+  }
+  *value = v;
+  return true;
+}
+
+struct SlabInfo {
+  int field, comp, axis;
+  int64_t from, count;
+  std::vector<double> b, a;
+};
+
+struct Series {
+  int field, comp;
+  int64_t lo[3], len[3];
+  int monitor;  // index into the engine's monitor list
+  std::vector<double> sums;  // complex interleaved, f major then k, j, i
+  int64_t volume() const { return len[0] * len[1] * len[2]; }
+};
+
+struct FluxFace {
+  int axis;
+  int64_t plane;
+  int64_t win[2][2];
+  double sign;
+  size_t series0;  // its 4 series: E b, E c, H b, H c
+};
+
+struct Monitor {
+  std::vector<double> freqs;
+  std::vector<size_t> series;
+};
+
+struct Probe {
+  int field, comp;
+  int64_t r;
+  std::vector<double> values;
+};
+
+struct MediaGroup {
+  std::vector<int32_t> comp;
+  std::vector<int64_t> r;
+  std::vector<double> scale;
+  double chi;
+  std::vector<double> poles;  // alpha, xi, gamma per pole
+};
+
+int set_error(std::string *where, int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (where) *where = buf;
+  return code;
+}
+
+// The medium's stability (src/fdtd/media.rs:261-309, 460-513): the largest |z| among the roots of
+// the update's characteristic polynomial for (K dt)^2 from 0 to its grid's largest, by Aberth's
+// iteration.
+std::vector<double> poly_multiply(const std::vector<double> &a, const std::vector<double> &b) {
+  std::vector<double> out(a.size() + b.size() - 1, 0.0);
+  for (size_t i = 0; i < a.size(); i++)
+    for (size_t j = 0; j < b.size(); j++) out[i + j] += a[i] * b[j];
+  return out;
+}
+double largest_root(std::vector<double> p) {
+  while (p.size() > 1 && p.back() == 0.0) p.pop_back();
+  size_t n = p.size() - 1;
+  if (n == 0) return 0.0;
+  double lead = p[n];
+  for (double &c : p) c /= lead;
+  double radius = std::max(std::pow(std::fabs(p[0]), 1.0 / (double)n), 1e-3);
+  std::vector<double> zr(n), zi(n);
+  for (size_t k = 0; k < n; k++) {
+    double ang = kTau * ((double)k + 0.25) / (double)n;
+    zr[k] = radius * std::cos(ang);
+    zi[k] = radius * std::sin(ang);
+  }
+  for (int it = 0; it < 500; it++) {
+    double largest = 0.0;
+    for (size_t k = 0; k < n; k++) {
+      double vr = 0, vi = 0, dr = 0, di = 0;
+      for (size_t q = p.size(); q-- > 0;) {
+        double ndr = dr * zr[k] - di * zi[k] + vr, ndi = dr * zi[k] + di * zr[k] + vi;
+        dr = ndr;
+        di = ndi;
+        double nvr = vr * zr[k] - vi * zi[k] + p[q], nvi = vr * zi[k] + vi * zr[k];
+        vr = nvr;
+        vi = nvi;
+      }
+      if (vr == 0.0 && vi == 0.0) continue;
+      double den = dr * dr + di * di;
+      double rr = (vr * dr + vi * di) / den, ri = (vi * dr - vr * di) / den;
+      double sr = 0, si = 0;
+      for (size_t j = 0; j < n; j++) {
+        if (j == k) continue;
+        double ar = zr[k] - zr[j], ai = zi[k] - zi[j], m = ar * ar + ai * ai;
+        sr += ar / m;
+        si += -ai / m;
+      }
+      double qr = 1.0 - (rr * sr - ri * si), qi = -(rr * si + ri * sr);
+      double qm = qr * qr + qi * qi;
+      double str = (rr * qr + ri * qi) / qm, sti = (ri * qr - rr * qi) / qm;
+      if (std::isfinite(str) && std::isfinite(sti)) {
+        zr[k] -= str;
+        zi[k] -= sti;
+        largest = std::max(largest, std::hypot(str, sti) / std::max(std::hypot(zr[k], zi[k]), 1e-300));
+      }
+    }
+    if (largest < 1e-15) break;
+  }
+  double m = 0.0;
+  for (size_t k = 0; k < n; k++) m = std::max(m, std::hypot(zr[k], zi[k]));
+  return m;
+}
+bool medium_stable(double eps_inf, const std::vector<double> &co, double sigma, double dt,
+                   double top) {
+  size_t np = co.size() / 3;
+  auto product = [&](long skip) {
+    std::vector<double> acc{1.0};
+    for (size_t i = 0; i < np; i++)
+      if ((long)i != skip) acc = poly_multiply(acc, {-co[3 * i + 1], -co[3 * i], 1.0});
+    return acc;
+  };
+  double most = top * dt * dt;
+  for (int i = 1; i <= 200; i++) {
+    double u = most * (double)i / 200.0;
+    double half = sigma * dt / 2.0;
+    std::vector<double> poly = poly_multiply({eps_inf - half, u - 2.0 * eps_inf, eps_inf + half},
+                                             product(-1));
+    for (size_t q = 0; q < np; q++) {
+      double gm = co[3 * q + 2];
+      std::vector<double> term =
+          poly_multiply({gm / 4.0, 0.0, -gm / 2.0, 0.0, gm / 4.0}, product((long)q));
+      for (size_t t = 0; t < poly.size() && t < term.size(); t++) poly[t] += term[t];
+    }
+    if (largest_root(poly) > 1.0 + 1e-6) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+struct pxs_sim {
+  std::string error;
+  Grid g;
+  int kind[3];
+  int64_t low[3], high[3];
+  double cpml[5];
+  int precision;
+  size_t budget;
+  double dt;
+  int64_t steps = 0;
+  bool varies[3];
+  std::vector<double> ca[3], cb[3], kn[3], kh[3];
+  std::vector<SlabInfo> slabs;
+  // host copies of the state; `host_fresh`: they hold the latest (the device's is stale)
+  std::vector<double> e, h;
+  std::vector<std::vector<double>> psi;
+  bool host_fresh = true;
+  bool device_fresh = false;
+  // sources, in CPU order: point sources first (src/fdtd.rs:1348-1359), then currents
+  std::vector<fdtd_waveform> waves;
+  std::vector<fdtd_injection> points, currents;
+  std::vector<Probe> probes;
+  std::vector<Monitor> monitors;
+  std::vector<Series> series;
+  std::vector<int> dft_monitor;  // add_dft's monitors, by number
+  std::vector<std::vector<FluxFace>> fluxes;
+  std::vector<MediaGroup> groups;
+  std::map<std::pair<int, int64_t>, int> members;
+  bool configured = false;  // sources, probes and transforms pushed to the engine
+  fdtd_ctx *ctx = nullptr;
+
+  int64_t N() const { return g.cells(); }
+  bool periodic(int a) const { return kind[a] == 1; }
+  int fail(int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    error = buf;
+    return code;
+  }
+  bool inside(int64_t i, int64_t j, int64_t k) const {
+    return i >= 0 && j >= 0 && k >= 0 && i < g.n[0] && j < g.n[1] && k < g.n[2];
+  }
+  int64_t index(int64_t i, int64_t j, int64_t k) const { return (k * g.n[1] + j) * g.n[0] + i; }
+
+  // Simulation::build_cpml (src/fdtd.rs:799-869)
+  void build_cpml() {
+    double R = cpml[0], sig = cpml[1], order = cpml[2], kmax = cpml[3], alpha = cpml[4];
+    for (int axis = 0; axis < 3; axis++) {
+      kn[axis].assign(g.n[axis], 1.0);
+      kh[axis].assign(g.n[axis], 1.0);
+      if (periodic(axis)) continue;
+      int64_t lo = low[axis], hi = high[axis], n = g.n[axis];
+      double hstep = g.d[axis];
+      auto profile = [&](double depth, int64_t cells, double &s, double &k) {
+        double d = (double)cells * hstep;
+        double x = std::pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
+        double smax = std::isnan(sig) ? (order + 1.0) * (-std::log(R)) / (2.0 * d) : sig;
+        s = smax * x;
+        k = 1.0 + (kmax - 1.0) * x;
+      };
+      auto at = [&](double pos, double &s, double &k) {
+        if (lo > 0 && pos < (double)lo) profile((double)lo - pos, lo, s, k);
+        else if (hi > 0 && pos > (double)(n - hi)) profile(pos - (double)(n - hi), hi, s, k);
+        else { s = 0.0; k = 1.0; }
+      };
+      for (int64_t m = 0; m < n; m++) {
+        double s, k;
+        at((double)m, s, k);
+        kn[axis][m] = 1.0 / k;
+        at((double)m + 0.5, s, k);
+        kh[axis][m] = 1.0 / k;
+      }
+      int64_t froms[2] = {0, n - hi}, counts[2] = {lo, hi};
+      for (int side = 0; side < 2; side++) {
+        if (counts[side] == 0) continue;
+        for (int field = 0; field < 2; field++) {
+          SlabInfo sl;
+          sl.field = field;
+          sl.axis = axis;
+          sl.from = froms[side];
+          sl.count = counts[side];
+          for (int64_t m = sl.from; m < sl.from + sl.count; m++) {
+            double s, k;
+            at((double)m + (field == 0 ? 0.0 : 0.5), s, k);
+            double b = pxp::exp(-(s / k + alpha) * dt);
+            double den = s * k + k * k * alpha;
+            sl.b.push_back(b);
+            sl.a.push_back((s > 0.0 && den > 0.0) ? s * (b - 1.0) / den : 0.0);
+          }
+          for (int comp : {first_of(axis), second_of(axis)}) {
+            sl.comp = comp;
+            slabs.push_back(sl);
+          }
+        }
+      }
+    }
+  }
+
+  // Brings the host's copies up to date with the device's.
+  int pull() {
+    if (host_fresh || !ctx) return 0;
+    e.resize(3 * N());
+    h.resize(3 * N());
+    std::vector<double *> ps;
+    for (auto &p : psi) ps.push_back(p.data());
+    if (int r = fdtd_download_fields(ctx, e.data(), h.data(), ps.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    host_fresh = true;
+    return 0;
+  }
+
+  // Adds the device's transform sums into the host's.
+  int pull_sums() {
+    if (!ctx || !configured || series.empty()) return 0;
+    int64_t total = 0;
+    for (auto &s : series) total += (int64_t)s.sums.size() / 2;
+    std::vector<double> add(2 * total, 0.0);
+    if (int r = fdtd_read_dft(ctx, add.data(), total)) return fail(r, "%s", fdtd_last_error(ctx));
+    int64_t at = 0;
+    for (auto &s : series)
+      for (size_t q = 0; q < s.sums.size(); q++) s.sums[q] += add[at++];
+    return 0;
+  }
+
+  // Something changed that the engine holds: its transforms are read out first.
+  int reconfigure() {
+    if (int r = pull_sums()) return r;
+    configured = false;
+    return 0;
+  }
+
+  int ensure_engine() {
+    if (ctx) return 0;
+    fdtd_grid gr;
+    for (int a = 0; a < 3; a++) {
+      gr.n[a] = g.n[a];
+      gr.periodic[a] = periodic(a) ? 1 : 0;
+      gr.low[a] = periodic(a) ? 0 : low[a];
+      gr.high[a] = periodic(a) ? 0 : high[a];
+    }
+    std::vector<double> fe, fh;
+    for (int a = 0; a < 3; a++)  // build_stencils (src/fdtd.rs:1552-1569): kappa/h
+      for (int64_t m = 0; m < g.n[a]; m++) {
+        fe.push_back(kn[a][m] / g.d[a]);
+        fh.push_back(kh[a][m] / g.d[a]);
+      }
+    std::vector<fdtd_slab> sl;
+    for (auto &s : slabs)
+      sl.push_back(fdtd_slab{s.field, s.comp, s.axis, s.from, s.count, s.b.data(), s.a.data()});
+    fdtd_ctx *c = nullptr;
+    int r = fdtd_create(&gr, dt, g.d, fe.data(), fh.data(), sl.data(), (int32_t)sl.size(),
+                        precision, budget, &c);
+    if (r) {
+      fail(r, "%s", c ? fdtd_last_error(c) : "the engine could not start");
+      fdtd_destroy(c);
+      return r;
+    }
+    ctx = c;
+    if (int q = push_coefficients()) return q;
+    if (!groups.empty()) {
+      std::vector<fdtd_media_group> mg;
+      for (auto &G : groups)
+        mg.push_back(fdtd_media_group{(int64_t)G.comp.size(), G.comp.data(), G.r.data(),
+                                      G.scale.data(), G.chi, (int32_t)(G.poles.size() / 3),
+                                      G.poles.data()});
+      if (int q = fdtd_set_media(ctx, (int32_t)mg.size(), mg.data()))
+        return fail(q, "%s", fdtd_last_error(ctx));
+    }
+    device_fresh = false;
+    return 0;
+  }
+
+  int push_coefficients() {
+    bool lossless = true;
+    for (int c = 0; c < 3 && lossless; c++)
+      for (int64_t r = 0; r < N(); r++) {
+        double want = cb[c][r] == 0.0 ? 0.0 : 1.0;
+        if (ca[c][r] != want) { lossless = false; break; }
+      }
+    std::vector<double> a, b;
+    for (int c = 0; c < 3; c++) {
+      b.insert(b.end(), cb[c].begin(), cb[c].end());
+      if (!lossless) a.insert(a.end(), ca[c].begin(), ca[c].end());
+    }
+    if (int r = fdtd_upload_coeffs(ctx, lossless ? nullptr : a.data(), b.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    return 0;
+  }
+
+  int configure() {
+    if (configured) return 0;
+    std::vector<fdtd_injection> inj(points);
+    inj.insert(inj.end(), currents.begin(), currents.end());
+    if (int r = fdtd_set_sources(ctx, (int32_t)waves.size(), waves.data(), (int64_t)inj.size(),
+                                 inj.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    std::vector<int32_t> pf, pc;
+    std::vector<int64_t> pr;
+    for (auto &p : probes) {
+      pf.push_back(p.field);
+      pc.push_back(p.comp);
+      pr.push_back(p.r);
+    }
+    if (int r = fdtd_set_probes(ctx, (int32_t)probes.size(), pf.data(), pc.data(), pr.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    std::vector<fdtd_series> fs;
+    for (auto &s : series) {
+      fdtd_series x;
+      x.field = s.field;
+      x.component = s.comp;
+      for (int a = 0; a < 3; a++) {
+        x.lo[a] = s.lo[a];
+        x.len[a] = s.len[a];
+      }
+      x.monitor = s.monitor;
+      fs.push_back(x);
+    }
+    std::vector<int32_t> per;
+    std::vector<double> fr;
+    for (auto &m : monitors) {
+      per.push_back((int32_t)m.freqs.size());
+      fr.insert(fr.end(), m.freqs.begin(), m.freqs.end());
+    }
+    if (int r = fdtd_set_dft(ctx, (int32_t)fs.size(), fs.data(), (int32_t)per.size(), per.data(),
+                             fr.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    configured = true;
+    return 0;
+  }
+
+  int push_fields() {
+    if (device_fresh) return 0;
+    std::vector<const double *> ps;
+    for (auto &p : psi) ps.push_back(p.empty() ? nullptr : p.data());
+    if (int r = fdtd_upload_fields(ctx, e.empty() ? nullptr : e.data(),
+                                   h.empty() ? nullptr : h.data(), ps.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    device_fresh = true;
+    return 0;
+  }
+
+  int run(int64_t count) {
+    if (count <= 0) return 0;
+    if (int r = ensure_engine()) return r;
+    if (int r = configure()) return r;
+    if (int r = push_fields()) return r;
+    if (int r = fdtd_run(ctx, count, steps)) return fail(r, "%s", fdtd_last_error(ctx));
+    host_fresh = false;
+    steps += count;
+    if (!probes.empty()) {
+      int64_t got = 0;
+      fdtd_read_probes(ctx, nullptr, 0, &got);
+      std::vector<double> rec(got * probes.size());
+      if (int r = fdtd_read_probes(ctx, rec.data(), (int64_t)rec.size(), &got))
+        return fail(r, "%s", fdtd_last_error(ctx));
+      for (int64_t m = 0; m < got; m++)
+        for (size_t p = 0; p < probes.size(); p++)
+          probes[p].values.push_back(rec[m * probes.size() + p]);
+    }
+    return 0;
+  }
+
+  bool value(size_t s0, size_t s1, int field, int comp, const int64_t at[3], int f, double *re,
+             double *im) const {
+    for (size_t q = s0; q < s1; q++) {
+      const Series &s = series[q];
+      if (s.field != field || s.comp != comp) continue;
+      bool in = true;
+      for (int a = 0; a < 3; a++)
+        if (at[a] < s.lo[a] || at[a] >= s.lo[a] + s.len[a]) in = false;
+      if (!in) continue;
+      int64_t o = ((at[2] - s.lo[2]) * s.len[1] + (at[1] - s.lo[1])) * s.len[0] + at[0] - s.lo[0];
+      *re = s.sums[2 * (f * s.volume() + o)];
+      *im = s.sums[2 * (f * s.volume() + o) + 1];
+      return true;
+    }
+    return false;
+  }
+
+  // FluxPlane::flux (src/fdtd/monitors.rs:320-351)
+  double face_flux(const FluxFace &F, int f) const {
+    int b = first_of(F.axis), c = second_of(F.axis);
+    auto lo_of = [&](int along) {
+      int sl = along == b ? 0 : 1;
+      return F.win[sl][0] < 0 ? (int64_t)0 : F.win[sl][0];
+    };
+    auto hi_of = [&](int along) {
+      int sl = along == b ? 0 : 1;
+      return F.win[sl][0] < 0 ? g.n[along] : F.win[sl][1] + 1;
+    };
+    auto weight = [&](int along, int64_t m, bool half) {
+      int sl = along == b ? 0 : 1;
+      if (F.win[sl][0] < 0) return 1.0;
+      int64_t lo = F.win[sl][0], hi = F.win[sl][1];
+      if (half) return (lo < m && m < hi) ? 1.0 : ((m == lo || m == hi) ? 0.5 : 0.0);
+      return (lo < m && m <= hi) ? 1.0 : 0.0;
+    };
+    double total = 0.0;
+    const int comps[2] = {b, c}, hs[2] = {c, b};
+    const double signs[2] = {0.5, -0.5};
+    for (int t = 0; t < 2; t++) {
+      for (int64_t v = lo_of(c); v < hi_of(c); v++)
+        for (int64_t u = lo_of(b); u < hi_of(b); u++) {
+          double w = weight(b, u, comps[t] == b) * weight(c, v, comps[t] == c);
+          if (w == 0.0) continue;
+          int64_t at[3];
+          at[F.axis] = F.plane;
+          at[b] = u;
+          at[c] = v;
+          double lr, li, hr, hi2, er, ei;
+          value(F.series0, F.series0 + 4, 0, comps[t], at, f, &lr, &li);
+          value(F.series0, F.series0 + 4, 1, hs[t], at, f, &hr, &hi2);
+          at[F.axis] = F.plane + 1;
+          value(F.series0, F.series0 + 4, 0, comps[t], at, f, &er, &ei);
+          double mr = 0.5 * (lr + er), mi = 0.5 * (li + ei);
+          // (m * conj(h)).re as num-complex: mr hr - mi (-hi)
+          double re = mr * hr - mi * (-hi2);
+          total += w * signs[t] * re;
+        }
+    }
+    return total * g.d[b] * g.d[c];
+  }
+
+  int check_frequencies(int nf, const double *freqs) {
+    if (nf <= 0) return fail(FDTD_E_INVALID, "a monitor needs at least one frequency");
+    for (int f = 0; f < nf; f++)
+      if (!(freqs[f] > 0.0 && kTau * freqs[f] * dt < kPi))
+        return fail(FDTD_E_INVALID, "%g c/um is beyond the time step's Nyquist frequency", freqs[f]);
+    return 0;
+  }
+
+  void add_plane_series(FluxFace &F, int monitor, int nf) {
+    int b = first_of(F.axis), c = second_of(F.axis);
+    F.series0 = series.size();
+    for (int field = 0; field < 2; field++)
+      for (int comp : {b, c}) {
+        Series s;
+        s.field = field;
+        s.comp = comp;
+        s.monitor = monitor;
+        s.lo[F.axis] = F.plane;
+        s.len[F.axis] = field == 0 ? 2 : 1;
+        for (int al : {b, c}) {
+          int sl = al == b ? 0 : 1;
+          s.lo[al] = F.win[sl][0] < 0 ? 0 : F.win[sl][0];
+          s.len[al] = (F.win[sl][0] < 0 ? g.n[al] : F.win[sl][1] + 1) - s.lo[al];
+        }
+        s.sums.assign(2 * s.volume() * nf, 0.0);
+        monitors[monitor].series.push_back(series.size());
+        series.push_back(s);
+      }
+  }
+};
+
+extern "C" {
+
+int pxs_average(const int64_t n[3], const double d[3], const double o[3], const pxs_geometry *gm,
+                double *out) {
+  Grid g{{n[0], n[1], n[2]}, {d[0], d[1], d[2]}, {o[0], o[1], o[2]}};
+  Geometry geo(gm);
+  int64_t N = g.cells();
+  std::vector<unsigned char> uniform(3 * N, 0);
+  for (int c = 0; c < 3; c++) {
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t r = 0; r < N; r++) {
+      double p[3], v;
+      g.e_position(c, r, p);
+      if (uniform_cell(geo, p, g.d, &v)) {
+        uniform[c * N + r] = 1;
+        out[c * N + r] = v;
+      } else {
+        out[c * N + r] = average_cell(geo, p, g.d, c);
+      }
+    }
+  }
+  // a uniform cell's average is a function of its value alone: taken once per value
+  std::vector<std::pair<double, double>> seen;
+  for (int64_t q = 0; q < 3 * N; q++) {
+    if (!uniform[q]) continue;
+    double v = out[q], a = 0.0;
+    bool found = false;
+    for (auto &pr : seen)
+      if (pr.first == v) { a = pr.second; found = true; break; }
+    if (!found) {
+      a = average_uniform(v);
+      seen.push_back({v, a});
+    }
+    out[q] = a;
+  }
+  return 0;
+}
+
+pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], const int32_t kind[3],
+                    const int64_t low[3], const int64_t high[3], const double cpml[5],
+                    double courant, const double *eps, const pxs_geometry *geometry,
+                    int32_t precision, size_t hbm_budget, char *err, int32_t errlen) {
+  std::string msg;
+  auto refuse = [&](const char *fmt, auto... args) -> pxs_sim * {
+    set_error(&msg, FDTD_E_INVALID, fmt, args...);
+    if (err && errlen > 0) snprintf(err, errlen, "%s", msg.c_str());
+    return nullptr;
+  };
+  auto ok = [](double v) { return std::isfinite(v) && v > 0.0; };
+  // the checks of with_permittivity (src/fdtd.rs:686-724)
+  if (n[0] <= 0 || n[1] <= 0 || n[2] <= 0 || !ok(d[0]) || !ok(d[1]) || !ok(d[2]))
+    return refuse("the grid needs cells and positive steps");
+  if (!(cpml[0] > 0.0 && cpml[0] < 1.0) || !(std::isfinite(cpml[2]) && cpml[2] >= 0.0) ||
+      !(std::isfinite(cpml[3]) && cpml[3] >= 1.0) || !(std::isfinite(cpml[4]) && cpml[4] >= 0.0) ||
+      (!std::isnan(cpml[1]) && !(std::isfinite(cpml[1]) && cpml[1] >= 0.0)))
+    return refuse("the CPML needs R in (0, 1), an order >= 0, kappa >= 1, alpha >= 0 and sigma >= 0");
+  for (int a = 0; a < 3; a++)
+    if (kind[a] == 0 && (low[a] < 0 || high[a] < 0 || low[a] + high[a] >= n[a]))
+      return refuse("CPMLs of %lld and %lld cells leave nothing of %lld cells", (long long)low[a],
+                    (long long)high[a], (long long)n[a]);
+  if (!(courant > 0.0 && courant <= 1.0))
+    return refuse("the Courant number must be in (0, 1], got %g", courant);
+  pxs_sim *s = new pxs_sim();
+  s->g = Grid{{n[0], n[1], n[2]}, {d[0], d[1], d[2]}, {o[0], o[1], o[2]}};
+  for (int a = 0; a < 3; a++) {
+    s->kind[a] = kind[a];
+    s->low[a] = kind[a] == 0 ? low[a] : 0;
+    s->high[a] = kind[a] == 0 ? high[a] : 0;
+    s->varies[a] = !(n[a] == 1 && kind[a] == 1);
+  }
+  for (int q = 0; q < 5; q++) s->cpml[q] = cpml[q];
+  s->precision = precision == 64 ? 64 : 32;
+  s->budget = hbm_budget;
+  // Delta t = C / sqrt(sum 1/d^2) over the axes the field varies along (bloch::curl_bound,
+  // src/fdtd/bloch.rs:31-43, with k = 0)
+  double sum = 0.0;
+  for (int a = 0; a < 3; a++)
+    if (s->varies[a]) sum += 1.0 / (d[a] * d[a]);
+  if (sum == 0.0) {
+    delete s;
+    return refuse("the field varies along no axis");
+  }
+  s->dt = courant / std::sqrt(sum);
+  int64_t N = s->N();
+  std::vector<double> avg;
+  if (!eps) {
+    avg.resize(3 * N);
+    pxs_average(n, d, o, geometry, avg.data());
+    eps = avg.data();
+  }
+  for (int c = 0; c < 3; c++) {
+    s->ca[c].assign(N, 1.0);
+    s->cb[c].resize(N);
+    for (int64_t r = 0; r < N; r++) {
+      double v = eps[c * N + r];
+      if (!(std::isfinite(v) && v > 0.0)) {
+        delete s;
+        return refuse("the permittivity must be finite and positive, got %g", v);
+      }
+      s->cb[c][r] = s->dt / v;
+    }
+  }
+  // walls: E tangential to a wall is zero on its node 0 (src/fdtd.rs:738-756)
+  for (int c = 0; c < 3; c++)
+    for (int a = 0; a < 3; a++) {
+      if (a == c || s->periodic(a)) continue;
+      int64_t stride = a == 0 ? 1 : (a == 1 ? n[0] : n[0] * n[1]);
+      for (int64_t r = 0; r < N; r++)
+        if ((r / stride) % n[a] == 0) s->ca[c][r] = s->cb[c][r] = 0.0;
+    }
+  s->build_cpml();
+  s->psi.resize(s->slabs.size());
+  return s;
+}
+
+void pxs_destroy(pxs_sim *s) {
+  if (!s) return;
+  fdtd_destroy(s->ctx);
+  delete s;
+}
+
+const char *pxs_last_error(const pxs_sim *s) { return s ? s->error.c_str() : "no simulation"; }
+
+int pxs_conductivity(pxs_sim *s, const double *sigma, const pxs_geometry *geometry) {
+  if (!s->groups.empty())
+    return s->fail(FDTD_E_INVALID,
+                   "the conductivity comes before the dispersive media: with_conductivity, then "
+                   "with_medium");
+  Geometry geo(geometry);
+  int64_t N = s->N();
+  for (int c = 0; c < 3; c++)
+    for (int64_t r = 0; r < N; r++) {
+      if (s->cb[c][r] == 0.0) continue;
+      double sg;
+      if (sigma) sg = sigma[c * N + r];
+      else {
+        double p[3];
+        s->g.e_position(c, r, p);
+        sg = geo.at(p);
+      }
+      if (!(std::isfinite(sg) && sg >= 0.0))
+        return s->fail(FDTD_E_INVALID, "the conductivity must be finite and >= 0, got %g", sg);
+      double half = sg * s->cb[c][r] / 2.0;
+      s->ca[c][r] = (1.0 - half) / (1.0 + half);
+      s->cb[c][r] /= 1.0 + half;
+    }
+  if (s->ctx) return s->push_coefficients();
+  return 0;
+}
+
+int pxs_conductor(pxs_sim *s, int32_t comp, int64_t i, int64_t j, int64_t k) {
+  if (comp < 0 || comp > 2 || !s->inside(i, j, k))
+    return s->fail(FDTD_E_INVALID, "(%lld, %lld, %lld) is outside the grid", (long long)i,
+                   (long long)j, (long long)k);
+  if (int r = s->pull()) return r;
+  int64_t r = s->index(i, j, k);
+  s->ca[comp][r] = s->cb[comp][r] = 0.0;
+  if (!s->e.empty()) s->e[comp * s->N() + r] = 0.0;
+  auto it = s->members.find({comp, r});
+  if (it != s->members.end()) {  // Media::remove (src/fdtd/media.rs:641-653)
+    MediaGroup &G = s->groups[it->second];
+    for (size_t v = 0; v < G.r.size(); v++)
+      if (G.comp[v] == comp && G.r[v] == r) {
+        G.comp.erase(G.comp.begin() + v);
+        G.r.erase(G.r.begin() + v);
+        G.scale.erase(G.scale.begin() + v);
+        break;
+      }
+    s->members.erase(it);
+  }
+  if (s->ctx) {
+    s->device_fresh = false;
+    return s->push_coefficients();
+  }
+  return 0;
+}
+
+int pxs_medium(pxs_sim *s, double eps_inf, int32_t npoles, const double *poles,
+               const uint8_t *inside, const pxs_geometry *geometry) {
+  // Simulation::medium (src/fdtd/media.rs:749-825), with its stability check
+  if (!(std::isfinite(eps_inf) && eps_inf > 0.0))
+    return s->fail(FDTD_E_INVALID, "a dispersive medium's eps_inf must be positive and finite");
+  if (s->steps > 0 || s->ctx)
+    return s->fail(FDTD_E_INVALID, "a dispersive medium goes in before the run starts");
+  double dt = s->dt;
+  std::vector<double> co;
+  double gsum = 0.0;
+  for (int p = 0; p < npoles; p++) {  // Pole::parts / coefficients (media.rs:74-109)
+    const double *x = poles + 4 * p;
+    double a, w0sq, gamma;
+    if ((int)x[0] == 0) {
+      double w0 = kTau * x[2];
+      a = x[1] * w0 * w0;
+      w0sq = w0 * w0;
+      gamma = kTau * x[3];
+    } else {
+      double wp = kTau * x[1];
+      a = wp * wp;
+      w0sq = 0.0;
+      gamma = kTau * x[2];
+    }
+    double dd = 1.0 + gamma * dt / 2.0;
+    co.push_back((2.0 - w0sq * dt * dt) / dd);
+    co.push_back((gamma * dt / 2.0 - 1.0) / dd);
+    co.push_back(a * dt * dt / dd);
+    gsum += co.back();
+  }
+  double chi = gsum / (4.0 * dt);
+  Geometry geo(geometry);
+  int64_t N = s->N();
+  {
+    double top = 0.0, largest = 0.0;
+    for (int a = 0; a < 3; a++)
+      if (s->varies[a]) top += 1.0 / (s->g.d[a] * s->g.d[a]);
+    top *= 4.0;
+    for (int c = 0; c < 3; c++)
+      for (int64_t r = 0; r < N; r++) {
+        if (s->cb[c][r] == 0.0) continue;
+        bool in;
+        if (inside) in = inside[c * N + r] != 0;
+        else {
+          double p[3];
+          s->g.e_position(c, r, p);
+          in = geo.at(p) != 0.0;
+        }
+        if (!in) continue;
+        auto it = s->members.find({c, r});
+        double old_chi = it != s->members.end() ? s->groups[it->second].chi : 0.0;
+        largest = std::max(largest, (1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi);
+      }
+    for (double sg : {0.0, largest})
+      if (!medium_stable(eps_inf, co, sg, dt, top))
+        return s->fail(FDTD_E_INVALID,
+                       "the medium isn't stable at the time step %g um/c (a term's w0 dt above 2, "
+                       "or a Courant number above sqrt(eps_inf)): take a smaller step", dt);
+  }
+  MediaGroup G;
+  G.chi = chi;
+  G.poles = co;
+  for (int c = 0; c < 3; c++)
+    for (int64_t r = 0; r < N; r++) {
+      if (s->cb[c][r] == 0.0) continue;
+      bool in;
+      if (inside) in = inside[c * N + r] != 0;
+      else {
+        double p[3];
+        s->g.e_position(c, r, p);
+        in = geo.at(p) != 0.0;
+      }
+      if (!in) continue;
+      double old_chi = 0.0;
+      auto it = s->members.find({c, r});
+      if (it != s->members.end()) old_chi = s->groups[it->second].chi;
+      double sg = std::max((1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi, 0.0);
+      if (it != s->members.end()) {
+        MediaGroup &O = s->groups[it->second];
+        for (size_t v = 0; v < O.r.size(); v++)
+          if (O.comp[v] == c && O.r[v] == r) {
+            O.comp.erase(O.comp.begin() + v);
+            O.r.erase(O.r.begin() + v);
+            O.scale.erase(O.scale.begin() + v);
+            break;
+          }
+        s->members.erase(it);
+      }
+      double nu = 1.0 + dt / eps_inf * (sg / 2.0 + chi);
+      s->ca[c][r] = (1.0 - dt * sg / (2.0 * eps_inf)) / nu;
+      s->cb[c][r] = dt / eps_inf / nu;
+      G.comp.push_back(c);
+      G.r.push_back(r);
+      G.scale.push_back(s->cb[c][r]);
+    }
+  if (npoles > 0 && !G.r.empty()) {
+    int gi = (int)s->groups.size();
+    (void)0;
+    for (size_t v = 0; v < G.r.size(); v++) s->members[{G.comp[v], G.r[v]}] = gi;
+    s->groups.push_back(G);
+  }
+  return 0;
+}
+
+int pxs_add_source(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j, int64_t k,
+                   const double wave[6]) {
+  if (!s->inside(i, j, k) || comp < 0 || comp > 2 || field < 0 || field > 1)
+    return s->fail(FDTD_E_INVALID, "(%lld, %lld, %lld) is outside the %lld x %lld x %lld grid",
+                   (long long)i, (long long)j, (long long)k, (long long)s->g.n[0],
+                   (long long)s->g.n[1], (long long)s->g.n[2]);
+  if (int r = s->reconfigure()) return r;
+  fdtd_waveform w;
+  w.kind = (int32_t)wave[0];
+  for (int q = 0; q < 5; q++) w.p[q] = wave[q + 1];
+  s->waves.push_back(w);
+  s->points.push_back(fdtd_injection{field, comp, s->index(i, j, k), 1.0, 0.0,
+                                     (int32_t)s->waves.size() - 1, 1});
+  return 0;
+}
+
+int pxs_add_current(pxs_sim *s, int32_t field, int64_t count, const int32_t *comps,
+                    const int64_t *at, const double *amps, const double wave[6]) {
+  for (int64_t q = 0; q < count; q++) {  // src/fdtd/sources.rs:223-242
+    const int64_t *p = at + 3 * q;
+    if (!s->inside(p[0], p[1], p[2]) || comps[q] < 0 || comps[q] > 2)
+      return s->fail(FDTD_E_INVALID, "a current's value is outside the grid");
+    if (!std::isfinite(amps[2 * q]) || !std::isfinite(amps[2 * q + 1]))
+      return s->fail(FDTD_E_INVALID, "a current's amplitude must be finite");
+  }
+  if (int r = s->reconfigure()) return r;
+  fdtd_waveform w;
+  w.kind = (int32_t)wave[0];
+  for (int q = 0; q < 5; q++) w.p[q] = wave[q + 1];
+  s->waves.push_back(w);
+  for (int64_t q = 0; q < count; q++) {
+    const int64_t *p = at + 3 * q;
+    s->currents.push_back(fdtd_injection{field, comps[q], s->index(p[0], p[1], p[2]), amps[2 * q],
+                                         amps[2 * q + 1], (int32_t)s->waves.size() - 1, 0});
+  }
+  return 0;
+}
+
+int pxs_add_dipole(pxs_sim *s, int32_t field, int32_t comp, const double pos[3], double are,
+                   double aim, const double wave[6]) {
+  // Simulation::add_dipole (src/fdtd/sources.rs:248-315), no Bloch phase
+  if (!std::isfinite(are) || !std::isfinite(aim) || !std::isfinite(pos[0]) ||
+      !std::isfinite(pos[1]) || !std::isfinite(pos[2]))
+    return s->fail(FDTD_E_INVALID, "a dipole must be finite");
+  int64_t idx[3][2];
+  double wt[3][2], volume = 1.0;
+  for (int axis = 0; axis < 3; axis++) {
+    int64_t n = s->g.n[axis];
+    if (!s->varies[axis]) {
+      idx[axis][0] = idx[axis][1] = 0;
+      wt[axis][0] = 1.0;
+      wt[axis][1] = 0.0;
+      continue;
+    }
+    volume *= s->g.d[axis];
+    bool half = field == 0 ? comp == axis : comp != axis;
+    double first = s->g.node(axis, 0) + (half ? 0.5 * s->g.d[axis] : 0.0);
+    double sp = (pos[axis] - first) / s->g.d[axis];
+    if (!s->periodic(axis) && !(sp >= 0.0 && sp <= (double)(n - 1)))
+      return s->fail(FDTD_E_INVALID, "the dipole is outside its component's values along axis %d",
+                     axis);
+    double m = std::floor(sp), f = sp - m;
+    if (s->periodic(axis)) {
+      int64_t m0 = (int64_t)m;
+      idx[axis][0] = ((m0 % n) + n) % n;
+      idx[axis][1] = (((m0 + 1) % n) + n) % n;
+    } else {
+      idx[axis][0] = (int64_t)m;
+      idx[axis][1] = std::min((int64_t)m + 1, n - 1);
+    }
+    wt[axis][0] = 1.0 - f;
+    wt[axis][1] = f;
+  }
+  std::map<int64_t, std::pair<double, double>> values;
+  for (int p = 0; p < 2; p++)
+    for (int q = 0; q < 2; q++)
+      for (int r = 0; r < 2; r++) {
+        double w = wt[0][p] * wt[1][q] * wt[2][r];
+        if (w == 0.0) continue;
+        double sc = w / volume;
+        auto &acc = values[s->index(idx[0][p], idx[1][q], idx[2][r])];
+        acc.first = acc.first + (are * sc - aim * 0.0);
+        acc.second = acc.second + (are * 0.0 + aim * sc);
+      }
+  if (int r = s->reconfigure()) return r;
+  fdtd_waveform wv;
+  wv.kind = (int32_t)wave[0];
+  for (int q = 0; q < 5; q++) wv.p[q] = wave[q + 1];
+  s->waves.push_back(wv);
+  for (auto &kv : values)
+    s->currents.push_back(fdtd_injection{field, comp, kv.first, kv.second.first, kv.second.second,
+                                         (int32_t)s->waves.size() - 1, 0});
+  return 0;
+}
+
+int pxs_add_probe(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j, int64_t k) {
+  if (!s->inside(i, j, k) || comp < 0 || comp > 2)
+    return s->fail(FDTD_E_INVALID, "(%lld, %lld, %lld) is outside the grid", (long long)i,
+                   (long long)j, (long long)k);
+  if (int r = s->reconfigure()) return r;
+  s->probes.push_back(Probe{field, comp, s->index(i, j, k), {}});
+  return (int)s->probes.size() - 1;
+}
+
+int pxs_add_dft(pxs_sim *s, const int64_t low[3], const int64_t high[3], int32_t nf,
+                const double *freqs) {
+  if (int r = s->check_frequencies(nf, freqs)) return r;
+  for (int a = 0; a < 3; a++)
+    if (low[a] < 0 || high[a] >= s->g.n[a] || low[a] > high[a])
+      return s->fail(FDTD_E_INVALID, "a transform's box must run from low to high indices on the grid");
+  if (int r = s->reconfigure()) return r;
+  Monitor m;
+  m.freqs.assign(freqs, freqs + nf);
+  s->monitors.push_back(m);
+  int mi = (int)s->monitors.size() - 1;
+  for (int field = 0; field < 2; field++)
+    for (int c = 0; c < 3; c++) {
+      Series sr;
+      sr.field = field;
+      sr.comp = c;
+      sr.monitor = mi;
+      for (int a = 0; a < 3; a++) {
+        sr.lo[a] = low[a];
+        sr.len[a] = high[a] - low[a] + 1;
+      }
+      sr.sums.assign(2 * sr.volume() * nf, 0.0);
+      s->monitors[mi].series.push_back(s->series.size());
+      s->series.push_back(sr);
+    }
+  s->dft_monitor.push_back(mi);
+  return (int)s->dft_monitor.size() - 1;
+}
+
+int pxs_add_flux(pxs_sim *s, int32_t axis, int64_t plane, const int64_t window[4], int32_t nf,
+                 const double *freqs) {
+  if (int r = s->check_frequencies(nf, freqs)) return r;
+  if (axis < 0 || axis > 2 || plane < 0 || plane + 1 >= s->g.n[axis])
+    return s->fail(FDTD_E_INVALID, "a flux plane after node %lld needs node %lld on the grid",
+                   (long long)plane, (long long)plane + 1);
+  FluxFace F{axis, plane, {{window[0], window[1]}, {window[2], window[3]}}, 1.0, 0};
+  for (int sl = 0; sl < 2; sl++) {
+    int along = sl == 0 ? first_of(axis) : second_of(axis);
+    if (F.win[sl][0] >= 0 && !(F.win[sl][0] < F.win[sl][1] && F.win[sl][1] < s->g.n[along]))
+      return s->fail(FDTD_E_INVALID, "a flux plane's window must run from one half-plane to a later one on the grid");
+  }
+  if (int r = s->reconfigure()) return r;
+  Monitor m;
+  m.freqs.assign(freqs, freqs + nf);
+  s->monitors.push_back(m);
+  s->add_plane_series(F, (int)s->monitors.size() - 1, nf);
+  s->fluxes.push_back({F});
+  return (int)s->fluxes.size() - 1;
+}
+
+int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const double *freqs) {
+  if (int r = s->check_frequencies(nf, freqs)) return r;
+  std::vector<FluxFace> faces;
+  for (int axis = 0; axis < 3; axis++) {
+    int64_t lo = planes[2 * axis], hi = planes[2 * axis + 1];
+    int b = first_of(axis), c = second_of(axis);
+    if (lo >= hi || lo < 0 || hi + 1 >= s->g.n[axis])
+      return s->fail(FDTD_E_INVALID, "a flux box's planes must be from low to high on the grid");
+    for (int side = 0; side < 2; side++)
+      faces.push_back(FluxFace{axis, side == 0 ? lo : hi,
+                               {{planes[2 * b], planes[2 * b + 1]}, {planes[2 * c], planes[2 * c + 1]}},
+                               side == 0 ? -1.0 : 1.0, 0});
+  }
+  if (int r = s->reconfigure()) return r;
+  for (auto &F : faces) {
+    Monitor m;
+    m.freqs.assign(freqs, freqs + nf);
+    s->monitors.push_back(m);
+    s->add_plane_series(F, (int)s->monitors.size() - 1, nf);
+  }
+  s->fluxes.push_back(faces);
+  return (int)s->fluxes.size() - 1;
+}
+
+int pxs_run(pxs_sim *s, int64_t steps) { return s->run(steps); }
+double pxs_dt(const pxs_sim *s) { return s->dt; }
+int64_t pxs_steps(const pxs_sim *s) { return s->steps; }
+
+int pxs_get_field(pxs_sim *s, int32_t field, int32_t comp, double *out) {
+  if (int r = s->pull()) return r;
+  const std::vector<double> &v = field == 0 ? s->e : s->h;
+  int64_t N = s->N();
+  if (v.empty()) std::fill(out, out + N, 0.0);
+  else std::copy(v.begin() + comp * N, v.begin() + (comp + 1) * N, out);
+  return 0;
+}
+
+int pxs_set_field(pxs_sim *s, int32_t field, int32_t comp, const double *in) {
+  if (int r = s->pull()) return r;
+  std::vector<double> &v = field == 0 ? s->e : s->h;
+  int64_t N = s->N();
+  if (v.empty()) v.assign(3 * N, 0.0);
+  std::copy(in, in + N, v.begin() + comp * N);
+  s->device_fresh = false;
+  return 0;
+}
+
+int64_t pxs_probe(pxs_sim *s, int32_t n, double *out) {
+  if (n < 0 || n >= (int32_t)s->probes.size()) return s->fail(FDTD_E_INVALID, "no probe %d", n);
+  const auto &v = s->probes[n].values;
+  if (out) std::copy(v.begin(), v.end(), out);
+  return (int64_t)v.size();
+}
+
+int64_t pxs_transforms(pxs_sim *s, double *out) {
+  if (int r = s->pull_sums()) return r;
+  int64_t at = 0;
+  // layout order: the transforms (add_dft), then the fluxes' faces (Monitors::all)
+  std::vector<size_t> order;
+  for (int mi : s->dft_monitor)
+    for (size_t q : s->monitors[mi].series) order.push_back(q);
+  for (auto &faces : s->fluxes)
+    for (auto &F : faces)
+      for (size_t q = F.series0; q < F.series0 + 4; q++) order.push_back(q);
+  for (size_t q : order) {
+    const Series &sr = s->series[q];
+    if (out) std::copy(sr.sums.begin(), sr.sums.end(), out + 2 * at);
+    at += (int64_t)sr.sums.size() / 2;
+  }
+  return at;
+}
+
+int pxs_flux(pxs_sim *s, int32_t n, double *out) {
+  if (n < 0 || n >= (int32_t)s->fluxes.size()) return s->fail(FDTD_E_INVALID, "no flux monitor %d", n);
+  if (int r = s->pull_sums()) return r;
+  const auto &faces = s->fluxes[n];
+  int nf = (int)(s->series[faces[0].series0].sums.size() / 2 / s->series[faces[0].series0].volume());
+  for (int f = 0; f < nf; f++) {
+    double total = 0.0;
+    for (auto &F : faces) total += F.sign * s->face_flux(F, f);
+    out[f] = total;
+  }
+  return nf;
+}
+
+int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out) {
+  int64_t at = 0;
+  auto put = [&](double v) {
+    if (out) out[at] = v;
+    at++;
+  };
+  if (which == 0 || which == 1) {
+    for (int c = 0; c < 3; c++)
+      for (double v : (which == 0 ? s->ca[c] : s->cb[c])) put(v);
+  } else if (which == 2 || which == 3) {
+    for (int c = 0; c < 3; c++)
+      for (int64_t m = 0; m < s->g.n[c]; m++) put((which == 2 ? s->kn[c][m] : s->kh[c][m]) / s->g.d[c]);
+  } else if (which == 4) {
+    for (const SlabInfo &sl : s->slabs) {
+      put(sl.field);
+      put(sl.comp);
+      put(sl.axis);
+      put((double)sl.from);
+      put((double)sl.count);
+      for (double v : sl.b) put(v);
+      for (double v : sl.a) put(v);
+    }
+  }
+  return at;
+}
+
+fdtd_ctx *pxs_engine(pxs_sim *s) { return s ? s->ctx : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,114 @@
+"""The CUDA engine against the oracle on the same inputs.
+
+- Without sources, the engine's f64 and f32 arithmetic IS the oracle's (the reference's CPU
+  kernel, src/fdtd/kernel/reference.rs, and its f32 `Yee<f32>`): fields equal bit for bit, on
+  every boundary kind (CPML with kappa and alpha, walls, periodic sides, 2D).
+- With sources and monitors too: the device evaluates the waveforms and the transforms' phases
+  in f64 with the reference's own exp and sincos algorithms (photonoxide_b200/csrc/portable.h),
+  accumulates the transforms in f64 in time order, and adds each source's amount where the CPU
+  step does. So the f64 engine's fields, probes, transforms and fluxes are the oracle's bits, and
+  the f32 engine's are the oracle's f32 bits; against the f64 oracle the f32 engine is within the
+  reference's GPU tolerance, 2e-5 over 800 steps (src/fdtd/gpu/tests.rs:51-66).
+"""
+import numpy as np
+import pytest
+
+from photonoxide_b200.fdtd import Simulation
+from photonoxide_b200.types import Axis, Boundaries, Field, Grid3d, Periodic
+from pyoracle import OracleSimulation
+from scenarios import busy, closed, noise, stirred
+
+pytestmark = pytest.mark.gpu
+
+
+def relative(a, b):
+    """The largest difference of a from b, relative to the largest of b (gpu/checks.rs:16-23)."""
+    a, b = np.asarray(a), np.asarray(b)
+    scale = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / scale) if scale > 0 else float(np.max(np.abs(a)))
+
+
+def fields(s):
+    return [s.e(c) for c in range(3)] + [s.h(c) for c in range(3)]
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+@pytest.mark.parametrize("periodic", [(), (0,), (1,), (2,), (0, 1), (0, 1, 2)])
+def test_stirred_bit_for_bit(precision, periodic):
+    p = stirred(lambda *a: Simulation(*a, precision=precision), periodic_axes=periodic)
+    o = stirred(lambda *a: OracleSimulation(*a, precision=precision), periodic_axes=periodic)
+    p.run(37)
+    o.run(37)
+    for c, (x, y) in enumerate(zip(fields(p), fields(o))):
+        assert np.array_equal(x, y), (c, relative(x, y))
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_two_d_bit_for_bit(precision):
+    """A grid one cell thick and periodic along z (Boundaries::cpml_2d), odd sizes."""
+    def make(cls):
+        g = Grid3d.centred((53, 29, 1), 0.05)
+        eps = np.ones((3, g.cells())) * 2.25
+        s = cls(g, eps, Boundaries.cpml_2d(6), 0.7, precision=precision)
+        r = np.arange(g.cells())
+        for c in range(3):
+            s.set_field(Field.E, c, noise(r + 5 * c))
+            s.set_field(Field.H, c, noise(r + 9 * c + 123))
+        return s
+    p, o = make(Simulation), make(OracleSimulation)
+    p.run(120)
+    o.run(120)
+    for x, y in zip(fields(p), fields(o)):
+        assert np.array_equal(x, y)
+
+
+def test_closed_box_f32_bit_for_bit_over_300_steps():
+    p = closed(lambda *a: Simulation(*a, precision=32), n=(40, 36, 32))
+    o = closed(lambda *a: OracleSimulation(*a, precision=32), n=(40, 36, 32))
+    p.run(300)
+    o.run(300)
+    for x, y in zip(fields(p), fields(o)):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("two_d", [False, True])
+def test_busy_bit_for_bit(two_d, precision):
+    p = busy(lambda *a: Simulation(*a, precision=precision), two_d)
+    o = busy(lambda *a: OracleSimulation(*a, precision=precision), two_d)
+    p.run(800)
+    o.run(800)
+    for c, (x, y) in enumerate(zip(fields(p), fields(o))):
+        assert np.array_equal(x, y), (c, relative(x, y))
+    for n in range(6):
+        assert np.array_equal(p.probe(n), o.probe(n)), n
+    assert np.array_equal(p.transforms(), o.transforms()), relative(p.transforms(), o.transforms())
+    assert np.array_equal(p.flux(0), o.flux(0))
+
+
+@pytest.mark.parametrize("two_d", [False, True])
+def test_busy_f32_within_the_reference_tolerance(two_d):
+    p = busy(lambda *a: Simulation(*a, precision=32), two_d)
+    o = busy(lambda *a: OracleSimulation(*a, precision=64), two_d)
+    p.run(800)
+    o.run(800)
+    for x, y in zip(fields(p), fields(o)):
+        assert relative(x, y) < 2e-5
+    assert relative(p.transforms(), o.transforms()) < 2e-5
+
+
+def test_runs_in_pieces_give_the_same_bits():
+    """Simulation::run gives the same bits however the steps are split (src/fdtd.rs:1169-1190),
+    and a run repeats bit for bit (src/fdtd/gpu/tests.rs:93-115)."""
+    a = busy(lambda *x: Simulation(*x), False)
+    b = busy(lambda *x: Simulation(*x), False)
+    c = busy(lambda *x: Simulation(*x), False)
+    a.run(800)
+    for _ in range(6):
+        b.run(130)
+    b.run(20)
+    c.run(800)
+    for x, y, z in zip(fields(a), fields(b), fields(c)):
+        assert np.array_equal(x, y) and np.array_equal(x, z)
+    assert np.array_equal(a.transforms(), b.transforms())
+    assert np.array_equal(a.probe(3), b.probe(3))
