@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -34,7 +35,7 @@
 namespace pxf {
 
 constexpr int TX = 32;  // a tile's values along x
-constexpr int TY = 8;   // and along y
+constexpr int TY = 16;  // and along y
 constexpr int NT = 256; // threads per CTA
 constexpr int RX = TX + 2, RY = TY + 2;  // E's staged region: x0-1 .. x0+TX, y0-1 .. y0+TY
 constexpr int HX = TX + 1, HY = TY + 1;  // H's computed region: x0-1 .. x0+TX-1, y0-1 ..
@@ -161,11 +162,17 @@ __device__ inline T slab_update(const StepArgs<T> &A, const SlabEntry *s, int c,
 }
 
 // The fused step over one tile column and a run of planes.
+template <typename T>
+constexpr size_t plain_smem_bytes() {
+  return sizeof(T) * (2 * 3 * RY * RX + 2 * 3 * HY * HX + 3 * TY * TX);
+}
+
 template <typename T, bool LOSSY, bool MEDIA>
 __global__ void __launch_bounds__(NT) step_kernel(StepArgs<T> A) {
-  __shared__ T sE[2][3][RY][RX];
-  __shared__ T sH[2][3][HY][HX];
-  __shared__ T sEn[3][TY][TX];
+  extern __shared__ __align__(16) unsigned char plain_raw[];
+  T(*sE)[3][RY][RX] = reinterpret_cast<T(*)[3][RY][RX]>(plain_raw);
+  T(*sH)[3][HY][HX] = reinterpret_cast<T(*)[3][HY][HX]>(plain_raw + sizeof(T) * 2 * 3 * RY * RX);
+  T(*sEn)[TY][TX] = reinterpret_cast<T(*)[TY][TX]>(plain_raw + sizeof(T) * (2 * 3 * RY * RX + 2 * 3 * HY * HX));
   const int tid = threadIdx.x;
   const int tile = blockIdx.x;
   const int x0 = (tile % A.tiles_x) * TX, y0 = (tile / A.tiles_x) * TY;
@@ -377,6 +384,1332 @@ __global__ void __launch_bounds__(NT) step_kernel(StepArgs<T> A) {
   }
 }
 
+
+// ------------------------------------------------------------------------------------------
+// The staged step (v1). The same arithmetic as step_kernel, with each plane's inputs brought into
+// shared memory ahead of use by cp.async in 16-byte chunks: E's plane k+1 over the tile and the
+// rows and columns around it, H's plane k over its region, cb's plane k over the tile. A ring of
+// STAGES plane-buffers keeps DEPTH = STAGES - 2 planes in flight while the CTA computes plane k
+// from buffers k and k-1. Needs nx a multiple of 16 bytes' worth of values (4 in f32, 2 in f64),
+// so a chunk never straddles the grid's edge: a chunk beyond a wall is zero-filled (src-size 0)
+// and one across a periodic side is read from the wrapped place.
+//
+// Work: the grid's (tile, plane) pairs in tile-major order, split evenly over the resident CTAs;
+// a CTA's share is one or a few runs of consecutive planes of a tile, each started by the
+// prologue that recomputes H's plane before its first.
+
+__device__ inline void cp_async16(void *smem, const void *gmem, bool valid) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
+               : "memory");
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ inline void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <typename T>
+struct Stage {
+  static constexpr int CH = 16 / (int)sizeof(T);  // values per 16-byte chunk
+  static constexpr int EW = TX + 2 * CH;          // E region: x0-CH .. x0+TX+CH-1
+  static constexpr int EH = TY + 2;               //           y0-1 .. y0+TY
+  static constexpr int HW = TX + CH;              // H region: x0-CH .. x0+TX-1
+  static constexpr int HH = TY + 1;               //           y0-1 .. y0+TY-1
+  static constexpr int E_VALS = 3 * EH * EW;
+  static constexpr int H_VALS = 3 * HH * HW;
+  static constexpr int B_VALS = 3 * TY * TX;
+  static constexpr int VALS = E_VALS + H_VALS + B_VALS;
+  static constexpr int E_CHUNKS = E_VALS / CH, H_CHUNKS = H_VALS / CH, B_CHUNKS = B_VALS / CH;
+  static constexpr int NEW_VALS = 3 * HH * (TX + 1);  // H's new plane over (x0-1.., y0-1..)
+};
+
+template <typename T, int STAGES>
+constexpr size_t staged_smem_bytes() {
+  return sizeof(T) * ((size_t)STAGES * Stage<T>::VALS + Stage<T>::NEW_VALS);
+}
+
+// Issues the copies of one stage: E's plane `ke` (the region), H's and cb's plane `kh`; a plane
+// of -1 is beyond a wall (zeros). `parts`: 1 E only, 3 everything.
+template <typename T>
+__device__ inline void issue_stage(const StepArgs<T> &A, T *buf, int x0, int y0, int ke, int kh,
+                                   int parts) {
+  using S = Stage<T>;
+  const int nx = A.n[0], ny = A.n[1];
+  const long long N = A.N;
+  const int tid = threadIdx.x;
+  const T *dummy = A.e_in;
+  for (int q = tid; q < S::E_CHUNKS; q += NT) {
+    int c = q / (S::EH * (S::EW / S::CH)), rem = q % (S::EH * (S::EW / S::CH));
+    int ry = rem / (S::EW / S::CH), cx = rem % (S::EW / S::CH);
+    int gx = x0 - S::CH + cx * S::CH;
+    int gy = wrap_index(y0 - 1 + ry, ny, A.periodic[1]);
+    if (gx < 0) gx = A.periodic[0] ? gx + nx : -1;
+    else if (gx >= nx) gx = (A.periodic[0] && gx == nx) ? 0 : -1;
+    bool ok = gx >= 0 && gy >= 0 && ke >= 0;
+    const T *src = ok ? A.e_in + c * N + ((long long)ke * ny + gy) * nx + gx : dummy;
+    cp_async16(buf + (size_t)q * S::CH, src, ok);
+  }
+  if (parts & 2) {
+    T *hb = buf + S::E_VALS;
+    for (int q = tid; q < S::H_CHUNKS; q += NT) {
+      int c = q / (S::HH * (S::HW / S::CH)), rem = q % (S::HH * (S::HW / S::CH));
+      int ry = rem / (S::HW / S::CH), cx = rem % (S::HW / S::CH);
+      int gx = x0 - S::CH + cx * S::CH;
+      int gy = wrap_index(y0 - 1 + ry, ny, A.periodic[1]);
+      if (gx < 0) gx = A.periodic[0] ? gx + nx : -1;
+      else if (gx >= nx) gx = -1;
+      bool ok = gx >= 0 && gy >= 0 && kh >= 0;
+      const T *src = ok ? A.h_in + c * N + ((long long)kh * ny + gy) * nx + gx : dummy;
+      cp_async16(hb + (size_t)q * S::CH, src, ok);
+    }
+    T *bb = hb + S::H_VALS;
+    for (int q = tid; q < S::B_CHUNKS; q += NT) {
+      int c = q / (TY * (TX / S::CH)), rem = q % (TY * (TX / S::CH));
+      int ry = rem / (TX / S::CH), cx = rem % (TX / S::CH);
+      int gx = x0 + cx * S::CH, gy = y0 + ry;
+      bool ok = gx < nx && gy < ny && kh >= 0;
+      const T *src = ok ? A.cb + c * N + ((long long)kh * ny + gy) * nx + gx : dummy;
+      cp_async16(bb + (size_t)q * S::CH, src, ok);
+    }
+  }
+}
+
+template <typename T, bool LOSSY, bool MEDIA, int STAGES>
+__global__ void __launch_bounds__(NT) staged_kernel(StepArgs<T> A, long long total, int ctas) {
+  using S = Stage<T>;
+  constexpr int DEPTH = STAGES - 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *stages = reinterpret_cast<T *>(smem_raw);
+  T *sHn = stages + (size_t)STAGES * S::VALS;  // [3][HH][TX+1]
+  T *sEn = sHn;  // [3][TY][TX]: E's new plane while sources add to it, once H's is read
+  const int tid = threadIdx.x;
+  const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
+  const long long N = A.N;
+  const long long begin = total * blockIdx.x / ctas, end = total * (blockIdx.x + 1) / ctas;
+  auto E = [&](int b, int c, int y, int x) -> T & {  // E region of buffer b
+    return stages[(size_t)b * S::VALS + ((size_t)c * S::EH + y) * S::EW + x];
+  };
+  auto Hold = [&](int b, int c, int y, int x) -> T & {
+    return stages[(size_t)b * S::VALS + S::E_VALS + ((size_t)c * S::HH + y) * S::HW + x];
+  };
+  auto CB = [&](int b, int c, int y, int x) -> T & {
+    return stages[(size_t)b * S::VALS + S::E_VALS + S::H_VALS + ((size_t)c * TY + y) * TX + x];
+  };
+  auto Hn = [&](int c, int y, int x) -> T & { return sHn[((size_t)c * S::HH + y) * (TX + 1) + x]; };
+
+  for (long long at = begin; at < end;) {
+    const int tile = (int)(at / nz);
+    const int k0 = (int)(at % nz);
+    const int k1 = (int)min((long long)nz, (long long)k0 + (end - at));
+    at += k1 - k0;
+    const int x0 = (tile % A.tiles_x) * TX, y0 = (tile / A.tiles_x) * TY;
+    const int km = wrap_index(k0 - 1, nz, A.periodic[2]);
+    // positions: 0 E(km) (when km exists), 1 stage k0-1, 2 + (k - k0) stage k
+    const int last = 2 + (k1 - 1 - k0);
+    auto issue = [&](int pos) {
+      if (pos <= last) {
+        T *buf = stages + (size_t)(pos % STAGES) * S::VALS;
+        if (pos == 0) {
+          if (km >= 0) issue_stage(A, buf, x0, y0, km, -1, 1);
+        } else {
+          int k = k0 - 2 + pos;  // the stage's plane: E's region of k+1, H's and cb's k
+          int kh = pos == 1 ? km : k;
+          issue_stage(A, buf, x0, y0, wrap_index(k + 1, nz, A.periodic[2]), kh, 3);
+        }
+      }
+      cp_async_commit();
+    };
+    for (int pos = 0; pos < 1 + DEPTH; pos++) issue(pos);
+    // -- prologue: H's new plane km over the region, from E(km) (position 0) and stage 1
+    T hprev[2][2];  // H_x and H_y of plane k-1 at this thread's two E values
+    cp_async_wait<DEPTH - 1>();  // positions 0 and 1 landed
+    __syncthreads();
+    issue(1 + DEPTH);  // into a buffer not used yet
+    // entering iteration p (= 2 + k - k0) the copies up to p + DEPTH - 1 have been issued
+    auto compute_h = [&](int bc, int bn, int bp, int kk, bool write) {
+      // bc: buffer holding E(kk) (as its E region), bn: buffer with E(kk+1) and H(kk)
+      const bool zslab = !A.periodic[2] && (kk < A.low[2] || kk >= nz - A.high[2]);
+      for (int q = tid; q < S::HH * (TX + 1); q += NT) {
+        int ly = q / (TX + 1), lx = q % (TX + 1);
+        int gxr = x0 - 1 + lx, gyr = y0 - 1 + ly;
+        int gi = wrap_index(gxr, nx, A.periodic[0]), gj = wrap_index(gyr, ny, A.periodic[1]);
+        if (gi < 0 || gj < 0 || gxr >= nx || gyr >= ny) {
+          Hn(0, ly, lx) = Hn(1, ly, lx) = Hn(2, ly, lx) = T(0);
+          continue;
+        }
+        bool own = write && lx >= 1 && ly >= 1;
+        int ex = lx - 1 + S::CH;  // this place in the E region
+        T ex0 = E(bc, 0, ly, ex), ey0 = E(bc, 1, ly, ex), ez0 = E(bc, 2, ly, ex);
+        T dyEz = E(bc, 2, ly + 1, ex) - ez0, dxEz = E(bc, 2, ly, ex + 1) - ez0;
+        T dxEy = E(bc, 1, ly, ex + 1) - ey0, dyEx = E(bc, 0, ly + 1, ex) - ex0;
+        T dzEy = E(bn, 1, ly, ex) - ey0, dzEx = E(bn, 0, ly, ex) - ex0;
+        T fx = A.fh[gi], fy = A.fh[nx + gj], fz = A.fh[nx + ny + kk];
+        int hx_ = lx - 1 + S::CH;
+        T hx = Hold(bn, 0, ly, hx_) - A.dt * (dyEz * fy - dzEy * fz);
+        T hy = Hold(bn, 1, ly, hx_) - A.dt * (dzEx * fz - dxEz * fx);
+        T hz = Hold(bn, 2, ly, hx_) - A.dt * (dxEy * fx - dyEx * fy);
+        const SlabEntry *sl;
+        if ((sl = slab_at(A, 1, 0, 1, gj))) hx = slab_update<T, 1>(A, sl, 0, 1, gi, gj, kk, dyEz, hx, T(0), own);
+        if (zslab && (sl = slab_at(A, 1, 0, 2, kk))) hx = slab_update<T, 1>(A, sl, 0, 2, gi, gj, kk, dzEy, hx, T(0), own);
+        if ((sl = slab_at(A, 1, 1, 0, gi))) hy = slab_update<T, 1>(A, sl, 1, 0, gi, gj, kk, dxEz, hy, T(0), own);
+        if (zslab && (sl = slab_at(A, 1, 1, 2, kk))) hy = slab_update<T, 1>(A, sl, 1, 2, gi, gj, kk, dzEx, hy, T(0), own);
+        if ((sl = slab_at(A, 1, 2, 0, gi))) hz = slab_update<T, 1>(A, sl, 2, 0, gi, gj, kk, dxEy, hz, T(0), own);
+        if ((sl = slab_at(A, 1, 2, 1, gj))) hz = slab_update<T, 1>(A, sl, 2, 1, gi, gj, kk, dyEx, hz, T(0), own);
+        Hn(0, ly, lx) = hx;
+        Hn(1, ly, lx) = hy;
+        Hn(2, ly, lx) = hz;
+      }
+      (void)bp;
+    };
+    auto inject_h = [&](int kk) {  // uniform: only CTAs whose bucket holds sources sync here
+      int bucket = tile * nz + kk;
+      int g0 = A.hbucket[bucket], g1 = A.hbucket[bucket + 1];
+      if (g1 > g0) {
+        __syncthreads();
+        for (int g = g0 + tid; g < g1; g += NT) {
+          Group gr = A.hgroups[g];
+          T *v = &sHn[(size_t)gr.comp * S::HH * (TX + 1) + gr.local];
+          for (int q = gr.first; q < gr.first + gr.count; q++) {
+            Entry en = A.entries[q];
+            double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
+            if (sizeof(T) == 8) *v = *v - (T)((double)A.dt * amount);
+            else *v = *v - A.dt * (T)amount;
+          }
+        }
+      }
+    };
+    if (km >= 0) {
+      compute_h(0 % STAGES, 1 % STAGES, 0, km, false);
+      inject_h(km);
+      __syncthreads();
+      for (int r = 0; r < 2; r++) {
+        int q = tid + r * NT;
+        int ey = q / TX, ex = q % TX;
+        hprev[r][0] = Hn(0, ey + 1, ex + 1);
+        hprev[r][1] = Hn(1, ey + 1, ex + 1);
+      }
+    } else {
+      hprev[0][0] = hprev[0][1] = hprev[1][0] = hprev[1][1] = T(0);
+    }
+    for (int k = k0; k < k1; k++) {
+      const int pos = 2 + (k - k0);
+      cp_async_wait<DEPTH - 1>();
+      __syncthreads();  // stage pos landed for every thread; everyone is done with plane k-1
+      issue(pos + DEPTH);
+      const int bc = (pos - 1) % STAGES, bn = pos % STAGES;
+      compute_h(bc, bn, 0, k, true);
+      inject_h(k);
+      __syncthreads();
+      // E's new plane k on the tile, two values a thread
+      const int ebucket = tile * nz + k;
+      const int eg0 = A.ebucket[ebucket], eg1 = A.ebucket[ebucket + 1];
+      const bool zslab = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
+      T enew[2][3];
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        int q = tid + r * NT;
+        int ey = q / TX, ex = q % TX;
+        int gi = x0 + ex, gj = y0 + ey;
+        bool valid = gi < nx && gj < ny;
+        T hxv = Hn(0, ey + 1, ex + 1), hyv = Hn(1, ey + 1, ex + 1), hzv = Hn(2, ey + 1, ex + 1);
+        if (valid) {
+          long long r0 = ((long long)k * ny + gj) * nx + gi;
+          A.h_out[r0] = hxv;
+          A.h_out[N + r0] = hyv;
+          A.h_out[2 * N + r0] = hzv;
+          bool zb = wrap_index(k - 1, nz, A.periodic[2]) >= 0;
+          T hz_xm = Hn(2, ey + 1, ex), hy_xm = Hn(1, ey + 1, ex);
+          T hz_ym = Hn(2, ey, ex + 1), hx_ym = Hn(0, ey, ex + 1);
+          T hy_zm = zb ? hprev[r][1] : T(0), hx_zm = zb ? hprev[r][0] : T(0);
+          T fx = A.fe[gi], fy = A.fe[nx + gj], fz = A.fe[nx + ny + k];
+          T dyHz = hzv - hz_ym, dzHy = hyv - hy_zm, dzHx = hxv - hx_zm, dxHz = hzv - hz_xm;
+          T dxHy = hyv - hy_xm, dyHx = hxv - hx_ym;
+          T curl[3] = {dyHz * fy - dzHy * fz, dzHx * fz - dxHz * fx, dxHy * fx - dyHx * fy};
+          T diffs[3][3] = {{T(0), dyHz, dzHy}, {dxHz, T(0), dzHx}, {dxHy, dyHx, T(0)}};
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            T eo = E(bc, c, ey + 1, ex + S::CH);
+            T cbv = CB(bn, c, ey, ex);
+            T cav;
+            if (LOSSY) cav = A.ca[c * N + r0];
+            else cav = cbv == T(0) ? T(0) : T(1);
+            T v = cav * eo + cbv * curl[c];
+            int w0 = (c + 1) % 3, w1 = (c + 2) % 3;
+            int wa = min(w0, w1), wb = max(w0, w1);
+            int m[3] = {gi, gj, k};
+            const SlabEntry *sl;
+            if ((wa != 2 || zslab) && (sl = slab_at(A, 0, c, wa, m[wa]))) v = slab_update<T, 0>(A, sl, c, wa, gi, gj, k, diffs[c][wa], v, cbv, true);
+            if ((wb != 2 || zslab) && (sl = slab_at(A, 0, c, wb, m[wb]))) v = slab_update<T, 0>(A, sl, c, wb, gi, gj, k, diffs[c][wb], v, cbv, true);
+            enew[r][c] = v;
+          }
+        }
+        hprev[r][0] = hxv;
+        hprev[r][1] = hyv;
+      }
+      if (eg1 > eg0) {  // electric currents on this tile and plane: through shared memory
+        __syncthreads();  // every thread has read H's new plane
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+          int q = tid + r * NT;
+#pragma unroll
+          for (int c = 0; c < 3; c++) sEn[(size_t)c * TY * TX + q] = enew[r][c];
+        }
+        __syncthreads();
+        for (int g = eg0 + tid; g < eg1; g += NT) {
+          Group gr = A.egroups[g];
+          int ey = gr.local / TX, ex = gr.local % TX;
+          long long r0 = ((long long)k * ny + (y0 + ey)) * nx + (x0 + ex);
+          T cbv = A.cb[gr.comp * N + r0];
+          T *v = &sEn[(size_t)gr.comp * TY * TX + gr.local];
+          for (int q = gr.first; q < gr.first + gr.count; q++) {
+            Entry en2 = A.entries[q];
+            double amount = en2.are * A.waves_e[2 * en2.emitter] - en2.aim * A.waves_e[2 * en2.emitter + 1];
+            if (sizeof(T) == 8) *v = *v - (T)((double)cbv * amount);
+            else *v = *v - cbv * (T)amount;
+          }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+          int q = tid + r * NT;
+#pragma unroll
+          for (int c = 0; c < 3; c++) enew[r][c] = sEn[(size_t)c * TY * TX + q];
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 2; r++) {
+        int q = tid + r * NT;
+        int ey = q / TX, ex = q % TX;
+        int gi = x0 + ex, gj = y0 + ey;
+        if (gi >= nx || gj >= ny) continue;
+        long long r0 = ((long long)k * ny + gj) * nx + gi;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          T v = enew[r][c];
+          if (MEDIA) {
+            int mi = A.media.member[c * N + r0];
+            if (mi >= 0) {
+              const MediaArgs<T> &M = A.media;
+              int g = M.group[mi];
+              int np = M.gpoles[g];
+              T before = M.before[mi];
+              T rest = M.gchi[g] * before;
+              const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+              T *cur = M.current + (long long)mi * M.maxpoles;
+              T *prev = M.previous + (long long)mi * M.maxpoles;
+              for (int p = 0; p < np; p++)
+                rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
+              T next = v + M.scale[mi] * rest;
+              T slope = (next - before) / M.two_dt;
+              for (int p = 0; p < np; p++) {
+                T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
+                prev[p] = cur[p];
+                cur[p] = jn;
+              }
+              M.before[mi] = E(bc, c, ey + 1, ex + S::CH);
+              v = next;
+            }
+          }
+          A.e_out[c * N + r0] = v;
+        }
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();  // the next run of planes reuses the buffers
+  }
+}
+
+
+// ------------------------------------------------------------------------------------------
+// The row step (v2). A CTA owns OWN = 63 values along x and RW rows along y of every plane in a
+// run of planes, and marches up z. Warp w holds row y0 - 1 + w (warp 0 the row before the tile,
+// whose new H the first row's E needs); lane l holds the values x0 - 1 + l and x0 + 31 + l of
+// its row, 64 H values, so each warp recomputes only one H value per row that its neighbour
+// along x owns. Neighbours along x come by warp shuffles, along y through a small exchange in
+// shared memory, along z from the registers of the previous plane. Each plane's inputs for the
+// next plane are loaded into registers one plane ahead. The arithmetic of every value is
+// step_kernel's, operation for operation.
+namespace rowstep {
+constexpr int SEG = 64;       // H values a warp row holds
+constexpr int OWN = SEG - 1;  // values a tile owns along x
+constexpr int RW = 7;         // rows a tile owns along y
+constexpr int WARPS = RW + 1;
+constexpr int THREADS = 32 * WARPS;
+}  // namespace rowstep
+
+// The CPML share of one value along axis w whose index is m there; `s` the slab holding it.
+template <typename T, int FIELD>
+__device__ __forceinline__ T slab_apply(const StepArgs<T> &A, const SlabEntry s, int c, int w,
+                                        int i, int j, int k, T diff, T v, T cbv, bool own) {
+  int m = w == 0 ? i : (w == 1 ? j : k);
+  int q = m - s.from;
+  int li = i, lj = j, lk = k;
+  int dx = A.n[0], dy = A.n[1];
+  if (w == 0) { li = q; dx = s.count; }
+  else if (w == 1) { lj = q; dy = s.count; }
+  else lk = q;
+  long long p = s.psi + ((long long)lk * dy + lj) * dx + li;
+  T d = diff / A.step[w];
+  T b = A.coefs[s.coef + q], a = A.coefs[s.coef + s.count + q];
+  T old = FIELD == 1 ? A.psi_h_in[p] : A.psi_e[p];
+  T psi = b * old + a * d;
+  if (own) {
+    if (FIELD == 1) A.psi_h_out[p] = psi;
+    else A.psi_e[p] = psi;
+  }
+  T sign = (w == (c + 1) % 3) ? T(1) : T(-1);
+  T u = sign * psi;
+  if (FIELD == 1) return v - A.dt * u;
+  return v + cbv * u;
+}
+// The slab of `field`'s component c along axis w on `side` (0 low, 1 high), from the table.
+template <typename T>
+__device__ __forceinline__ SlabEntry slab_of(const StepArgs<T> &A, int field, int c, int w, int side) {
+  return A.slab[field][c][w][side];
+}
+// The slab along z holding plane k for component c of `field`, or count 0.
+template <typename T>
+__device__ __forceinline__ SlabEntry zslab_of(const StepArgs<T> &A, int field, int c, int k) {
+  SlabEntry none;
+  none.count = 0;
+  none.from = 0;
+  none.psi = 0;
+  none.coef = 0;
+  if (A.periodic[2]) return none;
+  if (k < A.low[2]) return A.slab[field][c][2][0];
+  if (k >= A.n[2] - A.high[2]) return A.slab[field][c][2][1];
+  return none;
+}
+
+template <typename T, bool LOSSY, bool MEDIA>
+__global__ void __launch_bounds__(rowstep::THREADS, 2) row_kernel(StepArgs<T> A) {
+  using namespace rowstep;
+  __shared__ T sE[2][WARPS][SEG];  // E_x, E_z of plane k, each warp's row (for the row above)
+  __shared__ T sH[2][WARPS][SEG];  // H_x, H_z of plane k (for the row below)
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
+  const long long N = A.N;
+  const int tile = blockIdx.x;
+  const int x0 = (tile % A.tiles_x) * OWN, y0 = (tile / A.tiles_x) * RW;
+  const int kbeg = blockIdx.y * A.zchunk, kend = min(kbeg + A.zchunk, nz);
+  if (kbeg >= nz) return;
+  const int tileidx = tile;
+
+  // -- per lane: the two x places; per warp: the row
+  int gx[2], mx[2], mxp[2];
+  bool hval[2], own[2], ev[2];
+  const int gy = y0 - 1 + w;
+  const int my = wrap_index(gy, ny, A.periodic[1]);
+  const int myp = wrap_index(gy + 1, ny, A.periodic[1]);  // the row after (for +y at the last warp)
+  const bool rowok = my >= 0 && gy < ny;  // this row's H is computed
+  const bool rowe = my >= 0;                // this row's E is read (a wrapped row included)
+  T fhx[2], fex[2];
+  int sx[2];  // the CPML side along x at each place (0 low, 1 high, -1 none)
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    gx[h] = x0 - 1 + lane + 32 * h;
+    mx[h] = wrap_index(gx[h], nx, A.periodic[0]);
+    mxp[h] = wrap_index(gx[h] + 1, nx, A.periodic[0]);
+    hval[h] = rowok && mx[h] >= 0 && gx[h] < nx;
+    ev[h] = rowe && mx[h] >= 0;
+    own[h] = hval[h] && w >= 1 && (lane + 32 * h) >= 1 && gx[h] < nx;
+    fhx[h] = mx[h] >= 0 ? A.fh[mx[h]] : T(0);
+    fex[h] = mx[h] >= 0 ? A.fe[mx[h]] : T(0);
+    sx[h] = -1;
+    if (mx[h] >= 0 && !A.periodic[0]) {
+      if (mx[h] < A.low[0]) sx[h] = 0;
+      else if (mx[h] >= nx - A.high[0]) sx[h] = 1;
+    }
+  }
+  const T fhy = my >= 0 ? A.fh[nx + my] : T(0), fey = my >= 0 ? A.fe[nx + my] : T(0);
+  int sy = -1;  // the CPML side along y of this row
+  if (my >= 0 && !A.periodic[1]) {
+    if (my < A.low[1]) sy = 0;
+    else if (my >= ny - A.high[1]) sy = 1;
+  }
+  // the value after the warp's 64 along x (E_y, E_z of plane k there) for the last lane
+  const int gxe = x0 + OWN, mxe = wrap_index(gxe, nx, A.periodic[0]);
+  long long rowoff = my >= 0 ? (long long)my * nx : 0;
+  long long rowoffp = myp >= 0 ? (long long)myp * nx : 0;
+
+  // -- one plane's inputs: E(k+1) at the H places, H(k) there, cb(k) at the owned places, and
+  // E(k)'s values past the warp's row ends: x after the last lane (E_y, E_z), and for the last
+  // warp the row after (E_x, E_z)
+  struct Plane {
+    T e1[3][2], hold[3][2], cb[3][2], ca[3][2];
+    T xe[2];      // E_y, E_z(k) at x0 + 63
+    T ye[2][2];   // E_x, E_z(k) at row gy + 1 (last warp), per half
+  };
+  auto load = [&](Plane &P, int k) {
+    const int k1 = wrap_index(k + 1, nz, A.periodic[2]);
+    const long long pk = (long long)k * ny * nx, pk1 = (long long)k1 * ny * nx;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      long long at = pk + rowoff + mx[h], at1 = pk1 + rowoff + mx[h];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        P.e1[c][h] = (ev[h] && k1 >= 0) ? A.e_in[c * N + at1] : T(0);
+        P.hold[c][h] = hval[h] ? A.h_in[c * N + at] : T(0);
+        P.cb[c][h] = own[h] ? A.cb[c * N + at] : T(0);
+        if (LOSSY) P.ca[c][h] = own[h] ? A.ca[c * N + at] : T(0);
+      }
+      if (w == WARPS - 1) {
+        bool ok = myp >= 0 && mx[h] >= 0;
+        long long atp = pk + rowoffp + mx[h];
+        P.ye[0][h] = ok ? A.e_in[atp] : T(0);
+        P.ye[1][h] = ok ? A.e_in[2 * N + atp] : T(0);
+      }
+    }
+    bool okx = rowe && mxe >= 0;
+    long long atx = pk + rowoff + (mxe >= 0 ? mxe : 0);
+    P.xe[0] = okx ? A.e_in[N + atx] : T(0);
+    P.xe[1] = okx ? A.e_in[2 * N + atx] : T(0);
+  };
+  auto e_now = [&](T ek[3][2], int k) {  // E(k) at the H places
+    const long long pk = (long long)k * ny * nx;
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) ek[c][h] = ev[h] ? A.e_in[c * N + pk + rowoff + mx[h]] : T(0);
+  };
+
+  // H's new plane k at the H places (reference.rs:14-50, then the slabs x, y, z)
+  auto compute_h = [&](const Plane &P, const T ek[3][2], int k, bool write, T hn[3][2]) {
+    // E(k) of the row after: the next warp's row, or the loaded row for the last warp
+    sE[0][w][lane] = ek[0][0];
+    sE[0][w][lane + 32] = ek[0][1];
+    sE[1][w][lane] = ek[2][0];
+    sE[1][w][lane + 32] = ek[2][1];
+    __syncthreads();
+    const T fhz = A.fh[nx + ny + k];
+    const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      // +x: the next lane's value; lane 31 of the first half takes lane 0 of the second, lane 31
+      // of the second the value after the row
+      T ey_n = __shfl_down_sync(0xffffffffu, ek[1][h], 1);
+      T ez_n = __shfl_down_sync(0xffffffffu, ek[2][h], 1);
+      T ey_o = __shfl_sync(0xffffffffu, ek[1][1 - h], 0);
+      T ez_o = __shfl_sync(0xffffffffu, ek[2][1 - h], 0);
+      if (lane == 31) {
+        ey_n = h == 0 ? ey_o : P.xe[0];
+        ez_n = h == 0 ? ez_o : P.xe[1];
+      }
+      // a neighbour beyond a wall is zero: the place after x = nx - 1 (mxp < 0)
+      if (mxp[h] < 0) ey_n = ez_n = T(0);
+      T ex_yn, ez_yn;
+      if (w < WARPS - 1) {
+        ex_yn = sE[0][w + 1][lane + 32 * h];
+        ez_yn = sE[1][w + 1][lane + 32 * h];
+      } else {
+        ex_yn = P.ye[0][h];
+        ez_yn = P.ye[1][h];
+      }
+      if (myp < 0) ex_yn = ez_yn = T(0);
+      T dyEz = ez_yn - ek[2][h], dzEy = P.e1[1][h] - ek[1][h];
+      T dzEx = P.e1[0][h] - ek[0][h], dxEz = ez_n - ek[2][h];
+      T dxEy = ey_n - ek[1][h], dyEx = ex_yn - ek[0][h];
+      T hx = P.hold[0][h] - A.dt * (dyEz * fhy - dzEy * fhz);
+      T hy = P.hold[1][h] - A.dt * (dzEx * fhz - dxEz * fhx[h]);
+      T hz = P.hold[2][h] - A.dt * (dxEy * fhx[h] - dyEx * fhy);
+      if (hval[h]) {
+        const bool ow = write && own[h];
+        const int i = mx[h], j = my;
+        if ((sx[h] >= 0) | (sy >= 0) | zs) {
+          // H_x: y then z; H_y: x then z; H_z: x then y (the table's entry has count 0 where a
+          // side has no CPML)
+          if (sy >= 0) {
+            SlabEntry e = slab_of(A, 1, 0, 1, sy);
+            if (e.count) hx = slab_apply<T, 1>(A, e, 0, 1, i, j, k, dyEz, hx, T(0), ow);
+          }
+          if (zs) {
+            SlabEntry z0 = zslab_of(A, 1, 0, k);
+            if (z0.count) hx = slab_apply<T, 1>(A, z0, 0, 2, i, j, k, dzEy, hx, T(0), ow);
+          }
+          if (sx[h] >= 0) {
+            SlabEntry e = slab_of(A, 1, 1, 0, sx[h]);
+            if (e.count) hy = slab_apply<T, 1>(A, e, 1, 0, i, j, k, dxEz, hy, T(0), ow);
+          }
+          if (zs) {
+            SlabEntry z1 = zslab_of(A, 1, 1, k);
+            if (z1.count) hy = slab_apply<T, 1>(A, z1, 1, 2, i, j, k, dzEx, hy, T(0), ow);
+          }
+          if (sx[h] >= 0) {
+            SlabEntry e = slab_of(A, 1, 2, 0, sx[h]);
+            if (e.count) hz = slab_apply<T, 1>(A, e, 2, 0, i, j, k, dxEy, hz, T(0), ow);
+          }
+          if (sy >= 0) {
+            SlabEntry e = slab_of(A, 1, 2, 1, sy);
+            if (e.count) hz = slab_apply<T, 1>(A, e, 2, 1, i, j, k, dyEx, hz, T(0), ow);
+          }
+        }
+      } else {
+        hx = hy = hz = T(0);
+      }
+      hn[0][h] = hx;
+      hn[1][h] = hy;
+      hn[2][h] = hz;
+    }
+    // the magnetic currents at this tile and plane, each value's entries in CPU order
+    const int bucket = tileidx * nz + k;
+    const int g0 = A.hbucket[bucket], g1 = A.hbucket[bucket + 1];
+    for (int g = g0; g < g1; g++) {
+      Group gr = A.hgroups[g];
+      int gw = gr.local / SEG, gi = gr.local % SEG;
+      if (gw == w && (gi & 31) == lane) {
+        const bool second = (gi >> 5) != 0;
+        T v = T(0);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          if (gr.comp == c) v = second ? hn[c][1] : hn[c][0];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          Entry en = A.entries[q];
+          double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
+          if (sizeof(T) == 8) v = v - (T)((double)A.dt * amount);
+          else v = v - A.dt * (T)amount;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          if (gr.comp == c) {
+            if (second) hn[c][1] = v;
+            else hn[c][0] = v;
+          }
+      }
+    }
+  };
+
+  T ek[3][2], hprev[2][2], hn[3][2];
+  Plane P0, P1;
+  // prologue: H's new plane kbeg-1 (wrapped on a periodic z), which E's plane kbeg needs
+  const int km = wrap_index(kbeg - 1, nz, A.periodic[2]);
+  if (km >= 0) {
+    e_now(ek, km);
+    load(P0, km);
+    compute_h(P0, ek, km, false, hn);
+    hprev[0][0] = hn[0][0]; hprev[0][1] = hn[0][1];
+    hprev[1][0] = hn[1][0]; hprev[1][1] = hn[1][1];
+    __syncthreads();
+  } else {
+    hprev[0][0] = hprev[0][1] = hprev[1][0] = hprev[1][1] = T(0);
+  }
+  e_now(ek, kbeg);
+  load(P0, kbeg);
+  auto plane = [&](Plane &P, Plane &Q, int k) {
+    if (k + 1 < kend) load(Q, k + 1);
+    compute_h(P, ek, k, true, hn);
+    // H's tile to memory, and H_x, H_z to the row below
+    const long long pk = (long long)k * ny * nx;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (own[h]) {
+        long long at = pk + rowoff + mx[h];
+        A.h_out[at] = hn[0][h];
+        A.h_out[N + at] = hn[1][h];
+        A.h_out[2 * N + at] = hn[2][h];
+      }
+    }
+    sH[0][w][lane] = hn[0][0];
+    sH[0][w][lane + 32] = hn[0][1];
+    sH[1][w][lane] = hn[2][0];
+    sH[1][w][lane + 32] = hn[2][1];
+    __syncthreads();
+    // E's plane k at the owned places (reference.rs:14-50 with back differences, then the slabs)
+    const T fez = A.fe[nx + ny + k];
+    const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
+    const bool zb = wrap_index(k - 1, nz, A.periodic[2]) >= 0;
+    T en[3][2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      // -x: the previous lane's value; lane 0 of the second half takes lane 31 of the first
+      T hz_p = __shfl_up_sync(0xffffffffu, hn[2][h], 1);
+      T hy_p = __shfl_up_sync(0xffffffffu, hn[1][h], 1);
+      T hz_o = __shfl_sync(0xffffffffu, hn[2][0], 31);
+      T hy_o = __shfl_sync(0xffffffffu, hn[1][0], 31);
+      if (lane == 0) {
+        hz_p = h == 1 ? hz_o : T(0);
+        hy_p = h == 1 ? hy_o : T(0);
+      }
+      if (gx[h] == 0 && !A.periodic[0]) hz_p = hy_p = T(0);  // beyond the wall at x = 0
+      T hx_yp = w >= 1 ? sH[0][w - 1][lane + 32 * h] : T(0);
+      T hz_yp = w >= 1 ? sH[1][w - 1][lane + 32 * h] : T(0);
+      T hy_zp = zb ? hprev[1][h] : T(0), hx_zp = zb ? hprev[0][h] : T(0);
+      T dyHz = hn[2][h] - hz_yp, dzHy = hn[1][h] - hy_zp, dzHx = hn[0][h] - hx_zp;
+      T dxHz = hn[2][h] - hz_p, dxHy = hn[1][h] - hy_p, dyHx = hn[0][h] - hx_yp;
+      T curl[3] = {dyHz * fey - dzHy * fez, dzHx * fez - dxHz * fex[h], dxHy * fex[h] - dyHx * fey};
+      const int i = mx[h], j = my;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T cbv = P.cb[c][h];
+        T cav;
+        if (LOSSY) cav = P.ca[c][h];
+        else cav = cbv == T(0) ? T(0) : T(1);
+        en[c][h] = cav * ek[c][h] + cbv * curl[c];
+      }
+      if (own[h] && ((sx[h] >= 0) | (sy >= 0) | zs)) {
+        // E_x: y then z; E_y: x then z; E_z: x then y
+        if (sy >= 0) {
+          SlabEntry e = slab_of(A, 0, 0, 1, sy);
+          if (e.count) en[0][h] = slab_apply<T, 0>(A, e, 0, 1, i, j, k, dyHz, en[0][h], P.cb[0][h], true);
+        }
+        if (zs) {
+          SlabEntry z0 = zslab_of(A, 0, 0, k);
+          if (z0.count) en[0][h] = slab_apply<T, 0>(A, z0, 0, 2, i, j, k, dzHy, en[0][h], P.cb[0][h], true);
+        }
+        if (sx[h] >= 0) {
+          SlabEntry e = slab_of(A, 0, 1, 0, sx[h]);
+          if (e.count) en[1][h] = slab_apply<T, 0>(A, e, 1, 0, i, j, k, dxHz, en[1][h], P.cb[1][h], true);
+        }
+        if (zs) {
+          SlabEntry z1 = zslab_of(A, 0, 1, k);
+          if (z1.count) en[1][h] = slab_apply<T, 0>(A, z1, 1, 2, i, j, k, dzHx, en[1][h], P.cb[1][h], true);
+        }
+        if (sx[h] >= 0) {
+          SlabEntry e = slab_of(A, 0, 2, 0, sx[h]);
+          if (e.count) en[2][h] = slab_apply<T, 0>(A, e, 2, 0, i, j, k, dxHy, en[2][h], P.cb[2][h], true);
+        }
+        if (sy >= 0) {
+          SlabEntry e = slab_of(A, 0, 2, 1, sy);
+          if (e.count) en[2][h] = slab_apply<T, 0>(A, e, 2, 1, i, j, k, dyHx, en[2][h], P.cb[2][h], true);
+        }
+      }
+      hprev[0][h] = hn[0][h];
+      hprev[1][h] = hn[1][h];
+    }
+    // the electric currents (src/fdtd.rs:1375-1387)
+    {
+      const int bucket = tileidx * nz + k;
+      const int g0 = A.ebucket[bucket], g1 = A.ebucket[bucket + 1];
+      for (int g = g0; g < g1; g++) {
+        Group gr = A.egroups[g];
+        int gw = gr.local / SEG, gi = gr.local % SEG;
+        if (gw == w && (gi & 31) == lane) {
+          const bool second = (gi >> 5) != 0;
+          T cbv = T(0), v = T(0);
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            if (gr.comp == c) {
+              cbv = second ? P.cb[c][1] : P.cb[c][0];
+              v = second ? en[c][1] : en[c][0];
+            }
+          for (int q = gr.first; q < gr.first + gr.count; q++) {
+            Entry e2 = A.entries[q];
+            double amount = e2.are * A.waves_e[2 * e2.emitter] - e2.aim * A.waves_e[2 * e2.emitter + 1];
+            if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
+            else v = v - cbv * (T)amount;
+          }
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+            if (gr.comp == c) {
+              if (second) en[c][1] = v;
+              else en[c][0] = v;
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (!own[h]) continue;
+      long long at = pk + rowoff + mx[h];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T v = en[c][h];
+        if (MEDIA) {
+          int mi = A.media.member[c * N + at];
+          if (mi >= 0) {
+            const MediaArgs<T> &M = A.media;
+            int g = M.group[mi];
+            int np = M.gpoles[g];
+            T before = M.before[mi];
+            T rest = M.gchi[g] * before;
+            const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+            T *cur = M.current + (long long)mi * M.maxpoles;
+            T *prev = M.previous + (long long)mi * M.maxpoles;
+            for (int p = 0; p < np; p++)
+              rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
+            T next = v + M.scale[mi] * rest;
+            T slope = (next - before) / M.two_dt;
+            for (int p = 0; p < np; p++) {
+              T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
+              prev[p] = cur[p];
+              cur[p] = jn;
+            }
+            M.before[mi] = ek[c][h];
+            v = next;
+          }
+        }
+        A.e_out[c * N + at] = v;
+      }
+    }
+    // E(k+1) becomes E(k)
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) ek[c][h] = P.e1[c][h];
+    __syncthreads();  // the exchanges are rewritten next plane
+  };
+  // two planes a turn, so each plane's registers keep a fixed role
+  for (int k = kbeg; k < kend; k += 2) {
+    plane(P0, P1, k);
+    if (k + 1 < kend) plane(P1, P0, k + 1);
+  }
+}
+
+
+// ------------------------------------------------------------------------------------------
+// The quad step (v3), the default where nx is a multiple of 4. A CTA owns OWNX = 124 values along
+// x and RW rows along y of a run of planes. Warp w holds row y0 - 1 + w; lane l holds the four
+// values x0 - 4 + 4l .. x0 - 1 + 4l of it (128 a row: the tile's 124 and the 4 before it, whose
+// last H the tile's first E needs). Every global access is a 16-byte vector. The next plane's E,
+// H and cb rows are brought into shared memory by cp.async while the CTA computes this one (each
+// warp copies its own rows, its lanes' places fixed for the whole run); neighbours along x come
+// from the lane's own registers and one shuffle, along y from the staged rows and a small
+// exchange of H, along z from the registers of the previous plane. The CPML's psi along y and z
+// is read and written four values at once, its coefficients uniform over a row or a plane.
+// Every value's arithmetic is step_kernel's, operation for operation.
+namespace quad {
+constexpr int VEC = 4;
+constexpr int ROW = 128;      // H and E values a warp row holds
+constexpr int OWNX = 124;     // values a tile owns along x
+constexpr int RW = 7;         // rows a tile owns along y
+constexpr int WARPS = RW + 1;
+constexpr int THREADS = 32 * WARPS;
+constexpr int EW = ROW + VEC;  // staged E row: x0-4 .. x0+127 (the last chunk for lane 31's +x)
+constexpr int ER = RW + 2;     // staged E rows: y0-1 .. y0+RW
+template <typename T>
+struct Smem {
+  static constexpr int E_SLOT = 3 * ER * EW;             // E of one plane
+  static constexpr int HB_SLOT = 3 * WARPS * ROW + 3 * RW * ROW;  // H(k) rows, cb(k) rows
+  static constexpr int X = 2 * WARPS * ROW;              // H_x, H_z exchange
+  static constexpr size_t BYTES = sizeof(T) * (3 * (size_t)E_SLOT + 2 * (size_t)HB_SLOT + X);
+};
+}  // namespace quad
+
+template <typename T>
+struct Vec4 {
+  T v[4];
+};
+template <typename T>
+__device__ __forceinline__ Vec4<T> ld4(const T *p) {
+  Vec4<T> r;
+  if (sizeof(T) == 4) {
+    float4 f = *reinterpret_cast<const float4 *>(p);
+    r.v[0] = (T)f.x; r.v[1] = (T)f.y; r.v[2] = (T)f.z; r.v[3] = (T)f.w;
+  } else {
+    double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    r.v[0] = (T)a.x; r.v[1] = (T)a.y; r.v[2] = (T)b.x; r.v[3] = (T)b.y;
+  }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void st4(T *p, const Vec4<T> &r) {
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4((float)r.v[0], (float)r.v[1], (float)r.v[2], (float)r.v[3]);
+  } else {
+    *reinterpret_cast<double2 *>(p) = make_double2((double)r.v[0], (double)r.v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2((double)r.v[2], (double)r.v[3]);
+  }
+}
+
+// four values of a slab (its psi row contiguous in x) updated at once: psi <- b psi + a (d/h),
+// then H -= dt (sign psi) or E += cb (sign psi), each value as slab_update does
+template <typename T, int FIELD>
+__device__ __forceinline__ void slab4(const StepArgs<T> &A, T *psi_out, const T *psi_in, T b, T a,
+                                      T hstep, T sign, const T diff[4], T v[4], const T cbv[4],
+                                      bool write) {
+  Vec4<T> old = ld4(psi_in);
+  Vec4<T> nw;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    T d = diff[j] / hstep;
+    nw.v[j] = b * old.v[j] + a * d;
+    T u = sign * nw.v[j];
+    if (FIELD == 1) v[j] = v[j] - A.dt * u;
+    else v[j] = v[j] + cbv[j] * u;
+  }
+  if (write) st4(psi_out, nw);
+}
+
+template <typename T, bool LOSSY, bool MEDIA>
+__global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
+  using namespace quad;
+  using S = Smem<T>;
+  constexpr int CH = 16 / (int)sizeof(T);  // values a cp.async chunk carries
+  extern __shared__ __align__(16) unsigned char quad_raw[];
+  T *sEs = reinterpret_cast<T *>(quad_raw);          // [3 slots][3][ER][EW]
+  T *sHB = sEs + 3 * (size_t)S::E_SLOT;              // [2 slots][H 3][WARPS][ROW] + [cb 3][RW][ROW]
+  T *sX = sHB + 2 * (size_t)S::HB_SLOT;              // [2][WARPS][ROW]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
+  const long long N = A.N;
+  const int tile = blockIdx.x;
+  const int x0 = (tile % A.tiles_x) * OWNX, y0 = (tile / A.tiles_x) * RW;
+  const int kbeg = blockIdx.y * A.zchunk, kend = min(kbeg + A.zchunk, nz);
+  if (kbeg >= nz) return;
+  const long long plane = (long long)nx * ny;
+
+  // -- this lane's four places along x, this warp's row
+  const int xb = x0 - VEC + VEC * lane;  // the first of the four
+  int mxb;                               // where they are in memory (a wrapped group), or -1
+  if (xb >= 0 && xb < nx) mxb = xb;
+  else if (A.periodic[0] && xb == -VEC) mxb = nx - VEC;
+  else if (A.periodic[0] && xb == nx) mxb = 0;
+  else mxb = -1;
+  // the chunk after the row (lane 31's +x neighbour), x0 + 124
+  const int xa = x0 + OWNX;
+  const int mxa = xa < nx ? xa : ((A.periodic[0] && xa == nx) ? 0 : -1);
+  const int gy = y0 - 1 + w;
+  const int my = wrap_index(gy, ny, A.periodic[1]);
+  const int myp = wrap_index(gy + 1, ny, A.periodic[1]);
+  const bool rowe = my >= 0, rowh = my >= 0 && gy < ny;
+  bool hv[4], ownv[4];
+  T fhx[4], fex[4];
+  int sxs[4];  // the x CPML side of each place (-1 none)
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    int x = xb + j;
+    int mxj = wrap_index(x, nx, A.periodic[0]);
+    hv[j] = rowh && mxj >= 0 && x < nx;
+    ownv[j] = hv[j] && w >= 1 && lane >= 1;
+    fhx[j] = mxj >= 0 ? A.fh[mxj] : T(0);
+    fex[j] = mxj >= 0 ? A.fe[mxj] : T(0);
+    sxs[j] = -1;
+    if (mxj >= 0 && !A.periodic[0]) {
+      if (mxj < A.low[0]) sxs[j] = 0;
+      else if (mxj >= nx - A.high[0]) sxs[j] = 1;
+    }
+  }
+  const bool any_x = (sxs[0] >= 0) | (sxs[1] >= 0) | (sxs[2] >= 0) | (sxs[3] >= 0);
+  const bool any_own = ownv[0] | ownv[1] | ownv[2] | ownv[3];
+  const T fhy = my >= 0 ? A.fh[nx + my] : T(0), fey = my >= 0 ? A.fe[nx + my] : T(0);
+  int sy = -1;
+  if (my >= 0 && !A.periodic[1]) {
+    if (my < A.low[1]) sy = 0;
+    else if (my >= ny - A.high[1]) sy = 1;
+  }
+  const long long rowoff = my >= 0 ? (long long)my * nx : 0;
+
+  // -- copies: warp w copies E's row w (and the last warp also row RW+1), H's row w and cb's row
+  // w-1 of a plane; lane l the chunks of its four places (lane 0 also the chunk after the row)
+  const int myp_last = wrap_index(y0 + RW, ny, A.periodic[1]);
+  auto issue = [&](int eslot, int ke, int hslot, int kh) {
+    // E(ke) rows into E slot `eslot` (ke < 0: zeros); H(kh), cb(kh) rows into HB slot `hslot`
+    T *E = sEs + (size_t)eslot * S::E_SLOT;
+    const T *dummy = A.e_in;
+#pragma unroll
+    for (int rsel = 0; rsel < 2; rsel++) {
+      if (rsel == 1 && w != WARPS - 1) break;
+      const int r = rsel == 0 ? w : RW + 1;
+      const int yrow = rsel == 0 ? my : myp_last;
+      const bool rok = yrow >= 0 && ke >= 0;
+      const long long base = (long long)ke * plane + (long long)(yrow < 0 ? 0 : yrow) * nx;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T *dst = E + ((size_t)c * ER + r) * EW + VEC * lane;
+        const bool ok = rok && mxb >= 0;
+        const T *src = ok ? A.e_in + c * N + base + mxb : dummy;
+#pragma unroll
+        for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
+        if (lane == 0) {
+          const bool oka = rok && mxa >= 0;
+          const T *srca = oka ? A.e_in + c * N + base + mxa : dummy;
+          T *dsta = E + ((size_t)c * ER + r) * EW + ROW;
+#pragma unroll
+          for (int q = 0; q < VEC / CH; q++) cp_async16(dsta + q * CH, srca + q * CH, oka);
+        }
+      }
+    }
+    if (hslot >= 0) {
+      T *H = sHB + (size_t)hslot * S::HB_SLOT;
+      const bool ok = my >= 0 && mxb >= 0 && kh >= 0;
+      const long long at = (long long)(kh < 0 ? 0 : kh) * plane + rowoff + (mxb < 0 ? 0 : mxb);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        T *dst = H + ((size_t)c * WARPS + w) * ROW + VEC * lane;
+        const T *src = ok ? A.h_in + c * N + at : dummy;
+#pragma unroll
+        for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
+      }
+      if (w >= 1) {
+        T *B = H + 3 * WARPS * ROW;
+        const bool okb = ok && gy < ny;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          T *dst = B + ((size_t)c * RW + (w - 1)) * ROW + VEC * lane;
+          const T *src = okb ? A.cb + c * N + at : dummy;
+#pragma unroll
+          for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, okb);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  auto Erow = [&](int slot, int c, int r) -> const T * {
+    return sEs + (size_t)slot * S::E_SLOT + ((size_t)c * ER + r) * EW;
+  };
+  auto Hrow = [&](int slot, int c) -> const T * {
+    return sHB + (size_t)slot * S::HB_SLOT + ((size_t)c * WARPS + w) * ROW;
+  };
+  auto Brow = [&](int slot, int c) -> const T * {
+    return sHB + (size_t)slot * S::HB_SLOT + 3 * WARPS * ROW + ((size_t)c * RW + (w - 1)) * ROW;
+  };
+
+  // H's new plane k at the lane's four places, from E(k) (E slot se), E(k+1) (slot se1), H(k)
+  // (HB slot sh): the forward differences, then the slabs along x, y, z
+  auto compute_h = [&](int se, int se1, int sh, int k, bool write, T hn[3][4]) {
+    const int kn = wrap_index(k + 1, nz, A.periodic[2]);
+    const T fhz = A.fh[nx + ny + k];
+    Vec4<T> e[3], eyp[2], ez1[2], ho[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      e[c] = ld4(Erow(se, c, w) + VEC * lane);
+      ho[c] = ld4(Hrow(sh, c) + VEC * lane);
+    }
+    eyp[0] = ld4(Erow(se, 0, w + 1) + VEC * lane);  // E_x, E_z of the row after
+    eyp[1] = ld4(Erow(se, 2, w + 1) + VEC * lane);
+    ez1[0] = ld4(Erow(se1, 0, w) + VEC * lane);     // E_x, E_y of the plane after
+    ez1[1] = ld4(Erow(se1, 1, w) + VEC * lane);
+    // +x of the fourth place: the next lane's first, lane 31 the chunk after the row
+    T ey_n = __shfl_down_sync(0xffffffffu, e[1].v[0], 1);
+    T ez_n = __shfl_down_sync(0xffffffffu, e[2].v[0], 1);
+    if (lane == 31) {
+      ey_n = Erow(se, 1, w)[ROW];
+      ez_n = Erow(se, 2, w)[ROW];
+    }
+    const bool yb = myp >= 0;   // the row after exists (or wraps)
+    const bool zb = kn >= 0;    // the plane after exists (or wraps)
+    T dyEz[4], dzEy[4], dzEx[4], dxEz[4], dxEy[4], dyEx[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      T eyn = j < 3 ? e[1].v[j + 1] : ey_n, ezn = j < 3 ? e[2].v[j + 1] : ez_n;
+      T exy = yb ? eyp[0].v[j] : T(0), ezy = yb ? eyp[1].v[j] : T(0);
+      T exz = zb ? ez1[0].v[j] : T(0), eyz = zb ? ez1[1].v[j] : T(0);
+      dyEz[j] = ezy - e[2].v[j];
+      dzEy[j] = eyz - e[1].v[j];
+      dzEx[j] = exz - e[0].v[j];
+      dxEz[j] = ezn - e[2].v[j];
+      dxEy[j] = eyn - e[1].v[j];
+      dyEx[j] = exy - e[0].v[j];
+      hn[0][j] = ho[0].v[j] - A.dt * (dyEz[j] * fhy - dzEy[j] * fhz);
+      hn[1][j] = ho[1].v[j] - A.dt * (dzEx[j] * fhz - dxEz[j] * fhx[j]);
+      hn[2][j] = ho[2].v[j] - A.dt * (dxEy[j] * fhx[j] - dyEx[j] * fhy);
+    }
+    // the CPML: H_x along y then z, H_y along x then z, H_z along x then y
+    const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
+    if (rowh && (zs | (sy >= 0) | any_x)) {
+      const bool ow = write && w >= 1 && lane >= 1;
+      const long long rowat = rowoff + (mxb < 0 ? 0 : mxb);
+      T zero4[4] = {T(0), T(0), T(0), T(0)};
+      if (sy >= 0 && mxb >= 0) {
+        SlabEntry s0 = A.slab[1][0][1][sy];
+        if (s0.count) {
+          int q = my - s0.from;
+          long long p = s0.psi + ((long long)k * s0.count + q) * nx + mxb;
+          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s0.coef + q],
+                      A.coefs[s0.coef + s0.count + q], A.step[1], T(1), dyEz, hn[0], zero4, ow);
+        }
+      }
+      if (zs && mxb >= 0) {
+        SlabEntry s0 = k < A.low[2] ? A.slab[1][0][2][0] : A.slab[1][0][2][1];
+        if (s0.count) {
+          int q = k - s0.from;
+          long long p = s0.psi + (long long)q * plane + rowat;
+          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s0.coef + q],
+                      A.coefs[s0.coef + s0.count + q], A.step[2], T(-1), dzEy, hn[0], zero4, ow);
+        }
+      }
+      if (any_x) {  // one place at a time: a slab along x is a few columns
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (sxs[j] >= 0 && hv[j]) {
+            SlabEntry s1 = A.slab[1][1][0][sxs[j]];
+            if (s1.count) hn[1][j] = slab_apply<T, 1>(A, s1, 1, 0, xb + j < 0 ? nx - VEC + j : (xb + j >= nx ? xb + j - nx : xb + j), my, k, dxEz[j], hn[1][j], T(0), ow && (j + VEC * lane) >= VEC);
+          }
+      }
+      if (zs && mxb >= 0) {
+        SlabEntry s1 = k < A.low[2] ? A.slab[1][1][2][0] : A.slab[1][1][2][1];
+        if (s1.count) {
+          int q = k - s1.from;
+          long long p = s1.psi + (long long)q * plane + rowat;
+          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s1.coef + q],
+                      A.coefs[s1.coef + s1.count + q], A.step[2], T(1), dzEx, hn[1], zero4, ow);
+        }
+      }
+      if (any_x) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (sxs[j] >= 0 && hv[j]) {
+            SlabEntry s2 = A.slab[1][2][0][sxs[j]];
+            if (s2.count) hn[2][j] = slab_apply<T, 1>(A, s2, 2, 0, xb + j < 0 ? nx - VEC + j : (xb + j >= nx ? xb + j - nx : xb + j), my, k, dxEy[j], hn[2][j], T(0), ow && (j + VEC * lane) >= VEC);
+          }
+      }
+      if (sy >= 0 && mxb >= 0) {
+        SlabEntry s2 = A.slab[1][2][1][sy];
+        if (s2.count) {
+          int q = my - s2.from;
+          long long p = s2.psi + ((long long)k * s2.count + q) * nx + mxb;
+          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s2.coef + q],
+                      A.coefs[s2.coef + s2.count + q], A.step[1], T(-1), dyEx, hn[2], zero4, ow);
+        }
+      }
+    }
+    // beyond a wall H is zero (E's back differences read zero there)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (!hv[j]) hn[0][j] = hn[1][j] = hn[2][j] = T(0);
+    // the magnetic currents at this tile and plane, each value's entries in CPU order
+    const int bucket = tile * nz + k;
+    const int g0 = A.hbucket[bucket], g1 = A.hbucket[bucket + 1];
+    for (int g = g0; g < g1; g++) {
+      Group gr = A.hgroups[g];
+      const int gw = gr.local / ROW, gi = gr.local % ROW;
+      if (gw == w && (gi >> 2) == lane) {
+        const int jj = gi & 3;
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (gr.comp == c && jj == j) {
+              T v = hn[c][j];
+              for (int q = gr.first; q < gr.first + gr.count; q++) {
+                Entry en = A.entries[q];
+                double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
+                if (sizeof(T) == 8) v = v - (T)((double)A.dt * amount);
+                else v = v - A.dt * (T)amount;
+              }
+              hn[c][j] = v;
+            }
+      }
+    }
+  };
+
+  T hn[3][4], hprev[2][4];
+  // prologue: H's new plane kbeg-1 (wrapped on a periodic z)
+  const int km = wrap_index(kbeg - 1, nz, A.periodic[2]);
+  // positions: E slots by position p = plane - kbeg + 1 (km at 0), HB slots alike
+  issue(0, km, 0, km);                                   // E(km), H(km), cb(km)
+  issue(1, kbeg, -1, -1);                                // E(kbeg)
+  if (km >= 0) {
+    cp_async_wait<0>();
+    __syncthreads();
+    compute_h(0, 1, 0, km, false, hn);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      hprev[0][j] = hn[0][j];
+      hprev[1][j] = hn[1][j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; j++) hprev[0][j] = hprev[1][j] = T(0);
+  }
+  __syncthreads();
+  // plane kbeg's H and cb, and E(kbeg+1)
+  issue(2, wrap_index(kbeg + 1, nz, A.periodic[2]), 1, kbeg);
+  for (int k = kbeg; k < kend; k++) {
+    const int p = k - kbeg + 1;
+    const int se = p % 3, se1 = (p + 1) % 3, sh = p % 2;
+    cp_async_wait<0>();
+    __syncthreads();  // plane k's rows landed; every warp is done with plane k-1
+    if (k + 1 < kend) issue((p + 2) % 3, wrap_index(k + 2, nz, A.periodic[2]), (p + 1) % 2, k + 1);
+    compute_h(se, se1, sh, k, true, hn);
+    // H's tile to memory, H_x and H_z to the row below
+    const long long at = (long long)k * plane + rowoff + (mxb < 0 ? 0 : mxb);
+    if (w >= 1 && lane >= 1 && rowh && mxb >= 0 && xb < nx) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        Vec4<T> o;
+#pragma unroll
+        for (int j = 0; j < 4; j++) o.v[j] = hn[c][j];
+        st4(A.h_out + c * N + at, o);
+      }
+    }
+    {
+      Vec4<T> a, b;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        a.v[j] = hn[0][j];
+        b.v[j] = hn[2][j];
+      }
+      st4(sX + (size_t)w * ROW + VEC * lane, a);
+      st4(sX + (size_t)(WARPS + w) * ROW + VEC * lane, b);
+    }
+    __syncthreads();
+    // E's plane k at the owned places: back differences, then the slabs
+    const T fez = A.fe[nx + ny + k];
+    const bool zb = wrap_index(k - 1, nz, A.periodic[2]) >= 0;
+    const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
+    T en[3][4];
+    if (w >= 1) {
+      Vec4<T> e[3], cb[3], ca[3], hxm, hzm;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        e[c] = ld4(Erow(se, c, w) + VEC * lane);
+        cb[c] = ld4(Brow(sh, c) + VEC * lane);
+        if (LOSSY && any_own) ca[c] = ld4(A.ca + c * N + at);
+      }
+      hxm = ld4(sX + (size_t)(w - 1) * ROW + VEC * lane);  // the row before
+      hzm = ld4(sX + (size_t)(WARPS + w - 1) * ROW + VEC * lane);
+      // -x of the first place: the previous lane's fourth
+      T hz_p = __shfl_up_sync(0xffffffffu, hn[2][3], 1);
+      T hy_p = __shfl_up_sync(0xffffffffu, hn[1][3], 1);
+      T dyHz[4], dzHy[4], dzHx[4], dxHz[4], dxHy[4], dyHx[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        T hzx = j > 0 ? hn[2][j - 1] : hz_p, hyx = j > 0 ? hn[1][j - 1] : hy_p;
+        T hyz = zb ? hprev[1][j] : T(0), hxz = zb ? hprev[0][j] : T(0);
+        dyHz[j] = hn[2][j] - hzm.v[j];
+        dzHy[j] = hn[1][j] - hyz;
+        dzHx[j] = hn[0][j] - hxz;
+        dxHz[j] = hn[2][j] - hzx;
+        dxHy[j] = hn[1][j] - hyx;
+        dyHx[j] = hn[0][j] - hxm.v[j];
+        T curl0 = dyHz[j] * fey - dzHy[j] * fez;
+        T curl1 = dzHx[j] * fez - dxHz[j] * fex[j];
+        T curl2 = dxHy[j] * fex[j] - dyHx[j] * fey;
+        T cav[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) cav[c] = LOSSY ? ca[c].v[j] : (cb[c].v[j] == T(0) ? T(0) : T(1));
+        en[0][j] = cav[0] * e[0].v[j] + cb[0].v[j] * curl0;
+        en[1][j] = cav[1] * e[1].v[j] + cb[1].v[j] * curl1;
+        en[2][j] = cav[2] * e[2].v[j] + cb[2].v[j] * curl2;
+      }
+      // the CPML: E_x along y then z, E_y along x then z, E_z along x then y
+      if (any_own && (zs | (sy >= 0) | any_x)) {
+        T cbx[4], cby[4], cbz[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          cbx[j] = cb[0].v[j];
+          cby[j] = cb[1].v[j];
+          cbz[j] = cb[2].v[j];
+        }
+        const long long rowat = rowoff + mxb;
+        if (sy >= 0) {
+          SlabEntry s0 = A.slab[0][0][1][sy];
+          if (s0.count) {
+            int q = my - s0.from;
+            long long p2 = s0.psi + ((long long)k * s0.count + q) * nx + mxb;
+            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s0.coef + q],
+                        A.coefs[s0.coef + s0.count + q], A.step[1], T(1), dyHz, en[0], cbx, true);
+          }
+        }
+        if (zs) {
+          SlabEntry s0 = k < A.low[2] ? A.slab[0][0][2][0] : A.slab[0][0][2][1];
+          if (s0.count) {
+            int q = k - s0.from;
+            long long p2 = s0.psi + (long long)q * plane + rowat;
+            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s0.coef + q],
+                        A.coefs[s0.coef + s0.count + q], A.step[2], T(-1), dzHy, en[0], cbx, true);
+          }
+        }
+        if (any_x) {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (sxs[j] >= 0 && ownv[j]) {
+              SlabEntry s1 = A.slab[0][1][0][sxs[j]];
+              if (s1.count) en[1][j] = slab_apply<T, 0>(A, s1, 1, 0, xb + j, my, k, dxHz[j], en[1][j], cby[j], true);
+            }
+        }
+        if (zs) {
+          SlabEntry s1 = k < A.low[2] ? A.slab[0][1][2][0] : A.slab[0][1][2][1];
+          if (s1.count) {
+            int q = k - s1.from;
+            long long p2 = s1.psi + (long long)q * plane + rowat;
+            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s1.coef + q],
+                        A.coefs[s1.coef + s1.count + q], A.step[2], T(1), dzHx, en[1], cby, true);
+          }
+        }
+        if (any_x) {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (sxs[j] >= 0 && ownv[j]) {
+              SlabEntry s2 = A.slab[0][2][0][sxs[j]];
+              if (s2.count) en[2][j] = slab_apply<T, 0>(A, s2, 2, 0, xb + j, my, k, dxHy[j], en[2][j], cbz[j], true);
+            }
+        }
+        if (sy >= 0) {
+          SlabEntry s2 = A.slab[0][2][1][sy];
+          if (s2.count) {
+            int q = my - s2.from;
+            long long p2 = s2.psi + ((long long)k * s2.count + q) * nx + mxb;
+            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s2.coef + q],
+                        A.coefs[s2.coef + s2.count + q], A.step[1], T(-1), dyHx, en[2], cbz, true);
+          }
+        }
+      }
+      // the electric currents (src/fdtd.rs:1375-1387)
+      const int bucket = tile * nz + k;
+      const int g0 = A.ebucket[bucket], g1 = A.ebucket[bucket + 1];
+      for (int g = g0; g < g1; g++) {
+        Group gr = A.egroups[g];
+        const int gw = gr.local / ROW, gi = gr.local % ROW;
+        if (gw == w && (gi >> 2) == lane) {
+          const int jj = gi & 3;
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+              if (gr.comp == c && jj == j) {
+                T v = en[c][j];
+                const T cbv = cb[c].v[j];
+                for (int q = gr.first; q < gr.first + gr.count; q++) {
+                  Entry e2 = A.entries[q];
+                  double amount = e2.are * A.waves_e[2 * e2.emitter] - e2.aim * A.waves_e[2 * e2.emitter + 1];
+                  if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
+                  else v = v - cbv * (T)amount;
+                }
+                en[c][j] = v;
+              }
+        }
+      }
+      if (MEDIA && any_own) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            if (!ownv[j]) continue;
+            int mi = A.media.member[c * N + at + j];
+            if (mi < 0) continue;
+            const MediaArgs<T> &M = A.media;
+            int g = M.group[mi];
+            int np = M.gpoles[g];
+            T before = M.before[mi];
+            T rest = M.gchi[g] * before;
+            const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+            T *cur = M.current + (long long)mi * M.maxpoles;
+            T *prev = M.previous + (long long)mi * M.maxpoles;
+            for (int q = 0; q < np; q++)
+              rest = rest - T(0.5) * ((pl[3 * q] + T(1)) * cur[q] + pl[3 * q + 1] * prev[q]);
+            T next = en[c][j] + M.scale[mi] * rest;
+            T slope = (next - before) / M.two_dt;
+            for (int q = 0; q < np; q++) {
+              T jn = pl[3 * q] * cur[q] + pl[3 * q + 1] * prev[q] + pl[3 * q + 2] * slope;
+              prev[q] = cur[q];
+              cur[q] = jn;
+            }
+            M.before[mi] = e[c].v[j];
+            en[c][j] = next;
+          }
+      }
+      if (lane >= 1 && rowh && mxb >= 0 && xb < nx) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          Vec4<T> o;
+#pragma unroll
+          for (int j = 0; j < 4; j++) o.v[j] = en[c][j];
+          st4(A.e_out + c * N + at, o);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      hprev[0][j] = hn[0][j];
+      hprev[1][j] = hn[1][j];
+    }
+  }
+  cp_async_wait<0>();
+}
+
 // The waveforms of a batch of steps, in f64 (src/fdtd.rs:329-423): for step m of the batch, w
 // at H's time t = (first+m) dt and at E's t + dt/2, 2 doubles each per emitter.
 struct Wave {
@@ -546,6 +1879,15 @@ struct fdtd_ctx {
   SlabEntry table[2][3][3][2];
   // launch shape
   int tiles_x, tiles_y, zchunk, zchunks;
+  int sms = 148;
+  bool staged = false;  // the staged kernel (nx a multiple of 16 bytes' worth of values)
+  bool row = false;     // the row kernel
+  bool quad = false;    // the quad kernel (the default where nx is a multiple of 4)
+  // a tile's owned values along x and y, and how a source's place is numbered in its tile: over
+  // rows `loc_w` wide from (x0 - loc_x, y0 - 1), E too unless `e_tile` (then over the tile)
+  int tile_w = TX, tile_h = TY, loc_w = TX + 1, loc_x = 1;
+  bool e_tile = true;
+  int staged_per_sm[2][2][2] = {{{0, 0}, {0, 0}}, {{0, 0}, {0, 0}}};
   // sources
   int nwaves = 0;
   Wave *d_waves = nullptr;
@@ -711,15 +2053,72 @@ StepArgs<T> step_args(fdtd_ctx *c) {
   return A;
 }
 
+template <typename T, bool LOSSY, bool MEDIA, int STAGES>
+void launch_staged(fdtd_ctx *c, const StepArgs<T> &A) {
+  auto kernel = staged_kernel<T, LOSSY, MEDIA, STAGES>;
+  const size_t smem = staged_smem_bytes<T, STAGES>();
+  int &per_sm = c->staged_per_sm[sizeof(T) == 8][LOSSY][MEDIA];
+  if (per_sm == 0) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, smem);
+    if (per_sm < 1) per_sm = 1;
+  }
+  long long total = (long long)c->tiles_x * c->tiles_y * c->n[2];
+  int ctas = (int)std::min<long long>(total, (long long)per_sm * c->sms);
+  kernel<<<ctas, NT, smem, c->stream>>>(A, total, ctas);
+}
+
 template <typename T>
 void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
+  if (c->quad) {
+    dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
+    const size_t smem = quad::Smem<T>::BYTES;
+    auto go = [&](auto kernel) {
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      kernel<<<grid, quad::THREADS, smem, c->stream>>>(A);
+    };
+    if (c->media) {
+      if (c->lossless) go(quad_kernel<T, false, true>);
+      else go(quad_kernel<T, true, true>);
+    } else {
+      if (c->lossless) go(quad_kernel<T, false, false>);
+      else go(quad_kernel<T, true, false>);
+    }
+    return;
+  }
+  if (c->row) {
+    dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
+    if (c->media) {
+      if (c->lossless) row_kernel<T, false, true><<<grid, rowstep::THREADS, 0, c->stream>>>(A);
+      else row_kernel<T, true, true><<<grid, rowstep::THREADS, 0, c->stream>>>(A);
+    } else {
+      if (c->lossless) row_kernel<T, false, false><<<grid, rowstep::THREADS, 0, c->stream>>>(A);
+      else row_kernel<T, true, false><<<grid, rowstep::THREADS, 0, c->stream>>>(A);
+    }
+    return;
+  }
+  if (c->staged) {
+    if (c->media) {
+      if (c->lossless) launch_staged<T, false, true, 3>(c, A);
+      else launch_staged<T, true, true, 3>(c, A);
+    } else {
+      if (c->lossless) launch_staged<T, false, false, 3>(c, A);
+      else launch_staged<T, true, false, 3>(c, A);
+    }
+    return;
+  }
   dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
+  const size_t smem = plain_smem_bytes<T>();
+  auto go = [&](auto kernel) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid, NT, smem, c->stream>>>(A);
+  };
   if (c->media) {
-    if (c->lossless) step_kernel<T, false, true><<<grid, NT, 0, c->stream>>>(A);
-    else step_kernel<T, true, true><<<grid, NT, 0, c->stream>>>(A);
+    if (c->lossless) go(step_kernel<T, false, true>);
+    else go(step_kernel<T, true, true>);
   } else {
-    if (c->lossless) step_kernel<T, false, false><<<grid, NT, 0, c->stream>>>(A);
-    else step_kernel<T, true, false><<<grid, NT, 0, c->stream>>>(A);
+    if (c->lossless) go(step_kernel<T, false, false>);
+    else go(step_kernel<T, true, false>);
   }
 }
 
@@ -884,8 +2283,11 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
     d.count = sl.count;
     d.size = sl.count * (N / c->n[w]);
     d.coef = (long long)coefs.size();
-    d.psi = field == 1 ? c->psi_h_len : c->psi_e_len;
-    (field == 1 ? c->psi_h_len : c->psi_e_len) += d.size;
+    // each slab's psi starts on a 16-element boundary, so a row of four values is one aligned
+    // vector in f32 and two in f64
+    long long &len = field == 1 ? c->psi_h_len : c->psi_e_len;
+    d.psi = (len + 15) / 16 * 16;
+    len = d.psi + d.size;
     for (long long q = 0; q < sl.count; q++) coefs.push_back(sl.b[q]);
     for (long long q = 0; q < sl.count; q++) coefs.push_back(sl.a[q]);
     c->slabs.push_back(d);
@@ -913,9 +2315,39 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
+  c->sms = sms;
+  {
+    const char *force = getenv("PHOTONOXIDE_FDTD_KERNEL");
+    std::string kind = force ? force : (c->n[0] % 4 == 0 ? "quad" : "row");
+    if (kind == "quad" && c->n[0] % 4 != 0) kind = "row";
+    c->quad = kind == "quad";
+    c->row = kind == "row";
+    c->staged = kind == "staged" && (c->n[0] % (16 / (int)c->elem) == 0);
+  }
+  if (c->row) {
+    c->tile_w = rowstep::OWN;
+    c->tile_h = rowstep::RW;
+    c->loc_w = rowstep::SEG;
+    c->loc_x = 1;
+    c->e_tile = false;
+  } else if (c->quad) {
+    c->tile_w = quad::OWNX;
+    c->tile_h = quad::RW;
+    c->loc_w = quad::ROW;
+    c->loc_x = quad::VEC;
+    c->e_tile = false;
+  }
+  c->tiles_x = (c->n[0] + c->tile_w - 1) / c->tile_w;
+  c->tiles_y = (c->n[1] + c->tile_h - 1) / c->tile_h;
   long long tiles = (long long)c->tiles_x * c->tiles_y;
-  long long want = 8LL * sms;
-  int chunks = (int)std::min<long long>(c->n[2], std::max<long long>(1, (want + tiles - 1) / tiles));
+  // z cut into runs so that the CTAs fill the device at least twice over (the scheduler then
+  // balances them), each run at least 16 planes long (each run recomputes one plane of H)
+  long long want = 2LL * 3 * sms;
+  int chunks = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
+  chunks = std::min(chunks, std::max(1, c->n[2] / 16));
+  const char *zc = getenv("PHOTONOXIDE_FDTD_ZCHUNKS");
+  if (zc) chunks = std::max(1, atoi(zc));
+  chunks = std::min(chunks, c->n[2]);
   c->zchunk = (c->n[2] + chunks - 1) / chunks;
   c->zchunks = (c->n[2] + c->zchunk - 1) / c->zchunk;
   if (int r = empty_sources(c)) return r;
@@ -1036,7 +2468,10 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
       int comp = (int)(places[g] / c->N);
       long long r = places[g] % c->N;
       int i = (int)(r % nx), j = (int)((r / nx) % ny), k = (int)(r / ((long long)nx * ny));
-      int tx = i / TX, ty = j / TY;
+      const int tw = c->tile_w, th = c->tile_h;
+      // a place's number in its tile (see fdtd_ctx::loc_w)
+      const int hw = c->loc_w, lx0 = c->loc_x;
+      int tx = i / tw, ty = j / th;
       auto push = [&](int ttx, int tty, int lx, int ly, int width) {
         Item it;
         it.key = ((long long)(tty * c->tiles_x + ttx)) * nz + k;
@@ -1046,19 +2481,20 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
         per_field[f].push_back(it);
       };
       if (f == 0) {
-        push(tx, ty, i - tx * TX, j - ty * TY, TX);
+        if (!c->e_tile) push(tx, ty, i - tx * tw + lx0, j - ty * th + 1, hw);
+        else push(tx, ty, i - tx * tw, j - ty * th, TX);
       } else {
-        push(tx, ty, i - tx * TX + 1, j - ty * TY + 1, HX);
+        push(tx, ty, i - tx * tw + lx0, j - ty * th + 1, hw);
         // the tiles whose low halo this value is: next along x, next along y (wrapping on a
         // periodic axis), and the diagonal one
-        int txn = -1, tyn = -1, lxn = 0, lyn = 0;
-        if (i == (tx + 1) * TX - 1 && (tx + 1) < c->tiles_x) { txn = tx + 1; lxn = 0; }
-        if (c->periodic[0] && i == nx - 1 && c->tiles_x > 0) { txn = 0; lxn = 0; }
-        if (j == (ty + 1) * TY - 1 && (ty + 1) < c->tiles_y) { tyn = ty + 1; lyn = 0; }
-        if (c->periodic[1] && j == ny - 1 && c->tiles_y > 0) { tyn = 0; lyn = 0; }
-        if (txn >= 0) push(txn, ty, lxn, j - ty * TY + 1, HX);
-        if (tyn >= 0) push(tx, tyn, i - tx * TX + 1, lyn, HX);
-        if (txn >= 0 && tyn >= 0) push(txn, tyn, lxn, lyn, HX);
+        int txn = -1, tyn = -1;
+        if (i == (tx + 1) * tw - 1 && (tx + 1) < c->tiles_x) txn = tx + 1;
+        if (c->periodic[0] && i == nx - 1) txn = 0;
+        if (j == (ty + 1) * th - 1 && (ty + 1) < c->tiles_y) tyn = ty + 1;
+        if (c->periodic[1] && j == ny - 1) tyn = 0;
+        if (txn >= 0) push(txn, ty, lx0 - 1, j - ty * th + 1, hw);
+        if (tyn >= 0) push(tx, tyn, i - tx * tw + lx0, 0, hw);
+        if (txn >= 0 && tyn >= 0) push(txn, tyn, lx0 - 1, 0, hw);
       }
     }
   }

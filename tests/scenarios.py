@@ -23,17 +23,17 @@ def pulse() -> Waveform:
     return Waveform.pulse(1.0, 0.6)
 
 
-def busy(make, two_d: bool, sources: bool = True, scale: float = 0.01):
+def busy(make, two_d: bool, sources: bool = True, scale: float = 0.01, n=None):
     """A dielectric block and a lossy one, a conductor, CPMLs with kappa and alpha, a wall and (in
     2D) periodic sides, random fields, point sources on E and H, a current sharing a value with
     one, a dipole, probes, a transform box and a flux box (3D) or plane (2D). 3D: 37 x 21 x 19
     cells of 50 nm, sizes that leave tiles part-filled."""
     if two_d:
         b = Boundaries(Periodic(), Pml(6, 6), Periodic(), Cpml(kappa=2.0, alpha=0.3))
-        g = Grid3d.centred((70, 45, 1), 0.05)
+        g = Grid3d.centred(n or (70, 45, 1), 0.05)
     else:
         b = Boundaries(Pml(4, 5), Pml(4, 0), Pml(3, 3), Cpml(kappa=3.0, alpha=0.2))
-        g = Grid3d.centred((37, 21, 19), 0.05)
+        g = Grid3d.centred(n or (37, 21, 19), 0.05)
     eps = Boxes(1.0).add((-0.3, -0.2, -INF), (0.3, 0.2, INF), 12.0)
     s = make(g, eps, b, 0.9)
     s.with_conductivity(Boxes(0.0).add((0.6, 0.3, -INF), (INF, INF, INF), 2.0))

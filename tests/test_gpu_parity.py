@@ -32,11 +32,17 @@ def fields(s):
     return [s.e(c) for c in range(3)] + [s.h(c) for c in range(3)]
 
 
+# grid sizes: 33 along x takes the plain kernel; 36 and 68 (multiples of 4) the staged one, with
+# partial tiles along x and y, and several tiles and planes split among CTAs
+SIZES = [(33, 18, 11), (36, 18, 11), (68, 35, 12)]
+
+
 @pytest.mark.parametrize("precision", [32, 64])
 @pytest.mark.parametrize("periodic", [(), (0,), (1,), (2,), (0, 1), (0, 1, 2)])
-def test_stirred_bit_for_bit(precision, periodic):
-    p = stirred(lambda *a: Simulation(*a, precision=precision), periodic_axes=periodic)
-    o = stirred(lambda *a: OracleSimulation(*a, precision=precision), periodic_axes=periodic)
+@pytest.mark.parametrize("n", SIZES)
+def test_stirred_bit_for_bit(precision, periodic, n):
+    p = stirred(lambda *a: Simulation(*a, precision=precision), periodic_axes=periodic, n=n)
+    o = stirred(lambda *a: OracleSimulation(*a, precision=precision), periodic_axes=periodic, n=n)
     p.run(37)
     o.run(37)
     for c, (x, y) in enumerate(zip(fields(p), fields(o))):
@@ -72,10 +78,11 @@ def test_closed_box_f32_bit_for_bit_over_300_steps():
 
 
 @pytest.mark.parametrize("precision", [64, 32])
-@pytest.mark.parametrize("two_d", [False, True])
-def test_busy_bit_for_bit(two_d, precision):
-    p = busy(lambda *a: Simulation(*a, precision=precision), two_d)
-    o = busy(lambda *a: OracleSimulation(*a, precision=precision), two_d)
+@pytest.mark.parametrize("two_d,n", [(False, None), (True, None), (False, (40, 21, 19)),
+                                     (True, (72, 45, 1)), (False, (96, 37, 14))])
+def test_busy_bit_for_bit(two_d, n, precision):
+    p = busy(lambda *a: Simulation(*a, precision=precision), two_d, n=n)
+    o = busy(lambda *a: OracleSimulation(*a, precision=precision), two_d, n=n)
     p.run(800)
     o.run(800)
     for c, (x, y) in enumerate(zip(fields(p), fields(o))):
@@ -88,13 +95,18 @@ def test_busy_bit_for_bit(two_d, precision):
 
 @pytest.mark.parametrize("two_d", [False, True])
 def test_busy_f32_within_the_reference_tolerance(two_d):
+    """The reference's Agreement (src/fdtd/gpu/checks.rs:148-205): every output of each kind
+    together, E and H of all components, all probes, all transforms, all fluxes, each kind's
+    largest difference relative to its largest value; within 2e-5 after 800 steps."""
     p = busy(lambda *a: Simulation(*a, precision=32), two_d)
     o = busy(lambda *a: OracleSimulation(*a, precision=64), two_d)
     p.run(800)
     o.run(800)
-    for x, y in zip(fields(p), fields(o)):
-        assert relative(x, y) < 2e-5
+    assert relative(np.concatenate(fields(p)), np.concatenate(fields(o))) < 2e-5
+    assert relative(np.concatenate([p.probe(n) for n in range(6)]),
+                    np.concatenate([o.probe(n) for n in range(6)])) < 2e-5
     assert relative(p.transforms(), o.transforms()) < 2e-5
+    assert relative(p.flux(0), o.flux(0)) < 2e-5
 
 
 def test_runs_in_pieces_give_the_same_bits():
@@ -112,3 +124,17 @@ def test_runs_in_pieces_give_the_same_bits():
         assert np.array_equal(x, y) and np.array_equal(x, z)
     assert np.array_equal(a.transforms(), b.transforms())
     assert np.array_equal(a.probe(3), b.probe(3))
+
+
+@pytest.mark.parametrize("kind", ["plain", "staged", "row"])
+def test_every_kernel_gives_the_same_bits(kind, monkeypatch):
+    """The same grid (nx a multiple of 4, partial tiles) stepped by the default kernel and,
+    forced, by each other one: the same bits, fields and transforms."""
+    default = busy(lambda *a: Simulation(*a), False, n=(40, 21, 19))
+    monkeypatch.setenv("PHOTONOXIDE_FDTD_KERNEL", kind)
+    other = busy(lambda *a: Simulation(*a), False, n=(40, 21, 19))
+    default.run(300)
+    other.run(300)
+    for x, y in zip(fields(default), fields(other)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(default.transforms(), other.transforms())
