@@ -45,6 +45,9 @@ struct SlabEntry {
   int from, count;  // count 0: no slab
   long long psi;    // where its psi starts
   int coef;         // where its b starts (a follows after count)
+  // along x, psi's rows start at pf = from rounded down to a multiple of 4 and are pw values
+  // wide, a multiple of 4, so four places are one aligned vector (along y and z: from, count)
+  int pf, pw;
 };
 
 // A value the sources add to, with its entries (emitter, amplitude) in CPU order.
@@ -143,7 +146,7 @@ __device__ inline T slab_update(const StepArgs<T> &A, const SlabEntry *s, int c,
   int q = m - s->from;
   int li = i, lj = j, lk = k;
   int dx = A.n[0], dy = A.n[1];
-  if (w == 0) { li = q; dx = s->count; }
+  if (w == 0) { li = i - s->pf; dx = s->pw; }
   else if (w == 1) { lj = q; dy = s->count; }
   else lk = q;
   long long p = s->psi + ((long long)lk * dy + lj) * dx + li;
@@ -747,7 +750,7 @@ __device__ __forceinline__ T slab_apply(const StepArgs<T> &A, const SlabEntry s,
   int q = m - s.from;
   int li = i, lj = j, lk = k;
   int dx = A.n[0], dy = A.n[1];
-  if (w == 0) { li = q; dx = s.count; }
+  if (w == 0) { li = i - s.pf; dx = s.pw; }
   else if (w == 1) { lj = q; dy = s.count; }
   else lk = q;
   long long p = s.psi + ((long long)lk * dy + lj) * dx + li;
@@ -1231,6 +1234,99 @@ __device__ __forceinline__ void slab4(const StepArgs<T> &A, T *psi_out, const T 
   if (write) st4(psi_out, nw);
 }
 
+// slab4 with the psi row already read
+template <typename T, int FIELD>
+__device__ __forceinline__ void slab4_loaded(const StepArgs<T> &A, T *psi_out, const Vec4<T> &old,
+                                             const SlabEntry &s, int q, T hstep, T sign,
+                                             const T diff[4], T v[4], const T cbv[4], bool write) {
+  const T b = A.coefs[s.coef + q], a = A.coefs[s.coef + s.count + q];
+  Vec4<T> nw;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    T d = diff[j] / hstep;
+    nw.v[j] = b * old.v[j] + a * d;
+    T u = sign * nw.v[j];
+    if (FIELD == 1) v[j] = v[j] - A.dt * u;
+    else v[j] = v[j] + cbv[j] * u;
+  }
+  if (write) st4(psi_out, nw);
+}
+
+// The same along x, where each place has its own coefficients and only the places `in` the slab
+// change (the psi row is padded to whole vectors; the other places keep their psi).
+template <typename T, int FIELD>
+__device__ __forceinline__ void slab4x(const StepArgs<T> &A, const SlabEntry &s, T *psi_out,
+                                       const Vec4<T> &old, int x, const bool in[4], T sign,
+                                       const T diff[4], T v[4], const T cbv[4], bool write) {
+  Vec4<T> nw;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    nw.v[j] = old.v[j];
+    if (in[j]) {
+      const int q = x + j - s.from;
+      T d = diff[j] / A.step[0];
+      nw.v[j] = A.coefs[s.coef + q] * old.v[j] + A.coefs[s.coef + s.count + q] * d;
+      T u = sign * nw.v[j];
+      if (FIELD == 1) v[j] = v[j] - A.dt * u;
+      else v[j] = v[j] + cbv[j] * u;
+    }
+  }
+  if (write) st4(psi_out, nw);
+}
+
+// The CPML of one field at a lane's four places: each slab's psi read first, then the slabs in
+// the reference's order for each component (src/fdtd/kernel.rs:525-579: along x, y, z).
+template <typename T, int FIELD>
+__device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int mxb, int sx,
+                                      bool xmixed, const bool inx[4], bool zs, int sy, bool write,
+                                      T v[3][4], const T diff[3][3][4], const T cbv[3][4],
+                                      bool xdiv_fallback_ok) {
+  const int nx = A.n[0], ny = A.n[1];
+  const long long plane = (long long)nx * ny;
+  const long long rowat = (long long)my * nx + mxb;
+  const T *pin = FIELD == 1 ? A.psi_h_in : A.psi_e;
+  T *pout = FIELD == 1 ? A.psi_h_out : A.psi_e;
+  // the slabs: c = 0 along y (+) and z (-); c = 1 along x (-) and z (+); c = 2 along x (+) and y (-)
+  SlabEntry sy0{}, sz0{}, sx1{}, sz1{}, sx2{}, sy2{};
+  Vec4<T> py0, pz0, px1, pz1, px2, py2;
+  long long ay0 = 0, az0 = 0, ax1 = 0, az1 = 0, ax2 = 0, ay2 = 0;
+  if (sy >= 0) {
+    sy0 = A.slab[FIELD][0][1][sy];
+    sy2 = A.slab[FIELD][2][1][sy];
+    if (sy0.count) { ay0 = sy0.psi + ((long long)k * sy0.count + (my - sy0.from)) * nx + mxb; py0 = ld4(pin + ay0); }
+    if (sy2.count) { ay2 = sy2.psi + ((long long)k * sy2.count + (my - sy2.from)) * nx + mxb; py2 = ld4(pin + ay2); }
+  }
+  if (zs) {
+    const int side = k < A.low[2] ? 0 : 1;
+    sz0 = A.slab[FIELD][0][2][side];
+    sz1 = A.slab[FIELD][1][2][side];
+    if (sz0.count) { az0 = sz0.psi + (long long)(k - sz0.from) * plane + rowat; pz0 = ld4(pin + az0); }
+    if (sz1.count) { az1 = sz1.psi + (long long)(k - sz1.from) * plane + rowat; pz1 = ld4(pin + az1); }
+  }
+  if (sx >= 0 && !xmixed) {
+    sx1 = A.slab[FIELD][1][0][sx];
+    sx2 = A.slab[FIELD][2][0][sx];
+    const long long rx = ((long long)k * ny + my);
+    if (sx1.count) { ax1 = sx1.psi + rx * sx1.pw + (mxb - sx1.pf); px1 = ld4(pin + ax1); }
+    if (sx2.count) { ax2 = sx2.psi + rx * sx2.pw + (mxb - sx2.pf); px2 = ld4(pin + ax2); }
+  }
+  const T one = T(1), minus = T(-1);
+  const T zero4[4] = {T(0), T(0), T(0), T(0)};
+  const T *cb0 = FIELD == 1 ? zero4 : cbv[0];
+  const T *cb1 = FIELD == 1 ? zero4 : cbv[1];
+  const T *cb2 = FIELD == 1 ? zero4 : cbv[2];
+  // component x: y then z
+  if (sy0.count) slab4_loaded<T, FIELD>(A, pout + ay0, py0, sy0, my - sy0.from, A.step[1], one, diff[0][1], v[0], cb0, write);
+  if (sz0.count) slab4_loaded<T, FIELD>(A, pout + az0, pz0, sz0, k - sz0.from, A.step[2], minus, diff[0][2], v[0], cb0, write);
+  // component y: x then z
+  if (sx1.count) slab4x<T, FIELD>(A, sx1, pout + ax1, px1, mxb, inx, minus, diff[1][0], v[1], cb1, write);
+  if (sz1.count) slab4_loaded<T, FIELD>(A, pout + az1, pz1, sz1, k - sz1.from, A.step[2], one, diff[1][2], v[1], cb1, write);
+  // component z: x then y
+  if (sx2.count) slab4x<T, FIELD>(A, sx2, pout + ax2, px2, mxb, inx, one, diff[2][0], v[2], cb2, write);
+  if (sy2.count) slab4_loaded<T, FIELD>(A, pout + ay2, py2, sy2, my - sy2.from, A.step[1], minus, diff[2][1], v[2], cb2, write);
+  (void)xdiv_fallback_ok;
+}
+
 template <typename T, bool LOSSY, bool MEDIA>
 __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   using namespace quad;
@@ -1281,6 +1377,18 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
   }
   const bool any_x = (sxs[0] >= 0) | (sxs[1] >= 0) | (sxs[2] >= 0) | (sxs[3] >= 0);
+  // the lane's x-slab side, and whether its places touch both sides (then one place at a time)
+  int sxl = -1;
+  bool xmixed = false;
+  bool inx[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    inx[j] = sxs[j] >= 0;
+    if (sxs[j] >= 0) {
+      if (sxl >= 0 && sxl != sxs[j]) xmixed = true;
+      sxl = sxs[j];
+    }
+  }
   const bool any_own = ownv[0] | ownv[1] | ownv[2] | ownv[3];
   const T fhy = my >= 0 ? A.fh[nx + my] : T(0), fey = my >= 0 ? A.fe[nx + my] : T(0);
   int sy = -1;
@@ -1397,62 +1505,14 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
     // the CPML: H_x along y then z, H_y along x then z, H_z along x then y
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
-    if (rowh && (zs | (sy >= 0) | any_x)) {
+    if (rowh && mxb >= 0 && (zs | (sy >= 0) | any_x)) {
       const bool ow = write && w >= 1 && lane >= 1;
-      const long long rowat = rowoff + (mxb < 0 ? 0 : mxb);
-      T zero4[4] = {T(0), T(0), T(0), T(0)};
-      if (sy >= 0 && mxb >= 0) {
-        SlabEntry s0 = A.slab[1][0][1][sy];
-        if (s0.count) {
-          int q = my - s0.from;
-          long long p = s0.psi + ((long long)k * s0.count + q) * nx + mxb;
-          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s0.coef + q],
-                      A.coefs[s0.coef + s0.count + q], A.step[1], T(1), dyEz, hn[0], zero4, ow);
-        }
-      }
-      if (zs && mxb >= 0) {
-        SlabEntry s0 = k < A.low[2] ? A.slab[1][0][2][0] : A.slab[1][0][2][1];
-        if (s0.count) {
-          int q = k - s0.from;
-          long long p = s0.psi + (long long)q * plane + rowat;
-          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s0.coef + q],
-                      A.coefs[s0.coef + s0.count + q], A.step[2], T(-1), dzEy, hn[0], zero4, ow);
-        }
-      }
-      if (any_x) {  // one place at a time: a slab along x is a few columns
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (sxs[j] >= 0 && hv[j]) {
-            SlabEntry s1 = A.slab[1][1][0][sxs[j]];
-            if (s1.count) hn[1][j] = slab_apply<T, 1>(A, s1, 1, 0, xb + j < 0 ? nx - VEC + j : (xb + j >= nx ? xb + j - nx : xb + j), my, k, dxEz[j], hn[1][j], T(0), ow && (j + VEC * lane) >= VEC);
-          }
-      }
-      if (zs && mxb >= 0) {
-        SlabEntry s1 = k < A.low[2] ? A.slab[1][1][2][0] : A.slab[1][1][2][1];
-        if (s1.count) {
-          int q = k - s1.from;
-          long long p = s1.psi + (long long)q * plane + rowat;
-          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s1.coef + q],
-                      A.coefs[s1.coef + s1.count + q], A.step[2], T(1), dzEx, hn[1], zero4, ow);
-        }
-      }
-      if (any_x) {
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (sxs[j] >= 0 && hv[j]) {
-            SlabEntry s2 = A.slab[1][2][0][sxs[j]];
-            if (s2.count) hn[2][j] = slab_apply<T, 1>(A, s2, 2, 0, xb + j < 0 ? nx - VEC + j : (xb + j >= nx ? xb + j - nx : xb + j), my, k, dxEy[j], hn[2][j], T(0), ow && (j + VEC * lane) >= VEC);
-          }
-      }
-      if (sy >= 0 && mxb >= 0) {
-        SlabEntry s2 = A.slab[1][2][1][sy];
-        if (s2.count) {
-          int q = my - s2.from;
-          long long p = s2.psi + ((long long)k * s2.count + q) * nx + mxb;
-          slab4<T, 1>(A, A.psi_h_out + p, A.psi_h_in + p, A.coefs[s2.coef + q],
-                      A.coefs[s2.coef + s2.count + q], A.step[1], T(-1), dyEx, hn[2], zero4, ow);
-        }
-      }
+      const T diff[3][3][4] = {
+          {{T(0), T(0), T(0), T(0)}, {dyEz[0], dyEz[1], dyEz[2], dyEz[3]}, {dzEy[0], dzEy[1], dzEy[2], dzEy[3]}},
+          {{dxEz[0], dxEz[1], dxEz[2], dxEz[3]}, {T(0), T(0), T(0), T(0)}, {dzEx[0], dzEx[1], dzEx[2], dzEx[3]}},
+          {{dxEy[0], dxEy[1], dxEy[2], dxEy[3]}, {dyEx[0], dyEx[1], dyEx[2], dyEx[3]}, {T(0), T(0), T(0), T(0)}}};
+      const T nocb[3][4] = {};
+      cpml4<T, 1>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, ow, hn, diff, nocb, true);
     }
     // beyond a wall H is zero (E's back differences read zero there)
 #pragma unroll
@@ -1575,67 +1635,15 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         en[2][j] = cav[2] * e[2].v[j] + cb[2].v[j] * curl2;
       }
       // the CPML: E_x along y then z, E_y along x then z, E_z along x then y
-      if (any_own && (zs | (sy >= 0) | any_x)) {
-        T cbx[4], cby[4], cbz[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          cbx[j] = cb[0].v[j];
-          cby[j] = cb[1].v[j];
-          cbz[j] = cb[2].v[j];
-        }
-        const long long rowat = rowoff + mxb;
-        if (sy >= 0) {
-          SlabEntry s0 = A.slab[0][0][1][sy];
-          if (s0.count) {
-            int q = my - s0.from;
-            long long p2 = s0.psi + ((long long)k * s0.count + q) * nx + mxb;
-            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s0.coef + q],
-                        A.coefs[s0.coef + s0.count + q], A.step[1], T(1), dyHz, en[0], cbx, true);
-          }
-        }
-        if (zs) {
-          SlabEntry s0 = k < A.low[2] ? A.slab[0][0][2][0] : A.slab[0][0][2][1];
-          if (s0.count) {
-            int q = k - s0.from;
-            long long p2 = s0.psi + (long long)q * plane + rowat;
-            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s0.coef + q],
-                        A.coefs[s0.coef + s0.count + q], A.step[2], T(-1), dzHy, en[0], cbx, true);
-          }
-        }
-        if (any_x) {
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            if (sxs[j] >= 0 && ownv[j]) {
-              SlabEntry s1 = A.slab[0][1][0][sxs[j]];
-              if (s1.count) en[1][j] = slab_apply<T, 0>(A, s1, 1, 0, xb + j, my, k, dxHz[j], en[1][j], cby[j], true);
-            }
-        }
-        if (zs) {
-          SlabEntry s1 = k < A.low[2] ? A.slab[0][1][2][0] : A.slab[0][1][2][1];
-          if (s1.count) {
-            int q = k - s1.from;
-            long long p2 = s1.psi + (long long)q * plane + rowat;
-            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s1.coef + q],
-                        A.coefs[s1.coef + s1.count + q], A.step[2], T(1), dzHx, en[1], cby, true);
-          }
-        }
-        if (any_x) {
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            if (sxs[j] >= 0 && ownv[j]) {
-              SlabEntry s2 = A.slab[0][2][0][sxs[j]];
-              if (s2.count) en[2][j] = slab_apply<T, 0>(A, s2, 2, 0, xb + j, my, k, dxHy[j], en[2][j], cbz[j], true);
-            }
-        }
-        if (sy >= 0) {
-          SlabEntry s2 = A.slab[0][2][1][sy];
-          if (s2.count) {
-            int q = my - s2.from;
-            long long p2 = s2.psi + ((long long)k * s2.count + q) * nx + mxb;
-            slab4<T, 0>(A, A.psi_e + p2, A.psi_e + p2, A.coefs[s2.coef + q],
-                        A.coefs[s2.coef + s2.count + q], A.step[1], T(-1), dyHx, en[2], cbz, true);
-          }
-        }
+      if (any_own && mxb >= 0 && (zs | (sy >= 0) | any_x)) {
+        const T diff[3][3][4] = {
+            {{T(0), T(0), T(0), T(0)}, {dyHz[0], dyHz[1], dyHz[2], dyHz[3]}, {dzHy[0], dzHy[1], dzHy[2], dzHy[3]}},
+            {{dxHz[0], dxHz[1], dxHz[2], dxHz[3]}, {T(0), T(0), T(0), T(0)}, {dzHx[0], dzHx[1], dzHx[2], dzHx[3]}},
+            {{dxHy[0], dxHy[1], dxHy[2], dxHy[3]}, {dyHx[0], dyHx[1], dyHx[2], dyHx[3]}, {T(0), T(0), T(0), T(0)}}};
+        const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
+                             {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
+                             {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
+        cpml4<T, 0>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, true, en, diff, cbs, true);
       }
       // the electric currents (src/fdtd.rs:1375-1387)
       const int bucket = tile * nz + k;
@@ -1853,6 +1861,7 @@ using namespace pxf;
 struct DeviceSlab {
   int field, comp, axis;
   long long from, count, psi, coef, size;
+  long long pf, pw;  // x slabs: the padded rows (see SlabEntry)
 };
 
 struct fdtd_ctx {
@@ -2281,7 +2290,9 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
     d.axis = w;
     d.from = sl.from;
     d.count = sl.count;
-    d.size = sl.count * (N / c->n[w]);
+    d.pf = w == 0 ? sl.from / 4 * 4 : sl.from;
+    d.pw = w == 0 ? (sl.from + sl.count + 3) / 4 * 4 - d.pf : sl.count;
+    d.size = d.pw * (N / c->n[w]);
     d.coef = (long long)coefs.size();
     // each slab's psi starts on a 16-element boundary, so a row of four values is one aligned
     // vector in f32 and two in f64
@@ -2296,6 +2307,8 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
     t.count = (int)sl.count;
     t.psi = d.psi;
     t.coef = (int)d.coef;
+    t.pf = (int)d.pf;
+    t.pw = (int)d.pw;
   }
   if (int r = alloc(c, &c->coefs, coefs.size() * E)) return r;
   if (int r = upload(c, c->coefs, coefs.data(), (long long)coefs.size())) return r;
@@ -2318,8 +2331,12 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   c->sms = sms;
   {
     const char *force = getenv("PHOTONOXIDE_FDTD_KERNEL");
-    std::string kind = force ? force : (c->n[0] % 4 == 0 ? "quad" : "row");
-    if (kind == "quad" && c->n[0] % 4 != 0) kind = "row";
+    // the quad kernel takes four places along x at once: nx a multiple of 4, and no group of
+    // four holding places of both x CPMLs (an interior narrower than the group)
+    const bool quad_ok = c->n[0] % 4 == 0 &&
+        !(c->low[0] > 0 && c->high[0] > 0 && (c->low[0] - 1) / 4 == (c->n[0] - c->high[0]) / 4);
+    std::string kind = force ? force : (quad_ok ? "quad" : "row");
+    if (kind == "quad" && !quad_ok) kind = "row";
     c->quad = kind == "quad";
     c->row = kind == "row";
     c->staged = kind == "staged" && (c->n[0] % (16 / (int)c->elem) == 0);
@@ -2389,8 +2406,21 @@ int fdtd_upload_fields(fdtd_ctx *c, const double *e, const double *h, const doub
     const DeviceSlab &d = c->slabs[s];
     void *base = d.field == 1 ? c->psi_h[0] : c->psi_e;
     void *dst = (char *)base + d.psi * E;
-    if (psi && psi[s]) { if (int r = upload(c, dst, psi[s], d.size)) return r; }
-    else CUDA_TRY(c, cudaMemsetAsync(dst, 0, d.size * E, c->stream));
+    if (psi && psi[s]) {
+      if (d.axis == 0 && (d.pf != d.from || d.pw != d.count)) {
+        // the reference's rows of `count` values into the padded rows
+        long long rows = d.size / d.pw;
+        std::vector<double> padded(d.size, 0.0);
+        for (long long r = 0; r < rows; r++)
+          for (long long q = 0; q < d.count; q++)
+            padded[r * d.pw + (d.from - d.pf) + q] = psi[s][r * d.count + q];
+        if (int r = upload(c, dst, padded.data(), d.size)) return r;
+      } else if (int r = upload(c, dst, psi[s], d.size)) {
+        return r;
+      }
+    } else {
+      CUDA_TRY(c, cudaMemsetAsync(dst, 0, d.size * E, c->stream));
+    }
   }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->fields_set = true;
@@ -2407,7 +2437,17 @@ int fdtd_download_fields(fdtd_ctx *c, double *e, double *h, double *const *psi) 
       if (!psi[s]) continue;
       const DeviceSlab &d = c->slabs[s];
       const void *base = d.field == 1 ? c->psi_h[c->parity] : c->psi_e;
-      if (int r = download(c, psi[s], (const char *)base + d.psi * c->elem, d.size)) return r;
+      const void *src = (const char *)base + d.psi * c->elem;
+      if (d.axis == 0 && (d.pf != d.from || d.pw != d.count)) {
+        long long rows = d.size / d.pw;
+        std::vector<double> padded(d.size);
+        if (int r = download(c, padded.data(), src, d.size)) return r;
+        for (long long r = 0; r < rows; r++)
+          for (long long q = 0; q < d.count; q++)
+            psi[s][r * d.count + q] = padded[r * d.pw + (d.from - d.pf) + q];
+      } else if (int r = download(c, psi[s], src, d.size)) {
+        return r;
+      }
     }
   return 0;
 }
