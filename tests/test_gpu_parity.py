@@ -14,7 +14,8 @@ import numpy as np
 import pytest
 
 from photonoxide_b200.fdtd import Simulation
-from photonoxide_b200.types import Axis, Boundaries, Field, Grid3d, Periodic
+from photonoxide_b200.types import (INF, Axis, Boundaries, Boxes, Dispersive, Field, Grid3d,
+                                    Periodic, Pole, Source, Waveform)
 from pyoracle import OracleSimulation
 from scenarios import busy, closed, noise, stirred
 
@@ -138,3 +139,35 @@ def test_every_kernel_gives_the_same_bits(kind, monkeypatch):
     for x, y in zip(fields(default), fields(other)):
         assert np.array_equal(x, y)
     assert np.array_equal(default.transforms(), other.transforms())
+
+
+def dispersive(cls, precision, n):
+    """Drude and two-pole Lorentz boxes (src/fdtd/media_checks.rs:12 kind) with a conductivity
+    under part of one, CPML all round, random fields and a point source."""
+    g = Grid3d.centred(n, 0.02)
+    s = cls(g, Boxes(1.0).add((-0.1, -0.1, -INF), (0.1, 0.1, INF), 2.0), Boundaries.with_cpml(4),
+            0.5, precision=precision)
+    s.with_conductivity(Boxes(0.0).add((0.0, -INF, -INF), (INF, 0.0, INF), 0.5))
+    drude = Dispersive(1.0, [Pole.drude(7.27, 0.0531)])
+    lorentz = Dispersive(2.25, [Pole.lorentz(1.2, 0.7, 0.01), Pole.lorentz(0.6, 0.45, 0.02)])
+    s.with_medium(drude, Boxes(0.0).add((-0.3, -0.2, -INF), (-0.05, 0.25, INF), 1.0))
+    s.with_medium(lorentz, Boxes(0.0).add((-0.08, -0.3, -0.1), (0.3, 0.05, 0.12), 1.0))
+    r = np.arange(g.cells())
+    for c in range(3):
+        s.set_field(Field.E, c, 0.01 * noise(r + 5 * c))
+    s.add_source(Source(Field.E, Axis.Z, (g.nx // 2, g.ny // 2, g.nz // 2), Waveform.pulse(1.0, 0.5)))
+    p = s.add_probe(Field.E, Axis.Z, (g.nx // 3, g.ny // 2, g.nz // 2))
+    return s, p
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+@pytest.mark.parametrize("n", [(37, 29, 17), (40, 28, 16)])
+def test_dispersive_media_bit_for_bit(precision, n):
+    """The ADE currents (src/fdtd/media.rs:661-705) stepped in the same pass as E."""
+    p, pp = dispersive(Simulation, precision, n)
+    o, op = dispersive(OracleSimulation, precision, n)
+    p.run(300)
+    o.run(300)
+    for x, y in zip(fields(p), fields(o)):
+        assert np.array_equal(x, y), relative(x, y)
+    assert np.array_equal(p.probe(pp), o.probe(op))
