@@ -2,7 +2,7 @@
 
 The setup (cell-averaged permittivity, time step, walls, CPML tables, media, sources, monitors)
 is the C++ host library's and the stepping the CUDA engine's, both in ``libphotonoxide_fdtd.so``
-next to this file (``__graft_entry__.build()`` or ``make -C photonoxide_b200/csrc`` builds it).
+next to this file (``make -C photonoxide_b200/csrc`` builds it).
 There is no CPU fallback: without the library, or without a CUDA device at the first run, the
 calls raise.
 
@@ -47,7 +47,7 @@ def library():
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             raise GpuError(
-                f"{LIB_PATH} is not built: run __graft_entry__.build() or make -C {HERE}/csrc")
+                f"{LIB_PATH} is not built: run make -C {HERE}/csrc")
         x = C.CDLL(LIB_PATH)
         x.pxs_create.restype = P
         x.pxs_create.argtypes = [I64P, DP, DP, I32P, I64P, I64P, DP, D, DP, C.POINTER(Geometry),
