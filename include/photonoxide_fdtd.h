@@ -109,6 +109,16 @@ const char *fdtd_last_error(const fdtd_ctx *ctx);
 int fdtd_upload_coeffs(fdtd_ctx *ctx, const double *ca, const double *cb);
 /* The fields (3 x cells each) and each slab's psi (in slab order; NULL entries mean zero). */
 int fdtd_upload_fields(fdtd_ctx *ctx, const double *e, const double *h, const double *const *psi);
+/* fdtd_upload_fields(ctx, e, h, NULL) without allocating any device memory, for callers that
+ * can't allocate at that point: a serving loop that has handed out its whole HBM budget, an
+ * application whose CUDA allocator is its own, code that must leave a stream-ordered memory pool
+ * untouched. No counterpart in the reference (its uploads go through wgpu's staging buffers).
+ * The f64 host values pass through a fixed 16 MiB device array of the library (2^21 values, held
+ * by every GPU that loads it until exit), one field component at a time: a grid of more than
+ * 2^21 cells is refused (FDTD_E_INVALID); use fdtd_upload_fields. psi restarts from zero. The
+ * first call on a device looks the array up (call it before any stream capture); calls that
+ * overlap on the GPU share the array and race. */
+int fdtd_upload_fields_static(fdtd_ctx *ctx, const double *e, const double *h);
 /* Resident::download (resident.rs:402-413). Any pointer may be NULL to skip it. */
 int fdtd_download_fields(fdtd_ctx *ctx, double *e, double *h, double *const *psi);
 

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -2870,3 +2871,90 @@ int fdtd_profile_read(fdtd_ctx *c, double *ms, int64_t *launches) {
 int64_t fdtd_launches(const fdtd_ctx *c) { return c ? c->launches : 0; }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Uploading without allocating. fdtd_upload_fields stages each f32 upload through a device
+// buffer it allocates and frees per call. Some callers can't allocate device memory at that
+// point: a serving loop that has handed out its whole HBM budget up front, an application whose
+// CUDA allocator is its own and forbids others, code that must not perturb a stream-ordered
+// memory pool. fdtd_upload_fields_static stages through a fixed array instead: a file-scope
+// device array of STATIC_STAGE_VALUES doubles (16 MiB), which every GPU that loads this library
+// holds until the process exits. The array's address is looked up once per device (below), on
+// the first call made with that device current; that first call should come before any stream
+// capture. All calls share the array and it keeps the last call's contents (nothing in it has to
+// start at zero: each pass overwrites what it reads); calls that overlap on the GPU, from two
+// contexts on different streams, race on it.
+namespace {
+constexpr long long STATIC_STAGE_VALUES = 1LL << 21;
+}  // namespace
+static __device__ __align__(256) double g_static_stage[STATIC_STAGE_VALUES];
+
+namespace {
+constexpr int MAX_DEVICES = 64;
+void *g_static_stage_ptr[MAX_DEVICES] = {};
+std::mutex g_static_stage_mutex;
+
+// The device address of g_static_stage on the current device (host code can't use the symbol
+// itself: in host code its name is only a host-side stand-in).
+int static_stage_address(fdtd_ctx *c, double **out) {
+  int dev = 0;
+  CUDA_TRY(c, cudaGetDevice(&dev));
+  if (dev < 0 || dev >= MAX_DEVICES) return fail(c, FDTD_E_GPU, "device %d is beyond %d", dev, MAX_DEVICES);
+  std::lock_guard<std::mutex> lock(g_static_stage_mutex);
+  if (!g_static_stage_ptr[dev]) {
+    void *p = nullptr;
+    CUDA_TRY(c, cudaGetSymbolAddress(&p, g_static_stage));
+    g_static_stage_ptr[dev] = p;
+  }
+  *out = static_cast<double *>(g_static_stage_ptr[dev]);
+  return 0;
+}
+
+// One component (n values) from the host into dst, through the static array.
+template <typename T>
+int upload_static_as(fdtd_ctx *c, double *stage, void *dst, const double *src, long long n) {
+  if (sizeof(T) == 8) {
+    CUDA_TRY(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(stage, src, n * 8, cudaMemcpyHostToDevice, c->stream));
+  convert_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(stage, (T *)dst, n);
+  CUDA_TRY(c, cudaGetLastError());
+  return 0;
+}
+}  // namespace
+
+extern "C" int fdtd_upload_fields_static(fdtd_ctx *c, const double *e, const double *h) {
+  if (!c) return FDTD_E_INVALID;
+  if (c->N > STATIC_STAGE_VALUES)
+    return fail(c, FDTD_E_INVALID,
+                "a field component of %lld values exceeds the %lld-value static staging array: "
+                "use fdtd_upload_fields",
+                c->N, STATIC_STAGE_VALUES);
+  double *stage = nullptr;
+  if (int r = static_stage_address(c, &stage)) return r;
+  c->parity = 0;
+  const size_t E = c->elem;
+  const double *src[2] = {e, h};
+  void *dst[2] = {c->e[0], c->h[0]};
+  for (int f = 0; f < 2; f++) {
+    if (!src[f]) {
+      CUDA_TRY(c, cudaMemsetAsync(dst[f], 0, 3 * c->N * E, c->stream));
+      continue;
+    }
+    for (int comp = 0; comp < 3; comp++) {
+      void *d = (char *)dst[f] + comp * c->N * E;
+      int r = c->precision == 64 ? upload_static_as<double>(c, stage, d, src[f] + comp * c->N, c->N)
+                                 : upload_static_as<float>(c, stage, d, src[f] + comp * c->N, c->N);
+      if (r) return r;
+    }
+  }
+  for (size_t s = 0; s < c->slabs.size(); s++) {  // psi from zero, as fdtd_upload_fields with NULL
+    const DeviceSlab &d = c->slabs[s];
+    void *base = d.field == 1 ? c->psi_h[0] : c->psi_e;
+    CUDA_TRY(c, cudaMemsetAsync((char *)base + d.psi * E, 0, d.size * E, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->fields_set = true;
+  return 0;
+}
