@@ -1359,7 +1359,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const int gy = y0 - 1 + w;
   const int my = wrap_index(gy, ny, A.periodic[1]);
   const int myp = wrap_index(gy + 1, ny, A.periodic[1]);
-  const bool rowe = my >= 0, rowh = my >= 0 && gy < ny;
+  const bool rowh = my >= 0 && gy < ny;
   bool hv[4], ownv[4];
   T fhx[4], fex[4];
   int sxs[4];  // the x CPML side of each place (-1 none)
@@ -2358,11 +2358,12 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   c->tiles_x = (c->n[0] + c->tile_w - 1) / c->tile_w;
   c->tiles_y = (c->n[1] + c->tile_h - 1) / c->tile_h;
   long long tiles = (long long)c->tiles_x * c->tiles_y;
-  // z cut into runs so that the CTAs fill the device at least twice over (the scheduler then
-  // balances them), each run at least 16 planes long (each run recomputes one plane of H)
-  long long want = 2LL * 3 * sms;
+  // z cut into runs so that the CTAs fill the device about twelve times over: runs that meet a
+  // CPML take several times longer than the rest, and short runs let the scheduler balance
+  // them. Each run recomputes one plane of H, so a run is at least 4 planes long.
+  long long want = 24LL * sms;
   int chunks = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
-  chunks = std::min(chunks, std::max(1, c->n[2] / 16));
+  chunks = std::min(chunks, std::max(1, c->n[2] / 4));
   const char *zc = getenv("PHOTONOXIDE_FDTD_ZCHUNKS");
   if (zc) chunks = std::max(1, atoi(zc));
   chunks = std::min(chunks, c->n[2]);
@@ -2913,13 +2914,13 @@ int static_stage_address(fdtd_ctx *c, double **out) {
 // One component (n values) from the host into dst, through the static array.
 template <typename T>
 int upload_static_as(fdtd_ctx *c, double *stage, void *dst, const double *src, long long n) {
-  if (sizeof(T) == 8) {
+  if constexpr (sizeof(T) == 8) {
     CUDA_TRY(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->stream));
-    return 0;
+  } else {
+    CUDA_TRY(c, cudaMemcpyAsync(stage, src, n * 8, cudaMemcpyHostToDevice, c->stream));
+    convert_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(stage, (T *)dst, n);
+    CUDA_TRY(c, cudaGetLastError());
   }
-  CUDA_TRY(c, cudaMemcpyAsync(stage, src, n * 8, cudaMemcpyHostToDevice, c->stream));
-  convert_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(stage, (T *)dst, n);
-  CUDA_TRY(c, cudaGetLastError());
   return 0;
 }
 }  // namespace
