@@ -91,6 +91,18 @@ int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out);
 /* The device engine under it (created at the first run), or NULL. */
 struct fdtd_ctx *pxs_engine(pxs_sim *s);
 
+/* Batches (photonoxide_batch.h): 2D TE simulations stepped together, one launch per step. Each
+ * simulation afterwards reads out as if pxs_run had taken the steps. No counterpart in the
+ * reference, whose Simulation runs alone. */
+typedef struct pxs_batch pxs_batch;
+int pxs_batch_create(int32_t count, pxs_sim *const *sims, pxs_batch **out);
+const char *pxs_batch_last_error(const pxs_batch *b);
+int pxs_batch_run(pxs_batch *b, int64_t steps);
+int pxs_batch_tile(const pxs_batch *b, int32_t *width, int32_t *height);
+int pxs_batch_set_tile(pxs_batch *b, int32_t width, int32_t height);
+int64_t pxs_batch_launches(const pxs_batch *b);
+void pxs_batch_destroy(pxs_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,869 @@
+// Batched 2D TE stepping: many simulations' grids (one cell thick, periodic along z, as
+// Boundaries::cpml_2d in src/fdtd.rs:242-247) advanced together, one launch per step for all of
+// them. Each simulation is a context of the single-grid engine (engine.cu), already set up by
+// its own calls; the batch steps its buffers in place and leaves the context as if it had run
+// the steps itself.
+//
+// TE fields only: E_x, E_y and H_z. On such a grid the other three components (H_x, H_y, E_z)
+// start at zero and stay zero under the reference's update (src/fdtd/kernel/reference.rs:14-99),
+// and each TE value is computed with the same operations in the same order as the single-grid
+// kernel (curl, the CPML slabs along x then y, then the sources), so a simulation stepped in a
+// batch has the bits it has stepped alone.
+//
+// One step is ONE persistent launch: CTAs (a few per SM) take tiles of TW x TH cells from the
+// list of all the grids' tiles. A tile computes H_z over itself and the row and column below it
+// (its neighbours compute the same values), adds the magnetic sources there, then updates E_x and
+// E_y on its cells, adds the electric sources, and writes both to the other copy of the fields.
+// Steps run in chunks of G: the source waveforms and transform phases of a chunk are evaluated
+// first (f64, the reference's exp and sincos), the chunk's step launches follow, each with a
+// launch that adds the new values into the f64 transform sums in time order. A chunk is captured
+// once as a CUDA graph and replayed. The tile shape is chosen by timing: the first run tries each
+// shape on a chunk of real steps (every shape gives the same bits) and keeps the fastest.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "instance.h"
+#include "photonoxide_batch.h"
+
+namespace pxb {
+using namespace pxf;
+
+constexpr int THREADS = 256;
+constexpr int G = 32;  // steps per chunk (even: a chunk leaves the copies' parity as it was)
+
+template <typename T>
+struct TeInst {
+  int nx, ny, px, py;  // sizes, periodic flags
+  long long N;
+  T dt, sx, sy;        // the step's dt and the grid steps along x and y, as the kernel rounds them
+  double dt64;
+  T *e[2], *h[2], *psi_h[2];
+  T *psi_e;
+  const T *ca, *cb, *fe, *fh, *coefs;
+  // the CPML slabs a TE grid has: H_z along x and y, E_y along x, E_x along y (per side)
+  SlabEntry hx[2], hy[2], ex[2], ey[2];
+  int parity;         // the current copy (device: kept up to date across chunks)
+  long long first;    // the step index the next step has
+  double *rows;       // the probe record's next row
+  int tiles_x, tile0; // tiles along x; the first tile's number in the batch
+  int bucket0;        // the first of its tiles' buckets
+  int wave0, nwaves;  // its emitters in the batch's wave table
+  int slot0, nslots;  // its transform phase slots
+  const long long *where;
+  const SeriesDev *series;
+  const long long *value_series;
+  const double *omega;
+  const int *slot_field;
+  double *sums;
+  const long long *probes;
+  int nprobes;
+};
+
+// One record item: instance, then a transform value (kind 0) or a probe (kind 1) by index.
+struct RecItem {
+  int inst, kind;
+  long long index;
+};
+
+__device__ __forceinline__ bool in_slab(const SlabEntry &s, int m) {
+  return s.count > 0 && m >= s.from && m < s.from + s.count;
+}
+
+// psi <- b psi + a (d/h), then H -= dt (sign psi) or E += cb (sign psi) (slab4 in engine.cu)
+template <typename T>
+__device__ __forceinline__ T slab_h(const TeInst<T> &I, const SlabEntry &s, int m, long long at,
+                                    const T *pin, T *pout, bool own, T diff, T h, T sign, T v) {
+  const T b = I.coefs[s.coef + (m - s.from)], a = I.coefs[s.coef + s.count + (m - s.from)];
+  T d = diff / h;
+  T nw = b * pin[at] + a * d;
+  if (own) pout[at] = nw;
+  T u = sign * nw;
+  return v - I.dt * u;
+}
+template <typename T>
+__device__ __forceinline__ T slab_e(const TeInst<T> &I, const SlabEntry &s, int m, long long at,
+                                    T *psi, T diff, T h, T sign, T cbv, T v) {
+  const T b = I.coefs[s.coef + (m - s.from)], a = I.coefs[s.coef + s.count + (m - s.from)];
+  T d = diff / h;
+  T nw = b * psi[at] + a * d;
+  psi[at] = nw;
+  T u = sign * nw;
+  return v + cbv * u;
+}
+
+template <typename T, int TW, int TH>
+__global__ void __launch_bounds__(THREADS) te_step_kernel(
+    const TeInst<T> *insts, const int *tile_inst, int ntiles, const int *hbucket,
+    const int *ebucket, const Group *hgroups, const Group *egroups, const Entry *entries,
+    const double *waves_h, const double *waves_e, int m) {
+  constexpr int HW = TW + 1, HH = TH + 1;
+  __shared__ T sh[HW * HH];  // the new H_z over the tile and the row and column below it
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = tile_inst[t];
+    const TeInst<T> &I = insts[ii];
+    const int lt = t - I.tile0;
+    const int x0 = (lt % I.tiles_x) * TW, y0 = (lt / I.tiles_x) * TH;
+    const int nx = I.nx, ny = I.ny;
+    const long long N = I.N;
+    const int cur = (I.parity + m) & 1;
+    const T *ein = I.e[cur];
+    T *eout = I.e[1 - cur];
+    const T *hin = I.h[cur];
+    T *hout = I.h[1 - cur];
+    const T *pin = I.psi_h[cur];
+    T *pout = I.psi_h[1 - cur];
+    // -- H_z (src/fdtd/kernel/reference.rs:14-56 with E_z, H_x, H_y zero)
+    for (int q = threadIdx.x; q < HW * HH; q += THREADS) {
+      const int lx = q % HW, ly = q / HW;
+      const int x = x0 - 1 + lx, y = y0 - 1 + ly;
+      const int mx = wrap_index(x, nx, I.px), my = wrap_index(y, ny, I.py);
+      T hz = T(0);  // beyond a wall H is zero
+      if (mx >= 0 && my >= 0 && x < nx && y < ny) {
+        const int mxp = wrap_index(mx + 1, nx, I.px), myp = wrap_index(my + 1, ny, I.py);
+        const long long r = (long long)my * nx + mx;
+        const T ex = ein[r], ey = ein[N + r];
+        const T eyn = mxp >= 0 ? ein[N + (long long)my * nx + mxp] : T(0);
+        const T exn = myp >= 0 ? ein[(long long)myp * nx + mx] : T(0);
+        const T dxEy = eyn - ey, dyEx = exn - ex;
+        hz = hin[2 * N + r] - I.dt * (dxEy * I.fh[mx] - dyEx * I.fh[nx + my]);
+        const bool own = lx >= 1 && ly >= 1;
+        // the CPML: H_z along x (+), then along y (-)
+        if (!I.px) {
+          const int side = mx < nx / 2 ? 0 : 1;
+          const SlabEntry &s = I.hx[side];
+          if (in_slab(s, mx))
+            hz = slab_h(I, s, mx, s.psi + (long long)my * s.pw + (mx - s.pf), pin, pout, own, dxEy,
+                        I.sx, T(1), hz);
+        }
+        if (!I.py) {
+          const int side = my < ny / 2 ? 0 : 1;
+          const SlabEntry &s = I.hy[side];
+          if (in_slab(s, my))
+            hz = slab_h(I, s, my, s.psi + (long long)(my - s.from) * nx + mx, pin, pout, own, dyEx,
+                        I.sy, T(-1), hz);
+        }
+      }
+      sh[q] = hz;
+    }
+    const int b = I.bucket0 + lt;
+    const int hg0 = hbucket[b], hg1 = hbucket[b + 1];
+    if (hg1 > hg0) {
+      __syncthreads();
+      // the magnetic sources (src/fdtd.rs:1348-1359), each value's entries in CPU order
+      for (int g = hg0 + threadIdx.x; g < hg1; g += THREADS) {
+        const Group gr = hgroups[g];
+        T v = sh[gr.local];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          const Entry en = entries[q];
+          const double *w = waves_h + 2 * (long long)en.emitter;
+          const double amount = en.are * w[0] - en.aim * w[1];
+          if (sizeof(T) == 8) v = v - (T)(I.dt64 * amount);
+          else v = v - I.dt * (T)amount;
+        }
+        sh[gr.local] = v;
+      }
+    }
+    __syncthreads();
+    // -- E_x, E_y on the tile (reference.rs:58-99): back differences of the new H_z
+    for (int q = threadIdx.x; q < TW * TH; q += THREADS) {
+      const int lx = q % TW + 1, ly = q / TW + 1;
+      const int x = x0 + lx - 1, y = y0 + ly - 1;
+      if (x < nx && y < ny) {
+        const long long r = (long long)y * nx + x;
+        const T hz = sh[ly * HW + lx];
+        hout[2 * N + r] = hz;
+        const T dyHz = hz - sh[(ly - 1) * HW + lx], dxHz = hz - sh[ly * HW + lx - 1];
+        const T fex = I.fe[x], fey = I.fe[nx + y];
+        // curl_x = dyHz fey - dzHy fez and curl_y = dzHx fez - dxHz fex, with dzHy = dzHx = +0
+        const T curl0 = dyHz * fey;
+        const T curl1 = T(0) - dxHz * fex;
+        const T cbx = I.cb[r], cby = I.cb[N + r];
+        T cax, cay;
+        if (I.ca) {
+          cax = I.ca[r];
+          cay = I.ca[N + r];
+        } else {
+          cax = cbx == T(0) ? T(0) : T(1);
+          cay = cby == T(0) ? T(0) : T(1);
+        }
+        T nex = cax * ein[r] + cbx * curl0;
+        T ney = cay * ein[N + r] + cby * curl1;
+        // the CPML: E_x along y (+), E_y along x (-)
+        if (!I.py) {
+          const int side = y < ny / 2 ? 0 : 1;
+          const SlabEntry &s = I.ey[side];
+          if (in_slab(s, y))
+            nex = slab_e(I, s, y, s.psi + (long long)(y - s.from) * nx + x, I.psi_e, dyHz, I.sy,
+                         T(1), cbx, nex);
+        }
+        if (!I.px) {
+          const int side = x < nx / 2 ? 0 : 1;
+          const SlabEntry &s = I.ex[side];
+          if (in_slab(s, x))
+            ney = slab_e(I, s, x, s.psi + (long long)y * s.pw + (x - s.pf), I.psi_e, dxHz, I.sx,
+                         T(-1), cby, ney);
+        }
+        eout[r] = nex;
+        eout[N + r] = ney;
+      }
+    }
+    const int eg0 = ebucket[b], eg1 = ebucket[b + 1];
+    if (eg1 > eg0) {
+      __syncthreads();  // this CTA's E values are in memory
+      // the electric currents (src/fdtd.rs:1375-1387): local = the place in the tile, x fastest
+      for (int g = eg0 + threadIdx.x; g < eg1; g += THREADS) {
+        const Group gr = egroups[g];
+        const int lq = gr.local;
+        const int x = x0 + lq % TW, y = y0 + lq / TW;
+        const long long at = (long long)gr.comp * N + (long long)y * nx + x;
+        T v = eout[at];
+        const T cbv = I.cb[at];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          const Entry en = entries[q];
+          const double *w = waves_e + 2 * (long long)en.emitter;
+          const double amount = en.are * w[0] - en.aim * w[1];
+          if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
+          else v = v - cbv * (T)amount;
+        }
+        eout[at] = v;
+      }
+    }
+    __syncthreads();  // sh is reused by the next tile
+  }
+}
+
+// The chunk's waveforms: per (instance, emitter, step m) at H's time (first+m) dt and E's
+// (first+m+1/2) dt (waves_kernel in engine.cu). Emitter numbers in `entries` are batch-wide:
+// wave0 + the instance's own; the tables are [m][emitter].
+template <typename T>
+__global__ void te_waves_kernel(const TeInst<T> *insts, const int2 *items, int nitems,
+                                const Wave *waves, const int *point, int nwaves_total,
+                                double *out_h, double *out_e) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nitems * G) return;
+  const int m = q / nitems, it = q % nitems;
+  const int2 item = items[it];  // (instance, batch-wide emitter)
+  const TeInst<T> &I = insts[item.x];
+  const double t = (double)(I.first + m) * I.dt64;
+  double re, im;
+  wave_eval(waves[item.y], t, &re, &im, point[item.y]);
+  long long o = 2 * ((long long)m * nwaves_total + item.y);
+  out_h[o] = re;
+  out_h[o + 1] = im;
+  wave_eval(waves[item.y], t + 0.5 * I.dt64, &re, &im, point[item.y]);
+  out_e[o] = re;
+  out_e[o + 1] = im;
+}
+
+// The chunk's transform phases e^{i w t} dt: E at te = (first+m+1) dt, H at te - dt/2
+// (phase_kernel in engine.cu); [m][batch-wide slot].
+template <typename T>
+__global__ void te_phase_kernel(const TeInst<T> *insts, const int2 *items, int nitems,
+                                int nslots_total, double *phase) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nitems * G) return;
+  const int m = q / nitems, it = q % nitems;
+  const int2 item = items[it];  // (instance, its own slot)
+  const TeInst<T> &I = insts[item.x];
+  const double te = (double)(I.first + m + 1) * I.dt64;
+  const double t = I.slot_field[item.y] ? te - 0.5 * I.dt64 : te;
+  double sn, cs;
+  pxp::sincos(I.omega[item.y] * t, &sn, &cs);
+  long long o = 2 * ((long long)m * nslots_total + I.slot0 + item.y);
+  phase[o] = cs * I.dt64;
+  phase[o + 1] = sn * I.dt64;
+}
+
+// After step m of the chunk: each transform value's sums += F e^{i w t} dt (f64, time order),
+// each probe's value into its record row.
+template <typename T>
+__global__ void te_record_kernel(const TeInst<T> *insts, const RecItem *items, long long nitems,
+                                 const double *phase, int nslots_total, int m) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nitems) return;
+  const RecItem it = items[q];
+  const TeInst<T> &I = insts[it.inst];
+  const int now = (I.parity + m + 1) & 1;  // the copy the step wrote
+  if (it.kind == 1) {
+    const long long w = I.probes[it.index];
+    const T *f = (w >> 62) ? I.h[now] : I.e[now];
+    I.rows[(long long)m * I.nprobes + it.index] = (double)f[w & ((1LL << 62) - 1)];
+    return;
+  }
+  const long long v = it.index;
+  const long long w = I.where[v];
+  const T *f = (w >> 62) ? I.h[now] : I.e[now];
+  const double x = (double)f[w & ((1LL << 62) - 1)];
+  const SeriesDev s = I.series[I.value_series[v]];
+  const long long o = v - s.value0;
+  const double *ph = phase + 2 * ((long long)m * nslots_total + I.slot0 + s.slot0);
+  for (int k = 0; k < s.nf; k++) {
+    double *acc = I.sums + 2 * (s.sum0 + (long long)k * s.volume + o);
+    acc[0] = acc[0] + x * ph[2 * k];
+    acc[1] = acc[1] + x * ph[2 * k + 1];
+  }
+}
+
+// After `count` steps: each instance's step index, copy and record row move on.
+template <typename T>
+__global__ void te_advance_kernel(TeInst<T> *insts, int n, int count) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  TeInst<T> &I = insts[q];
+  I.first += count;
+  I.parity = (I.parity + count) & 1;
+  if (I.rows) I.rows += (long long)count * I.nprobes;
+}
+
+// Nonzero values among H_x, H_y, E_z of the current copy (the batch steps TE grids only).
+template <typename T>
+__global__ void te_tm_check_kernel(const T *e, const T *h, long long N, int *bad) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  if (h[q] != T(0) || h[N + q] != T(0) || e[2 * N + q] != T(0)) atomicOr(bad, 1);
+}
+
+struct Shape {
+  int tw, th;
+};
+const Shape SHAPES[] = {{32, 8}, {32, 16}, {64, 4}, {64, 8}, {128, 2}, {128, 4}};
+constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
+constexpr int DEFAULT_SHAPE = 3;  // 64 x 8
+
+}  // namespace pxb
+
+using namespace pxb;
+
+struct fdtd_batch {
+  std::string error;
+  std::vector<fdtd_ctx *> ctxs;
+  int precision = 32;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+  int shape = -1;  // index into SHAPES; -1: choose by timing on the next run
+  long long launches = 0;
+  int sms = 148;
+  std::vector<void *> allocs;  // this run's tables
+  cudaGraphExec_t graph = nullptr;
+  // the current tables (rebuilt at each run)
+  void *d_insts = nullptr;
+  int ntiles = 0;
+  int *d_tile_inst = nullptr;
+  int *d_hbucket = nullptr, *d_ebucket = nullptr;
+  Group *d_hgroups = nullptr, *d_egroups = nullptr;
+  Entry *d_entries = nullptr;
+  Wave *d_waves = nullptr;
+  int *d_point = nullptr;
+  int2 *d_wave_items = nullptr, *d_slot_items = nullptr;
+  int nwave_items = 0, nslot_items = 0, nwaves_total = 0, nslots_total = 0;
+  double *d_waves_h = nullptr, *d_waves_e = nullptr, *d_phase = nullptr;
+  RecItem *d_rec = nullptr;
+  long long nrec = 0;
+  int blocks = 0;
+  int *d_bad = nullptr;  // the TE check's flag
+};
+
+namespace {
+
+int bfail(fdtd_batch *b, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  b->error = buf;
+  return code;
+}
+
+#define BTRY(b, call)                                                                     \
+  do {                                                                                    \
+    cudaError_t err_ = (call);                                                            \
+    if (err_ != cudaSuccess)                                                              \
+      return bfail((b), FDTD_E_GPU, "%s: %s", #call, cudaGetErrorString(err_));           \
+  } while (0)
+
+void free_tables(fdtd_batch *b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  for (void *p : b->allocs) cudaFree(p);
+  b->allocs.clear();
+}
+
+// Whether the batch can step simulation i (a 2D TE grid in the batch's precision, no media).
+int admissible(fdtd_batch *b, const InstanceView &v, int i) {
+  if (v.precision != b->precision)
+    return bfail(b, FDTD_E_INVALID, "simulation %d is in f%d, the batch in f%d", i, v.precision,
+                 b->precision);
+  if (v.n[2] != 1 || !v.periodic[2])
+    return bfail(b, FDTD_E_INVALID,
+                 "simulation %d is not a 2D grid (one cell along z, periodic there)", i);
+  if (v.media)
+    return bfail(b, FDTD_E_INVALID,
+                 "simulation %d has dispersive media, which the batch does not step", i);
+  return 0;
+}
+
+template <typename V>
+int upload_vec(fdtd_batch *b, V **dst, const std::vector<V> &v) {
+  *dst = nullptr;
+  size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(V);
+  void *p = nullptr;
+  BTRY(b, cudaMalloc(&p, bytes));
+  b->allocs.push_back(p);
+  if (!v.empty()) BTRY(b, cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  *dst = static_cast<V *>(p);
+  return 0;
+}
+int zeros(fdtd_batch *b, double **dst, size_t n) {
+  void *p = nullptr;
+  BTRY(b, cudaMalloc(&p, std::max<size_t>(n, 1) * 8));
+  b->allocs.push_back(p);
+  *dst = static_cast<double *>(p);
+  return 0;
+}
+
+// The tables for tile shape `sh`: per-instance descriptors (starting at step first[i], copy
+// parity[i], record row rows[i]), the tile list, the sources' groups per tile, the waveforms,
+// the transforms' phase slots and the record items.
+template <typename T>
+int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vector<int64_t> &first,
+          const std::vector<int> &parity, const std::vector<double *> &rows, int sh) {
+  free_tables(b);
+  const int TW = SHAPES[sh].tw, TH = SHAPES[sh].th;
+  std::vector<TeInst<T>> insts(views.size());
+  std::vector<int> tile_inst;
+  std::vector<int> hb{0}, eb{0};
+  std::vector<Group> hgroups, egroups;
+  std::vector<Entry> entries;
+  std::vector<Wave> waves;
+  std::vector<int> point;
+  std::vector<int2> wave_items, slot_items;
+  std::vector<RecItem> rec;
+  int bucket = 0, slots = 0;
+  for (size_t i = 0; i < views.size(); i++) {
+    const InstanceView &v = views[i];
+    TeInst<T> &I = insts[i];
+    memset(&I, 0, sizeof I);
+    I.nx = v.n[0];
+    I.ny = v.n[1];
+    I.px = v.periodic[0];
+    I.py = v.periodic[1];
+    I.N = v.N;
+    I.dt = (T)v.dt;
+    I.dt64 = v.dt;
+    I.sx = (T)v.step[0];
+    I.sy = (T)v.step[1];
+    for (int p = 0; p < 2; p++) {
+      I.e[p] = (T *)v.e[p];
+      I.h[p] = (T *)v.h[p];
+      I.psi_h[p] = (T *)v.psi_h[p];
+    }
+    I.psi_e = (T *)v.psi_e;
+    I.ca = (const T *)v.ca;
+    I.cb = (const T *)v.cb;
+    I.fe = (const T *)v.fe;
+    I.fh = (const T *)v.fh;
+    I.coefs = (const T *)v.coefs;
+    for (int s = 0; s < 2; s++) {
+      I.hx[s] = v.table[1][2][0][s];
+      I.hy[s] = v.table[1][2][1][s];
+      I.ex[s] = v.table[0][1][0][s];
+      I.ey[s] = v.table[0][0][1][s];
+    }
+    I.parity = parity[i];
+    I.first = first[i];
+    I.rows = rows[i];
+    I.tiles_x = (I.nx + TW - 1) / TW;
+    const int tiles_y = (I.ny + TH - 1) / TH;
+    const int ntile = I.tiles_x * tiles_y;
+    I.tile0 = (int)tile_inst.size();
+    for (int t = 0; t < ntile; t++) tile_inst.push_back((int)i);
+    I.bucket0 = bucket;
+    // the waveforms, numbered batch-wide
+    I.wave0 = (int)waves.size();
+    I.nwaves = (int)v.waves->size();
+    std::vector<int> pt(I.nwaves, 0);
+    for (const fdtd_injection &x : *v.inj) pt[x.emitter] = x.point ? 1 : 0;
+    for (int e = 0; e < I.nwaves; e++) {
+      Wave w;
+      w.kind = (*v.waves)[e].kind;
+      for (int p = 0; p < 5; p++) w.p[p] = (*v.waves)[e].p[p];
+      waves.push_back(w);
+      point.push_back(pt[e]);
+      wave_items.push_back(make_int2((int)i, I.wave0 + e));
+    }
+    // sources: grouped by value in CPU order (as fdtd_set_sources), then by tile. An H value
+    // goes to each tile whose H region (its cells and the row and column below) holds it.
+    std::vector<std::vector<Group>> hper(ntile), eper(ntile);
+    for (int f = 0; f < 2; f++) {
+      std::unordered_map<long long, int> index;
+      std::vector<long long> places;
+      std::vector<std::vector<Entry>> lists;
+      for (const fdtd_injection &x : *v.inj) {
+        if (x.field != f) continue;
+        const long long place = (long long)x.component * v.N + x.r;
+        auto it = index.find(place);
+        int at;
+        if (it == index.end()) {
+          at = (int)places.size();
+          index[place] = at;
+          places.push_back(place);
+          lists.emplace_back();
+        } else {
+          at = it->second;
+        }
+        Entry en;
+        en.are = x.a_re;
+        en.aim = x.a_im;
+        en.emitter = I.wave0 + x.emitter;
+        en.pad = 0;
+        lists[at].push_back(en);
+      }
+      for (size_t g = 0; g < places.size(); g++) {
+        const int comp = (int)(places[g] / v.N);
+        const long long r = places[g] % v.N;
+        const int x = (int)(r % I.nx), y = (int)(r / I.nx);
+        if ((f == 1 && comp != 2) || (f == 0 && comp == 2))
+          return bfail(b, FDTD_E_INVALID,
+                       "simulation %zu has a source on %s_%c: the batch steps TE grids (E_x, E_y, "
+                       "H_z)", i, f ? "H" : "E", "xyz"[comp]);
+        auto add = [&](std::vector<Group> &to, int local) {
+          Group c;
+          c.local = local;
+          c.comp = comp;
+          c.first = (int)entries.size();
+          c.count = (int)lists[g].size();
+          for (const Entry &e : lists[g]) entries.push_back(e);
+          to.push_back(c);
+        };
+        if (f == 0) {
+          const int tx = x / TW, ty = y / TH;
+          add(eper[ty * I.tiles_x + tx], (y - ty * TH) * TW + (x - tx * TW));
+          continue;
+        }
+        // (tile, position in its H region) along each axis: its own tile, and the tile whose
+        // column (row) below it is, also across a periodic wrap
+        auto options = [](int c, int n, int w, int periodic) {
+          std::vector<std::pair<int, int>> o{{c / w, c - (c / w) * w + 1}};
+          if (c + 1 < n && (c + 1) % w == 0) o.push_back({(c + 1) / w, 0});
+          if (periodic && c == n - 1) o.push_back({0, 0});
+          return o;
+        };
+        for (auto oy : options(y, I.ny, TH, I.py))
+          for (auto ox : options(x, I.nx, TW, I.px))
+            add(hper[oy.first * I.tiles_x + ox.first], oy.second * (TW + 1) + ox.second);
+      }
+    }
+    for (int t = 0; t < ntile; t++) {
+      for (const Group &g : hper[t]) hgroups.push_back(g);
+      for (const Group &g : eper[t]) egroups.push_back(g);
+      hb.push_back((int)hgroups.size());
+      eb.push_back((int)egroups.size());
+    }
+    bucket += ntile;
+    // transforms and probes
+    I.where = v.where;
+    I.series = v.series;
+    I.value_series = v.value_series;
+    I.omega = v.omega;
+    I.slot_field = v.slot_field;
+    I.sums = v.sums;
+    I.probes = v.probes;
+    I.nprobes = v.nprobes;
+    I.slot0 = slots;
+    I.nslots = v.nvalues > 0 ? v.nslots : 0;
+    for (int s = 0; s < I.nslots; s++) slot_items.push_back(make_int2((int)i, s));
+    slots += I.nslots;
+    for (long long q = 0; q < v.nvalues; q++) rec.push_back(RecItem{(int)i, 0, q});
+    for (int p = 0; p < v.nprobes; p++) rec.push_back(RecItem{(int)i, 1, p});
+  }
+  b->ntiles = (int)tile_inst.size();
+  b->nwaves_total = (int)waves.size();
+  b->nslots_total = slots;
+  b->nwave_items = (int)wave_items.size();
+  b->nslot_items = (int)slot_items.size();
+  b->nrec = (long long)rec.size();
+  if (int r = upload_vec(b, (TeInst<T> **)&b->d_insts, insts)) return r;
+  if (int r = upload_vec(b, &b->d_tile_inst, tile_inst)) return r;
+  if (int r = upload_vec(b, &b->d_hbucket, hb)) return r;
+  if (int r = upload_vec(b, &b->d_ebucket, eb)) return r;
+  if (int r = upload_vec(b, &b->d_hgroups, hgroups)) return r;
+  if (int r = upload_vec(b, &b->d_egroups, egroups)) return r;
+  if (int r = upload_vec(b, &b->d_entries, entries)) return r;
+  if (int r = upload_vec(b, &b->d_waves, waves)) return r;
+  if (int r = upload_vec(b, &b->d_point, point)) return r;
+  if (int r = upload_vec(b, &b->d_wave_items, wave_items)) return r;
+  if (int r = upload_vec(b, &b->d_slot_items, slot_items)) return r;
+  if (int r = upload_vec(b, &b->d_rec, rec)) return r;
+  if (int r = zeros(b, &b->d_waves_h, (size_t)G * std::max(b->nwaves_total, 1) * 2)) return r;
+  if (int r = zeros(b, &b->d_waves_e, (size_t)G * std::max(b->nwaves_total, 1) * 2)) return r;
+  if (int r = zeros(b, &b->d_phase, (size_t)G * std::max(b->nslots_total, 1) * 2)) return r;
+  b->shape = sh;
+  return 0;
+}
+
+template <typename T, int TW, int TH>
+void launch_step(fdtd_batch *b, int m) {
+  te_step_kernel<T, TW, TH><<<b->blocks, THREADS, 0, b->stream>>>(
+      (const TeInst<T> *)b->d_insts, b->d_tile_inst, b->ntiles, b->d_hbucket, b->d_ebucket,
+      b->d_hgroups, b->d_egroups, b->d_entries,
+      b->d_waves_h + 2LL * m * b->nwaves_total, b->d_waves_e + 2LL * m * b->nwaves_total, m);
+}
+
+template <typename T>
+void step_by_shape(fdtd_batch *b, int m) {
+  switch (b->shape) {
+    case 0: launch_step<T, 32, 8>(b, m); break;
+    case 1: launch_step<T, 32, 16>(b, m); break;
+    case 2: launch_step<T, 64, 4>(b, m); break;
+    case 3: launch_step<T, 64, 8>(b, m); break;
+    case 4: launch_step<T, 128, 2>(b, m); break;
+    default: launch_step<T, 128, 4>(b, m); break;
+  }
+}
+
+template <typename T>
+int occupancy(fdtd_batch *b) {
+  int per = 1;
+  switch (b->shape) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 32, 8>, THREADS, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 32, 16>, THREADS, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 64, 4>, THREADS, 0); break;
+    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 64, 8>, THREADS, 0); break;
+    case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 128, 2>, THREADS, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 128, 4>, THREADS, 0); break;
+  }
+  return std::max(per, 1);
+}
+
+// `count` (<= G) steps of the current tables on the batch's stream; then the instances advance.
+template <typename T>
+void enqueue(fdtd_batch *b, int count) {
+  TeInst<T> *insts = (TeInst<T> *)b->d_insts;
+  const int n = (int)b->ctxs.size();
+  if (b->nwave_items > 0) {
+    int total = b->nwave_items * G;
+    te_waves_kernel<T><<<(total + 127) / 128, 128, 0, b->stream>>>(
+        insts, b->d_wave_items, b->nwave_items, b->d_waves, b->d_point, b->nwaves_total,
+        b->d_waves_h, b->d_waves_e);
+    b->launches++;
+  }
+  if (b->nslot_items > 0) {
+    int total = b->nslot_items * G;
+    te_phase_kernel<T><<<(total + 127) / 128, 128, 0, b->stream>>>(
+        insts, b->d_slot_items, b->nslot_items, b->nslots_total, b->d_phase);
+    b->launches++;
+  }
+  for (int m = 0; m < count; m++) {
+    step_by_shape<T>(b, m);
+    b->launches++;
+    if (b->nrec > 0) {
+      te_record_kernel<T><<<(unsigned)((b->nrec + 255) / 256), 256, 0, b->stream>>>(
+          insts, b->d_rec, b->nrec, b->d_phase, b->nslots_total, m);
+      b->launches++;
+    }
+  }
+  te_advance_kernel<T><<<(n + 127) / 128, 128, 0, b->stream>>>(insts, n, count);
+  b->launches++;
+}
+
+template <typename T>
+int run_impl(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
+  const int n = (int)b->ctxs.size();
+  std::vector<InstanceView> views(n);
+  std::vector<int64_t> first(n);
+  std::vector<int> parity(n);
+  std::vector<double *> rows(n, nullptr);
+  int dev = 0;
+  BTRY(b, cudaGetDevice(&dev));
+  BTRY(b, cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev));
+  for (int i = 0; i < n; i++) {
+    fdtd_ctx *c = b->ctxs[i];
+    if (int r = fdtd_instance_view(c, &views[i]))
+      return bfail(b, r, "simulation %d: %s", i, fdtd_last_error(c));
+    const InstanceView &v = views[i];
+    if (int r = admissible(b, v, i)) return r;
+    if (int r = fdtd_instance_reserve(c, steps, &rows[i]))
+      return bfail(b, r, "simulation %d: %s", i, fdtd_last_error(c));
+    first[i] = first_steps ? first_steps[i] : 0;
+    parity[i] = v.parity;
+    BTRY(b, cudaStreamSynchronize(v.stream));
+    BTRY(b, cudaMemsetAsync(b->d_bad, 0, 4, b->stream));
+    te_tm_check_kernel<T><<<(unsigned)((v.N + 255) / 256), 256, 0, b->stream>>>(
+        (const T *)v.e[v.parity], (const T *)v.h[v.parity], v.N, b->d_bad);
+    int bad = 0;
+    BTRY(b, cudaMemcpyAsync(&bad, b->d_bad, 4, cudaMemcpyDeviceToHost, b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    if (bad)
+      return bfail(b, FDTD_E_INVALID,
+                   "simulation %d has H_x, H_y or E_z values: the batch steps TE fields only", i);
+    // the other copy's TM components stay zero too
+    const size_t E = sizeof(T);
+    BTRY(b, cudaMemsetAsync((char *)v.h[1 - v.parity], 0, 2 * v.N * E, b->stream));
+    BTRY(b, cudaMemsetAsync((char *)v.e[1 - v.parity] + 2 * v.N * E, 0, v.N * E, b->stream));
+  }
+  // where the device's descriptors have moved the instances to
+  auto pull = [&]() -> int {
+    std::vector<TeInst<T>> now(n);
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    BTRY(b, cudaMemcpy(now.data(), b->d_insts, n * sizeof(TeInst<T>), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; i++) {
+      first[i] = now[i].first;
+      parity[i] = now[i].parity;
+      rows[i] = now[i].rows;
+    }
+    return 0;
+  };
+  auto rebuild = [&](int sh) -> int {
+    if (int r = build<T>(b, views, first, parity, rows, sh)) return r;
+    b->blocks = occupancy<T>(b) * b->sms;
+    return 0;
+  };
+  int64_t done = 0;
+  // the tile shape: each shape times one chunk of real steps (after one warm chunk), the
+  // fastest is kept; every shape gives the same bits
+  if (b->shape < 0) {
+    if (steps >= 2LL * NSHAPES * G + G) {
+      float best = 1e30f;
+      int pick = 0;
+      for (int sh = 0; sh < NSHAPES; sh++) {
+        if (int r = rebuild(sh)) return r;
+        enqueue<T>(b, G);
+        BTRY(b, cudaEventRecord(b->t0, b->stream));
+        enqueue<T>(b, G);
+        BTRY(b, cudaEventRecord(b->t1, b->stream));
+        BTRY(b, cudaEventSynchronize(b->t1));
+        float ms = 0.f;
+        BTRY(b, cudaEventElapsedTime(&ms, b->t0, b->t1));
+        if (ms < best) {
+          best = ms;
+          pick = sh;
+        }
+        done += 2 * G;
+        if (int r = pull()) return r;
+      }
+      b->shape = pick;
+    } else {
+      b->shape = DEFAULT_SHAPE;
+    }
+  }
+  if (int r = rebuild(b->shape)) return r;
+  const int64_t full = (steps - done) / G;
+  if (full > 0) {
+    // one chunk captured as a graph, replayed
+    cudaGraph_t g = nullptr;
+    const long long before = b->launches;
+    BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue<T>(b, G);
+    cudaError_t err = cudaStreamEndCapture(b->stream, &g);
+    if (err != cudaSuccess)
+      return bfail(b, FDTD_E_GPU, "cudaStreamEndCapture: %s", cudaGetErrorString(err));
+    const long long per_chunk = b->launches - before;
+    b->launches = before;
+    err = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (err != cudaSuccess)
+      return bfail(b, FDTD_E_GPU, "cudaGraphInstantiate: %s", cudaGetErrorString(err));
+    for (int64_t c = 0; c < full; c++) {
+      BTRY(b, cudaGraphLaunch(b->graph, b->stream));
+      b->launches += per_chunk;
+    }
+    done += full * G;
+  }
+  if (done < steps) enqueue<T>(b, (int)(steps - done));
+  BTRY(b, cudaGetLastError());
+  BTRY(b, cudaEventRecord(b->done, b->stream));
+  for (int i = 0; i < n; i++) {
+    BTRY(b, cudaStreamWaitEvent(views[i].stream, b->done, 0));
+    fdtd_instance_advance(b->ctxs[i], steps);
+  }
+  BTRY(b, cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(int32_t count, fdtd_ctx *const *ctxs, fdtd_batch **out) {
+  if (!out) return FDTD_E_INVALID;
+  *out = nullptr;
+  fdtd_batch *b = new fdtd_batch();
+  *out = b;
+  if (count <= 0 || !ctxs) return bfail(b, FDTD_E_INVALID, "a batch needs simulations");
+  for (int i = 0; i < count; i++) {
+    if (!ctxs[i]) return bfail(b, FDTD_E_INVALID, "simulation %d has no engine", i);
+    for (int j = 0; j < i; j++)
+      if (ctxs[j] == ctxs[i]) return bfail(b, FDTD_E_INVALID, "simulation %d is in the batch twice", i);
+    b->ctxs.push_back(ctxs[i]);
+  }
+  for (int i = 0; i < count; i++) {
+    InstanceView v;
+    if (int r = fdtd_instance_view(ctxs[i], &v))
+      return bfail(b, r, "simulation %d: %s", i, fdtd_last_error(ctxs[i]));
+    if (i == 0) b->precision = v.precision;
+    if (int r = admissible(b, v, i)) return r;
+  }
+  BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BTRY(b, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  BTRY(b, cudaEventCreate(&b->t0));
+  BTRY(b, cudaEventCreate(&b->t1));
+  BTRY(b, cudaMalloc(&b->d_bad, 4));
+  return 0;
+}
+
+const char *fdtd_batch_last_error(const fdtd_batch *b) { return b ? b->error.c_str() : "no batch"; }
+
+int fdtd_batch_run(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
+  if (!b) return FDTD_E_INVALID;
+  if (steps < 0) return bfail(b, FDTD_E_INVALID, "a negative number of steps");
+  if (steps == 0) return 0;
+  int r = b->precision == 64 ? run_impl<double>(b, steps, first_steps)
+                             : run_impl<float>(b, steps, first_steps);
+  return r;
+}
+
+int fdtd_batch_tile(const fdtd_batch *b, int32_t *width, int32_t *height) {
+  if (!b || !width || !height) return FDTD_E_INVALID;
+  *width = b->shape >= 0 ? SHAPES[b->shape].tw : 0;
+  *height = b->shape >= 0 ? SHAPES[b->shape].th : 0;
+  return 0;
+}
+
+int fdtd_batch_set_tile(fdtd_batch *b, int32_t width, int32_t height) {
+  if (!b) return FDTD_E_INVALID;
+  if (width == 0 && height == 0) {
+    b->shape = -1;
+    return 0;
+  }
+  for (int s = 0; s < NSHAPES; s++)
+    if (SHAPES[s].tw == width && SHAPES[s].th == height) {
+      b->shape = s;
+      return 0;
+    }
+  return bfail(b, FDTD_E_INVALID, "no tile shape %d x %d", width, height);
+}
+
+int64_t fdtd_batch_launches(const fdtd_batch *b) { return b ? b->launches : 0; }
+
+void fdtd_batch_destroy(fdtd_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  free_tables(b);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
+  if (b->d_bad) cudaFree(b->d_bad);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+}  // extern "C"

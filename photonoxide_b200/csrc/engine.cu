@@ -31,6 +31,8 @@
 #include <vector>
 
 #include "photonoxide_fdtd.h"
+#include "common.cuh"
+#include "instance.h"
 #include "portable.h"
 
 namespace pxf {
@@ -40,28 +42,8 @@ constexpr int TY = 16;  // and along y
 constexpr int NT = 256; // threads per CTA
 constexpr int RX = TX + 2, RY = TY + 2;  // E's staged region: x0-1 .. x0+TX, y0-1 .. y0+TY
 constexpr int HX = TX + 1, HY = TY + 1;  // H's computed region: x0-1 .. x0+TX-1, y0-1 ..
-constexpr double TAU = 6.283185307179586476925286766559;
 
-struct SlabEntry {
-  int from, count;  // count 0: no slab
-  long long psi;    // where its psi starts
-  int coef;         // where its b starts (a follows after count)
-  // along x, psi's rows start at pf = from rounded down to a multiple of 4 and are pw values
-  // wide, a multiple of 4, so four places are one aligned vector (along y and z: from, count)
-  int pf, pw;
-};
 
-// A value the sources add to, with its entries (emitter, amplitude) in CPU order.
-struct Group {
-  int local;  // index in the CTA's staged region: H's (HX x HY) or E's tile (TX x TY), x fastest
-  int comp;
-  int first, count;
-};
-struct Entry {
-  double are, aim;
-  int emitter;
-  int pad;
-};
 
 struct Pole3 {
   double alpha, xi, gamma;
@@ -116,14 +98,6 @@ struct StepArgs {
   MediaArgs<T> media;
 };
 
-__host__ __device__ inline int wrap_index(int g, int n, int periodic) {
-  if (g >= 0 && g < n) return g;
-  if (periodic) {
-    if (g == n) return 0;
-    if (g == -1) return n - 1;
-  }
-  return -1;
-}
 
 // Whether value m along axis w is in a CPML slab there, and which.
 template <typename T>
@@ -1721,48 +1695,6 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 
 // The waveforms of a batch of steps, in f64 (src/fdtd.rs:329-423): for step m of the batch, w
 // at H's time t = (first+m) dt and at E's t + dt/2, 2 doubles each per emitter.
-struct Wave {
-  int kind;
-  double p[5];
-};
-// The waveforms with the reference's exp and sincos (portable.h), so the sources' values are
-// its bits: w.at(t) for a point source, the analytic form w(t) for a current.
-__device__ inline void wave_eval(const Wave &w, double t, double *re, double *im, int point) {
-  if (w.kind == 0) {
-    double u = (t - w.p[2]) / w.p[1];
-    double g = pxp::exp(-u * u);
-    double s, c;
-    if (point) {  // e^{-u^2} sin(omega (t - delay))
-      pxp::sincos((TAU * w.p[0]) * (t - w.p[2]), &s, &c);
-      *re = g * s;
-      *im = 0.0;
-    } else {  // (i e^{-u^2}) e^{-i omega (t - delay)}, as num-complex multiplies
-      pxp::sincos(-(TAU * w.p[0]) * (t - w.p[2]), &s, &c);
-      *re = 0.0 * c - g * s;
-      *im = 0.0 * s + g * c;
-    }
-  } else if (w.kind == 1) {
-    double u = (t - w.p[1]) / w.p[0];
-    *re = -u * pxp::exp(-u * u) * sqrt(2.0 * 2.718281828459045235);
-    *im = 0.0;
-  } else {
-    double ss = 1.0;
-    if (w.p[3] > 0.0) {
-      double r = fmin(fmax(t / w.p[3], 0.0), 1.0);
-      ss = r * r * (3.0 - 2.0 * r);
-    }
-    double s, c;
-    pxp::sincos(-(TAU * w.p[0]) * t, &s, &c);
-    if (point) {  // smoothstep * Re(amplitude e^{-i omega t})
-      *re = ss * (w.p[1] * c - w.p[2] * s);
-      *im = 0.0;
-    } else {  // (smoothstep amplitude) e^{-i omega t}
-      double ar = ss * w.p[1], ai = ss * w.p[2];
-      *re = ar * c - ai * s;
-      *im = ar * s + ai * c;
-    }
-  }
-}
 // point[e]: 1 if emitter e is a point source (w.at), else 0 (complex_at)
 __global__ void waves_kernel(const Wave *waves, const int *point, int nw, long long first,
                              int batch, double dt, double *out_h, double *out_e) {
@@ -1812,13 +1744,6 @@ __global__ void phase_kernel(const double *omega, const int *slot_field, int nsl
 }
 
 // sums[f][v] += sum_m ring[m][v] * phase[m][slot(f)], m in time order, f64 (monitors.rs:185-206).
-struct SeriesDev {
-  long long value0;  // first value in the ring
-  long long volume;
-  long long sum0;    // first sum (complex)
-  int nf;
-  int slot0;         // its phases' slot for frequency 0
-};
 template <typename T>
 __global__ void dft_kernel(const SeriesDev *series, int nseries, const long long *value_series,
                            long long nvalues, const T *ring, int batch, const double *phase,
@@ -1923,6 +1848,9 @@ struct fdtd_ctx {
   void *ring = nullptr;
   double *phase = nullptr;
   int ring_k = 0;
+  // the sources as last set (the batch builds its own tables from them)
+  std::vector<fdtd_waveform> src_waves;
+  std::vector<fdtd_injection> src_inj;
   // media
   bool media = false;
   MediaArgs<float> mf;
@@ -2474,6 +2402,8 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   for (int w = 0; w < nwaves; w++)
     if (waves[w].kind < 0 || waves[w].kind > 2)
       return fail(c, FDTD_E_INVALID, "waveform %d has no kind %d", w, waves[w].kind);
+  c->src_waves.assign(waves, waves + std::max(nwaves, 0));
+  c->src_inj.assign(inj, inj + std::max<int64_t>(ninj, 0));
   // Group by value in CPU order (Resident::plan, resident.rs:546-590), then by (tile, plane):
   // an H value also goes to the tiles whose low halo row or column it is.
   struct Item { long long key; int local; int comp; std::vector<int> entries; };
@@ -2958,4 +2888,81 @@ extern "C" int fdtd_upload_fields_static(fdtd_ctx *c, const double *e, const dou
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   c->fields_set = true;
   return 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// What the batch (batch.cu) reads of a context: its device buffers and tables, in place.
+
+int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
+  if (!c || !v) return FDTD_E_INVALID;
+  if (!c->coeffs_set || !c->fields_set)
+    return fail(c, FDTD_E_STATE, "upload the coefficients and the fields before a batch run");
+  v->precision = c->precision;
+  for (int a = 0; a < 3; a++) {
+    v->n[a] = c->n[a];
+    v->periodic[a] = c->periodic[a];
+    v->low[a] = c->low[a];
+    v->high[a] = c->high[a];
+    v->step[a] = c->step[a];
+  }
+  v->N = c->N;
+  v->dt = c->dt;
+  v->parity = c->parity;
+  for (int p = 0; p < 2; p++) {
+    v->e[p] = c->e[p];
+    v->h[p] = c->h[p];
+    v->psi_h[p] = c->psi_h[p];
+  }
+  v->psi_e = c->psi_e;
+  v->ca = c->lossless ? nullptr : c->ca;
+  v->cb = c->cb;
+  v->fe = c->fe;
+  v->fh = c->fh;
+  v->coefs = c->coefs;
+  memcpy(v->table, c->table, sizeof v->table);
+  v->waves = &c->src_waves;
+  v->inj = &c->src_inj;
+  v->nvalues = c->nvalues;
+  v->where = c->d_where;
+  v->series = c->d_series;
+  v->value_series = c->d_value_series;
+  v->nslots = c->nslots;
+  v->omega = c->d_omega;
+  v->slot_field = c->d_slot_field;
+  v->sums = c->sums;
+  v->nprobes = c->nprobes;
+  v->probes = c->d_probes;
+  v->media = c->media;
+  v->stream = c->stream;
+  return 0;
+}
+
+int fdtd_instance_reserve(fdtd_ctx *c, long long steps, double **rows) {
+  if (!c) return FDTD_E_INVALID;
+  *rows = nullptr;
+  if (c->nprobes == 0) return 0;
+  if (c->recorded + steps > c->record_cap) {
+    long long cap = std::max<long long>(c->recorded + steps, 2 * c->record_cap);
+    double *nr = nullptr;
+    if (int r = alloc(c, (void **)&nr, (size_t)cap * c->nprobes * 8)) return r;
+    if (c->record && c->recorded)
+      CUDA_TRY(c, cudaMemcpyAsync(nr, c->record, (size_t)c->recorded * c->nprobes * 8,
+                                  cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    release(c, c->record);
+    c->record = nr;
+    c->record_cap = cap;
+  }
+  *rows = c->record + c->recorded * c->nprobes;
+  return 0;
+}
+
+void fdtd_instance_advance(fdtd_ctx *c, long long steps) {
+  if (!c) return;
+  if (steps & 1) c->parity = 1 - c->parity;
+  if (c->nprobes > 0) c->recorded += steps;
+}
+
+int fdtd_instance_fail(fdtd_ctx *c, int code, const char *what) {
+  return c ? fail(c, code, "%s", what) : code;
 }

@@ -14,6 +14,7 @@
 
 #include "photonoxide_fdtd.h"
 #include "photonoxide_sim.h"
+#include "photonoxide_batch.h"
 #include "portable.h"
 
 namespace {
@@ -506,12 +507,22 @@ struct pxs_sim {
     return 0;
   }
 
-  int run(int64_t count) {
-    if (count <= 0) return 0;
+  // The engine made, the sources, probes and transforms set, the fields on the device.
+  int prepare() {
     if (int r = ensure_engine()) return r;
     if (int r = configure()) return r;
-    if (int r = push_fields()) return r;
+    return push_fields();
+  }
+
+  int run(int64_t count) {
+    if (count <= 0) return 0;
+    if (int r = prepare()) return r;
     if (int r = fdtd_run(ctx, count, steps)) return fail(r, "%s", fdtd_last_error(ctx));
+    return finish(count);
+  }
+
+  // After `count` steps on the device (fdtd_run or a batch): the count, the probes' values.
+  int finish(int64_t count) {
     host_fresh = false;
     steps += count;
     if (!probes.empty()) {
@@ -1166,5 +1177,91 @@ int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out) {
 }
 
 fdtd_ctx *pxs_engine(pxs_sim *s) { return s ? s->ctx : nullptr; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Batches of simulations (photonoxide_batch.h) at the level of this API: each simulation's
+// engine is set up as for pxs_run before the batch steps it, and its step count and probes are
+// brought up to date after.
+
+struct pxs_batch {
+  std::string error;
+  std::vector<pxs_sim *> sims;
+  fdtd_batch *batch = nullptr;
+};
+
+extern "C" {
+
+int pxs_batch_create(int32_t count, pxs_sim *const *sims, pxs_batch **out) {
+  if (!out) return FDTD_E_INVALID;
+  pxs_batch *b = new pxs_batch();
+  *out = b;
+  if (count <= 0 || !sims) {
+    b->error = "a batch needs simulations";
+    return FDTD_E_INVALID;
+  }
+  std::vector<fdtd_ctx *> ctxs;
+  for (int i = 0; i < count; i++) {
+    if (!sims[i]) {
+      b->error = "a batch's simulation is missing";
+      return FDTD_E_INVALID;
+    }
+    if (int r = sims[i]->prepare()) {
+      b->error = "simulation " + std::to_string(i) + ": " + sims[i]->error;
+      return r;
+    }
+    b->sims.push_back(sims[i]);
+    ctxs.push_back(sims[i]->ctx);
+  }
+  int r = fdtd_batch_create(count, ctxs.data(), &b->batch);
+  if (r) b->error = fdtd_batch_last_error(b->batch);
+  return r;
+}
+
+const char *pxs_batch_last_error(const pxs_batch *b) { return b ? b->error.c_str() : "no batch"; }
+
+int pxs_batch_run(pxs_batch *b, int64_t steps) {
+  if (!b || !b->batch) return FDTD_E_INVALID;
+  if (steps <= 0) return 0;
+  std::vector<int64_t> first;
+  for (size_t i = 0; i < b->sims.size(); i++) {
+    pxs_sim *s = b->sims[i];
+    if (int r = s->prepare()) {
+      b->error = "simulation " + std::to_string(i) + ": " + s->error;
+      return r;
+    }
+    first.push_back(s->steps);
+  }
+  if (int r = fdtd_batch_run(b->batch, steps, first.data())) {
+    b->error = fdtd_batch_last_error(b->batch);
+    return r;
+  }
+  for (size_t i = 0; i < b->sims.size(); i++)
+    if (int r = b->sims[i]->finish(steps)) {
+      b->error = "simulation " + std::to_string(i) + ": " + b->sims[i]->error;
+      return r;
+    }
+  return 0;
+}
+
+int pxs_batch_tile(const pxs_batch *b, int32_t *width, int32_t *height) {
+  return b ? fdtd_batch_tile(b->batch, width, height) : FDTD_E_INVALID;
+}
+
+int pxs_batch_set_tile(pxs_batch *b, int32_t width, int32_t height) {
+  if (!b) return FDTD_E_INVALID;
+  int r = fdtd_batch_set_tile(b->batch, width, height);
+  if (r) b->error = fdtd_batch_last_error(b->batch);
+  return r;
+}
+
+int64_t pxs_batch_launches(const pxs_batch *b) { return b ? fdtd_batch_launches(b->batch) : 0; }
+
+void pxs_batch_destroy(pxs_batch *b) {
+  if (!b) return;
+  fdtd_batch_destroy(b->batch);
+  delete b;
+}
 
 }  // extern "C"
