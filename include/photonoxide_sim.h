@@ -103,6 +103,23 @@ int pxs_batch_set_tile(pxs_batch *b, int32_t width, int32_t height);
 int64_t pxs_batch_launches(const pxs_batch *b);
 void pxs_batch_destroy(pxs_batch *b);
 
+/* The derivative of pxs_flux(s, n)'s value at frequency f by the real and imaginary parts of
+ * every transform sum, times scale, ADDED into grad (pxs_transforms' layout, complex
+ * interleaved). No counterpart in the reference, whose adjoint sources come from its own terms
+ * (src/fdtd/adjoint.rs:704-734). */
+int pxs_flux_gradient(pxs_sim *s, int32_t n, int32_t f, double scale, double *grad);
+
+/* The time-reversed adjoint (photonoxide_adjoint.h) of the next `steps` steps of a 2D TE
+ * simulation: pxs_adjoint_forward runs them (the simulation then reads out as after pxs_run),
+ * pxs_adjoint_backward gives dJ/dcb at the design values from dJ/dtransforms. */
+typedef struct pxs_adjoint pxs_adjoint;
+int pxs_adjoint_create(pxs_sim *s, int64_t steps, int32_t segment, int64_t count,
+                       const int32_t *component, const int64_t *r, pxs_adjoint **out);
+const char *pxs_adjoint_last_error(const pxs_adjoint *a);
+int pxs_adjoint_forward(pxs_adjoint *a);
+int pxs_adjoint_backward(pxs_adjoint *a, const double *grad_sums, double *grad_cb);
+void pxs_adjoint_destroy(pxs_adjoint *a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,7 @@
 
 #include "common.cuh"
 #include "instance.h"
+#include "photonoxide_adjoint.h"
 #include "photonoxide_batch.h"
 
 namespace pxb {
@@ -331,6 +332,259 @@ __global__ void te_tm_check_kernel(const T *e, const T *h, long long N, int *bad
   if (h[q] != T(0) || h[N + q] != T(0) || e[2 * N + q] != T(0)) atomicOr(bad, 1);
 }
 
+// After step m of a chunk: the curl E's update multiplies by cb, at each design value (its
+// component 0 or 1 and index: component * N + r), from the new H_z: the derivative of the new E
+// by cb where no CPML, source or medium is (those the adjoint's caller keeps off the design).
+template <typename T>
+__global__ void te_design_kernel(const TeInst<T> *insts, const long long *design, long long n,
+                                 T *K, long long k_first, int m) {
+  long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  const TeInst<T> &I = insts[0];
+  const T *hz = I.h[(I.parity + m + 1) & 1] + 2 * I.N;
+  const long long place = design[d];
+  const int comp = (int)(place / I.N);
+  const long long r = place % I.N;
+  const int x = (int)(r % I.nx), y = (int)(r / I.nx);
+  T curl;
+  if (comp == 0) {
+    const int ym = wrap_index(y - 1, I.ny, I.py);
+    const T below = ym >= 0 ? hz[(long long)ym * I.nx + x] : T(0);
+    curl = (hz[r] - below) * I.fe[I.nx + y];
+  } else {
+    const int xm = wrap_index(x - 1, I.nx, I.px);
+    const T left = xm >= 0 ? hz[(long long)y * I.nx + xm] : T(0);
+    curl = T(0) - (hz[r] - left) * I.fe[x];
+  }
+  K[(I.first + m - k_first) * n + d] = curl;
+}
+
+// ------------------------------------------------------------------------------------------
+// The time-reversed adjoint of the TE step. The step is linear in (E, H_z, psi), so the
+// gradient of J(transform sums) reverses it: with the adjoint state (E~, H~, psi~) of the
+// values after step n, the adjoint of the values before it is the step's transpose applied to
+// them. Its stencil is the step's with the roles of the fields swapped: H~ at a cell gathers
+// from E~ at the cell and at the cells above along x and y (where the step's E read this H_z),
+// then E~ gathers from H~ at the cell and the cells below (where the step's H_z read this E) --
+// so a tile computes H~ over itself and the row and column below it, then E~ on its cells,
+// exactly as the forward step does. All adjoint copies are ping-ponged.
+template <typename T>
+struct AdjState {
+  T *e[2];    // E~_x, E~_y: 2N
+  T *h[2];    // H~_z: N
+  T *pe[2];   // psi~ of E's slabs, laid out as psi_e
+  T *ph[2];   // psi~ of H's slabs, laid out as psi_h
+  int cur;
+};
+
+template <typename T>
+__device__ __forceinline__ T coef_b(const TeInst<T> &I, const SlabEntry &s, int m) {
+  return I.coefs[s.coef + (m - s.from)];
+}
+template <typename T>
+__device__ __forceinline__ T coef_a(const TeInst<T> &I, const SlabEntry &s, int m) {
+  return I.coefs[s.coef + s.count + (m - s.from)];
+}
+
+template <typename T, int TW, int TH>
+__global__ void __launch_bounds__(THREADS) te_adjoint_kernel(const TeInst<T> *insts,
+                                                             AdjState<T> A, int ntiles) {
+  constexpr int HW = TW + 1, HH = TH + 1;
+  __shared__ T sh[HW * HH];  // H~ of the step's H_z over the tile and the row and column below
+  const TeInst<T> &I = insts[0];
+  const int nx = I.nx, ny = I.ny;
+  const long long N = I.N;
+  const T *eb = A.e[A.cur];
+  T *eo = A.e[1 - A.cur];
+  const T *hb = A.h[A.cur];
+  T *ho = A.h[1 - A.cur];
+  const T *pei = A.pe[A.cur];
+  T *peo = A.pe[1 - A.cur];
+  const T *phi = A.ph[A.cur];
+  T *pho = A.ph[1 - A.cur];
+  // psi~ of an E slab value in total: what the later steps carried, plus this step's use of it
+  // (E_x += cb (+psi') along y; E_y += cb (-psi') along x)
+  auto psi_ex_total = [&](int x, int y, long long r, const SlabEntry &s) -> T {
+    return pei[s.psi + (long long)(y - s.from) * nx + x] + I.cb[r] * eb[r];
+  };
+  auto psi_ey_total = [&](int x, int y, long long r, const SlabEntry &s) -> T {
+    return pei[s.psi + (long long)y * s.pw + (x - s.pf)] - I.cb[N + r] * eb[N + r];
+  };
+  // psi~ of an H slab value in total (H_z -= dt (+psi') along x, H_z -= dt (-psi') along y)
+  auto psi_hx_total = [&](int x, int y, T hbar, const SlabEntry &s) -> T {
+    return phi[s.psi + (long long)y * s.pw + (x - s.pf)] - I.dt * hbar;
+  };
+  auto psi_hy_total = [&](int x, int y, T hbar, const SlabEntry &s) -> T {
+    return phi[s.psi + (long long)(y - s.from) * nx + x] + I.dt * hbar;
+  };
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int x0 = (t % I.tiles_x) * TW, y0 = (t / I.tiles_x) * TH;
+    // -- H~ of the step's new H_z (total)
+    for (int q = threadIdx.x; q < HW * HH; q += THREADS) {
+      const int lx = q % HW, ly = q / HW;
+      const int x = x0 - 1 + lx, y = y0 - 1 + ly;
+      const int mx = wrap_index(x, nx, I.px), my = wrap_index(y, ny, I.py);
+      T acc = T(0);
+      if (mx >= 0 && my >= 0 && x < nx && y < ny) {
+        const bool own = lx >= 1 && ly >= 1;
+        const int mxp = wrap_index(mx + 1, nx, I.px), myp = wrap_index(my + 1, ny, I.py);
+        const long long r = (long long)my * nx + mx;
+        // E_x(x, y) read H_z(x, y) with cb fey(y), E_x(x, y+1) with -cb fey(y+1); E_y(x, y) with
+        // -cb fex(x), E_y(x+1, y) with +cb fex(x+1)
+        acc = hb[r] + I.cb[r] * I.fe[nx + my] * eb[r] - I.cb[N + r] * I.fe[mx] * eb[N + r];
+        if (myp >= 0) {
+          const long long rp = (long long)myp * nx + mx;
+          acc = acc - I.cb[rp] * I.fe[nx + myp] * eb[rp];
+        }
+        if (mxp >= 0) {
+          const long long rp = (long long)my * nx + mxp;
+          acc = acc + I.cb[N + rp] * I.fe[mxp] * eb[N + rp];
+        }
+        // the E slabs: psi' = b psi + (a/h) (difference of H_z)
+        if (!I.py) {
+          const SlabEntry &s0 = I.ey[my < ny / 2 ? 0 : 1];
+          if (in_slab(s0, my)) {
+            const T tot = psi_ex_total(mx, my, r, s0);
+            acc = acc + coef_a(I, s0, my) / I.sy * tot;
+            if (own) peo[s0.psi + (long long)(my - s0.from) * nx + mx] = coef_b(I, s0, my) * tot;
+          }
+          if (myp >= 0) {
+            const SlabEntry &s1 = I.ey[myp < ny / 2 ? 0 : 1];
+            if (in_slab(s1, myp)) {
+              const long long rp = (long long)myp * nx + mx;
+              acc = acc - coef_a(I, s1, myp) / I.sy * psi_ex_total(mx, myp, rp, s1);
+            }
+          }
+        }
+        if (!I.px) {
+          const SlabEntry &s0 = I.ex[mx < nx / 2 ? 0 : 1];
+          if (in_slab(s0, mx)) {
+            const T tot = psi_ey_total(mx, my, r, s0);
+            acc = acc + coef_a(I, s0, mx) / I.sx * tot;
+            if (own) peo[s0.psi + (long long)my * s0.pw + (mx - s0.pf)] = coef_b(I, s0, mx) * tot;
+          }
+          if (mxp >= 0) {
+            const SlabEntry &s1 = I.ex[mxp < nx / 2 ? 0 : 1];
+            if (in_slab(s1, mxp)) {
+              const long long rp = (long long)my * nx + mxp;
+              acc = acc - coef_a(I, s1, mxp) / I.sx * psi_ey_total(mxp, my, rp, s1);
+            }
+          }
+        }
+        if (own) ho[r] = acc;
+      }
+      sh[q] = acc;
+    }
+    __syncthreads();
+    // -- E~ of the values before the step, on the tile
+    for (int q = threadIdx.x; q < TW * TH; q += THREADS) {
+      const int lx = q % TW + 1, ly = q / TW + 1;
+      const int x = x0 + lx - 1, y = y0 + ly - 1;
+      if (x >= nx || y >= ny) continue;
+      const long long r = (long long)y * nx + x;
+      const T hc = sh[ly * HW + lx], hy = sh[(ly - 1) * HW + lx], hx = sh[ly * HW + lx - 1];
+      const int xm = wrap_index(x - 1, nx, I.px), ym = wrap_index(y - 1, ny, I.py);
+      const T cbx = I.cb[r], cby = I.cb[N + r];
+      T cax, cay;
+      if (I.ca) {
+        cax = I.ca[r];
+        cay = I.ca[N + r];
+      } else {
+        cax = cbx == T(0) ? T(0) : T(1);
+        cay = cby == T(0) ? T(0) : T(1);
+      }
+      // H_z(x, y) read E_x(x, y) with -dt fhy(y) and E_y(x, y) with +dt fhx(x); H_z(x, y-1)
+      // read E_x(x, y) with +dt fhy(y-1); H_z(x-1, y) read E_y(x, y) with -dt fhx(x-1)
+      T ax = cax * eb[r] - I.dt * I.fh[nx + y] * hc;
+      T ay = cay * eb[N + r] + I.dt * I.fh[x] * hc;
+      if (ym >= 0) ax = ax + I.dt * I.fh[nx + ym] * hy;
+      if (xm >= 0) ay = ay - I.dt * I.fh[xm] * hx;
+      if (!I.py) {
+        const SlabEntry &s0 = I.hy[y < ny / 2 ? 0 : 1];
+        if (in_slab(s0, y)) {
+          const T tot = psi_hy_total(x, y, hc, s0);
+          ax = ax - coef_a(I, s0, y) / I.sy * tot;
+          pho[s0.psi + (long long)(y - s0.from) * nx + x] = coef_b(I, s0, y) * tot;
+        }
+        if (ym >= 0) {
+          const SlabEntry &s1 = I.hy[ym < ny / 2 ? 0 : 1];
+          if (in_slab(s1, ym)) ax = ax + coef_a(I, s1, ym) / I.sy * psi_hy_total(x, ym, hy, s1);
+        }
+      }
+      if (!I.px) {
+        const SlabEntry &s0 = I.hx[x < nx / 2 ? 0 : 1];
+        if (in_slab(s0, x)) {
+          const T tot = psi_hx_total(x, y, hc, s0);
+          ay = ay - coef_a(I, s0, x) / I.sx * tot;
+          pho[s0.psi + (long long)y * s0.pw + (x - s0.pf)] = coef_b(I, s0, x) * tot;
+        }
+        if (xm >= 0) {
+          const SlabEntry &s1 = I.hx[xm < nx / 2 ? 0 : 1];
+          if (in_slab(s1, xm)) ay = ay + coef_a(I, s1, xm) / I.sx * psi_hx_total(xm, y, hx, s1);
+        }
+      }
+      eo[r] = ax;
+      eo[N + r] = ay;
+    }
+    __syncthreads();
+  }
+}
+
+// The transform phases of one segment's steps, [m][slot] (as te_phase_kernel).
+template <typename T>
+__global__ void te_segment_phase_kernel(const TeInst<T> *insts, long long first, int steps,
+                                        double *phase) {
+  const TeInst<T> &I = insts[0];
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= steps * I.nslots) return;
+  const int m = q / I.nslots, s = q % I.nslots;
+  const double te = (double)(first + m + 1) * I.dt64;
+  const double t = I.slot_field[s] ? te - 0.5 * I.dt64 : te;
+  double sn, cs;
+  pxp::sincos(I.omega[s] * t, &sn, &cs);
+  phase[2 * (long long)q] = cs * I.dt64;
+  phase[2 * (long long)q + 1] = sn * I.dt64;
+}
+
+// Step m's direct part of J's derivative: the transforms took F dt e^{i w t} of each value, so
+// dJ/dF = sum over frequencies of dJ/dRe(sum) Re(phase) + dJ/dIm(sum) Im(phase), added to E~
+// or H~ of the value (TE components only: the others are zero whatever the permittivity).
+template <typename T>
+__global__ void te_inject_kernel(const TeInst<T> *insts, const RecItem *items, long long nitems,
+                                 const double *phase, const double *grad_sums, AdjState<T> A,
+                                 int m) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nitems) return;
+  const RecItem it = items[q];
+  if (it.kind != 0) return;
+  const TeInst<T> &I = insts[0];
+  const long long v = it.index;
+  const long long w = I.where[v];
+  const bool hfield = (w >> 62) != 0;
+  const long long place = w & ((1LL << 62) - 1);
+  const int comp = (int)(place / I.N);
+  if (hfield ? comp != 2 : comp == 2) return;
+  const SeriesDev s = I.series[I.value_series[v]];
+  const long long o = v - s.value0;
+  const double *ph = phase + 2 * ((long long)m * I.nslots + s.slot0);
+  double x = 0.0;
+  for (int k = 0; k < s.nf; k++) {
+    const double *g = grad_sums + 2 * (s.sum0 + (long long)k * s.volume + o);
+    x += g[0] * ph[2 * k] + g[1] * ph[2 * k + 1];
+  }
+  if (hfield) atomicAdd(A.h[A.cur] + (place - 2 * I.N), (T)x);
+  else atomicAdd(A.e[A.cur] + place, (T)x);
+}
+
+// dJ/dcb at each design value += E~ (of the values after the step) x the step's curl there.
+template <typename T>
+__global__ void te_grad_kernel(const long long *design, long long n, const T *K, AdjState<T> A,
+                               double *grad) {
+  long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  grad[d] += (double)A.e[A.cur][design[d]] * (double)K[d];
+}
+
 struct Shape {
   int tw, th;
 };
@@ -369,6 +623,13 @@ struct fdtd_batch {
   long long nrec = 0;
   int blocks = 0;
   int *d_bad = nullptr;  // the TE check's flag
+  // for the adjoint's recomputation: transforms and probes off, and after each step the E curl
+  // at the design's values into K[step - k_first][value]
+  bool record = true;
+  const long long *d_design = nullptr;
+  long long ndesign = 0;
+  void *d_K = nullptr;
+  long long k_first = 0;
 };
 
 namespace {
@@ -656,7 +917,7 @@ void enqueue(fdtd_batch *b, int count) {
         b->d_waves_h, b->d_waves_e);
     b->launches++;
   }
-  if (b->nslot_items > 0) {
+  if (b->nslot_items > 0 && b->record) {
     int total = b->nslot_items * G;
     te_phase_kernel<T><<<(total + 127) / 128, 128, 0, b->stream>>>(
         insts, b->d_slot_items, b->nslot_items, b->nslots_total, b->d_phase);
@@ -665,9 +926,14 @@ void enqueue(fdtd_batch *b, int count) {
   for (int m = 0; m < count; m++) {
     step_by_shape<T>(b, m);
     b->launches++;
-    if (b->nrec > 0) {
+    if (b->nrec > 0 && b->record) {
       te_record_kernel<T><<<(unsigned)((b->nrec + 255) / 256), 256, 0, b->stream>>>(
           insts, b->d_rec, b->nrec, b->d_phase, b->nslots_total, m);
+      b->launches++;
+    }
+    if (b->ndesign > 0) {
+      te_design_kernel<T><<<(unsigned)((b->ndesign + 255) / 256), 256, 0, b->stream>>>(
+          insts, b->d_design, b->ndesign, (T *)b->d_K, b->k_first, m);
       b->launches++;
     }
   }
@@ -864,6 +1130,275 @@ void fdtd_batch_destroy(fdtd_batch *b) {
   if (b->d_bad) cudaFree(b->d_bad);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The adjoint of one 2D TE simulation's run (include/photonoxide_adjoint.h): the forward steps
+// keep a checkpoint at the start of each segment; the reverse pass recomputes each segment from
+// its checkpoint (keeping the curls at the design's values), then steps the adjoint back through
+// it, adding E~ x curl into dJ/dcb.
+
+struct fdtd_adjoint {
+  std::string error;
+  fdtd_ctx *ctx = nullptr;
+  fdtd_batch *batch = nullptr;  // the simulation alone, for its forward steps
+  int precision = 32;
+  int64_t steps = 0;
+  int segment = 0;
+  int nseg = 0;
+  int64_t first = 0;  // the forward run's first step index
+  bool forward_done = false;
+  long long ndesign = 0;
+  long long *d_design = nullptr;
+  void *d_K = nullptr;          // segment x ndesign curls
+  double *d_grad = nullptr;     // ndesign
+  double *d_gsums = nullptr;    // dJ/dsums
+  double *d_phase = nullptr;    // segment x nslots phases
+  // checkpoints: E_x, E_y, H_z, H's psi and E's psi at the start of each segment, and at the end
+  void *d_ckpt = nullptr;
+  size_t ckpt_bytes = 0;
+  // the adjoint state: E~ (2N), H~ (N), psi~ (E's, H's), two copies
+  void *d_adj = nullptr;
+  long long N = 0, psi_e_len = 0, psi_h_len = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int afail(fdtd_adjoint *a, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  a->error = buf;
+  return code;
+}
+
+#define ATRY(a, call)                                                                     \
+  do {                                                                                    \
+    cudaError_t err_ = (call);                                                            \
+    if (err_ != cudaSuccess)                                                              \
+      return afail((a), FDTD_E_GPU, "%s: %s", #call, cudaGetErrorString(err_));           \
+  } while (0)
+
+int amalloc(fdtd_adjoint *a, void **p, size_t bytes) {
+  *p = nullptr;
+  ATRY(a, cudaMalloc(p, std::max<size_t>(bytes, 16)));
+  a->allocs.push_back(*p);
+  return 0;
+}
+
+// Copies the simulation's state (its current copies) into checkpoint k, or back from it.
+int checkpoint(fdtd_adjoint *a, int k, bool save) {
+  InstanceView v;
+  if (int r = fdtd_instance_view(a->ctx, &v)) return afail(a, r, "%s", fdtd_last_error(a->ctx));
+  const size_t E = a->precision == 64 ? 8 : 4;
+  char *base = (char *)a->d_ckpt + (size_t)k * a->ckpt_bytes;
+  struct Part {
+    void *dev;
+    size_t bytes;
+  };
+  const Part parts[] = {{v.e[v.parity], 2 * v.N * E},
+                        {(char *)v.h[v.parity] + 2 * v.N * E, v.N * E},
+                        {v.psi_h[v.parity], v.psi_h_len * E},
+                        {v.psi_e, v.psi_e_len * E}};
+  size_t at = 0;
+  for (const Part &p : parts) {
+    if (p.bytes) {
+      if (save)
+        ATRY(a, cudaMemcpyAsync(base + at, p.dev, p.bytes, cudaMemcpyDeviceToDevice, v.stream));
+      else
+        ATRY(a, cudaMemcpyAsync(p.dev, base + at, p.bytes, cudaMemcpyDeviceToDevice, v.stream));
+    }
+    at += (p.bytes + 255) / 256 * 256;
+  }
+  ATRY(a, cudaStreamSynchronize(v.stream));
+  return 0;
+}
+
+// The forward run: segment by segment, each one's start kept as a checkpoint, then the end.
+int forward_impl(fdtd_adjoint *a, int64_t first) {
+  a->first = first;
+  int64_t done = 0;
+  for (int k = 0; k < a->nseg; k++) {
+    if (int r = checkpoint(a, k, true)) return r;
+    const int64_t len = std::min<int64_t>(a->segment, a->steps - done);
+    const int64_t at = first + done;
+    if (int r = fdtd_batch_run(a->batch, len, &at))
+      return afail(a, r, "%s", fdtd_batch_last_error(a->batch));
+    done += len;
+  }
+  if (int r = checkpoint(a, a->nseg, true)) return r;
+  a->forward_done = true;
+  return 0;
+}
+
+template <typename T>
+int backward_impl(fdtd_adjoint *a, const double *grad_sums, double *grad_cb) {
+  fdtd_batch *b = a->batch;
+  InstanceView v;
+  if (int r = fdtd_instance_view(a->ctx, &v)) return afail(a, r, "%s", fdtd_last_error(a->ctx));
+  const long long N = a->N;
+  // the adjoint state, from zero
+  T *base = (T *)a->d_adj;
+  AdjState<T> A;
+  const long long pe = (a->psi_e_len + 63) / 64 * 64, ph = (a->psi_h_len + 63) / 64 * 64;
+  const long long per = 3 * N + pe + ph;
+  for (int c = 0; c < 2; c++) {
+    T *p = base + c * per;
+    A.e[c] = p;
+    A.h[c] = p + 2 * N;
+    A.pe[c] = p + 3 * N;
+    A.ph[c] = p + 3 * N + pe;
+  }
+  A.cur = 0;
+  ATRY(a, cudaMemsetAsync(a->d_adj, 0, 2 * per * sizeof(T), b->stream));
+  ATRY(a, cudaMemsetAsync(a->d_grad, 0, a->ndesign * 8, b->stream));
+  if (v.nsums > 0)
+    ATRY(a, cudaMemcpyAsync(a->d_gsums, grad_sums, v.nsums * 16, cudaMemcpyHostToDevice,
+                            b->stream));
+  ATRY(a, cudaStreamSynchronize(b->stream));
+  const int TW = 64, TH = 8;
+  const int tiles = ((v.n[0] + TW - 1) / TW) * ((v.n[1] + TH - 1) / TH);
+  int per_sm = 1, dev = 0, sms = 148;
+  ATRY(a, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, te_adjoint_kernel<T, 64, 8>,
+                                                        THREADS, 0));
+  ATRY(a, cudaGetDevice(&dev));
+  ATRY(a, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = std::max(1, std::min(tiles, std::max(per_sm, 1) * sms));
+  for (int k = a->nseg - 1; k >= 0; k--) {
+    const int64_t seg0 = (int64_t)k * a->segment;
+    const int len = (int)std::min<int64_t>(a->segment, a->steps - seg0);
+    // the segment again from its checkpoint: transforms and probes off, the curls kept
+    if (int r = checkpoint(a, k, false)) return r;
+    b->record = false;
+    b->d_design = a->d_design;
+    b->ndesign = a->ndesign;
+    b->d_K = a->d_K;
+    b->k_first = a->first + seg0;
+    const int64_t at = a->first + seg0;
+    const int r = fdtd_batch_run(b, len, &at);
+    b->record = true;
+    b->d_design = nullptr;
+    b->ndesign = 0;
+    b->d_K = nullptr;
+    if (r) return afail(a, r, "%s", fdtd_batch_last_error(b));
+    fdtd_instance_advance(a->ctx, -len);  // its probe record stays as the forward run left it
+    // that run's tables (the one simulation) hold what the adjoint reads
+    const TeInst<T> *insts = (const TeInst<T> *)b->d_insts;
+    if (v.nsums > 0 && v.nslots > 0) {
+      const int total = len * v.nslots;
+      te_segment_phase_kernel<T><<<(total + 127) / 128, 128, 0, b->stream>>>(insts, at, len,
+                                                                            a->d_phase);
+    }
+    for (int m = len - 1; m >= 0; m--) {
+      if (v.nsums > 0 && b->nrec > 0)
+        te_inject_kernel<T><<<(unsigned)((b->nrec + 255) / 256), 256, 0, b->stream>>>(
+            insts, b->d_rec, b->nrec, a->d_phase, a->d_gsums, A, m);
+      te_grad_kernel<T><<<(unsigned)((a->ndesign + 255) / 256), 256, 0, b->stream>>>(
+          a->d_design, a->ndesign, (const T *)a->d_K + (long long)m * a->ndesign, A, a->d_grad);
+      te_adjoint_kernel<T, 64, 8><<<blocks, THREADS, 0, b->stream>>>(insts, A, tiles);
+      A.cur = 1 - A.cur;
+    }
+    ATRY(a, cudaGetLastError());
+  }
+  ATRY(a, cudaMemcpyAsync(grad_cb, a->d_grad, a->ndesign * 8, cudaMemcpyDeviceToHost, b->stream));
+  ATRY(a, cudaStreamSynchronize(b->stream));
+  // the simulation as the forward run left it
+  return checkpoint(a, a->nseg, false);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_adjoint_create(fdtd_ctx *ctx, int64_t steps, int32_t segment, int64_t count,
+                        const int32_t *component, const int64_t *r, fdtd_adjoint **out) {
+  if (!out) return FDTD_E_INVALID;
+  fdtd_adjoint *a = new fdtd_adjoint();
+  *out = a;
+  if (!ctx) return afail(a, FDTD_E_INVALID, "no simulation");
+  if (steps <= 0)
+    return afail(a, FDTD_E_INVALID, "an adjoint needs steps, got %lld", (long long)steps);
+  if (segment <= 0) return afail(a, FDTD_E_INVALID, "segments need steps, got %d", segment);
+  if (count <= 0 || !component || !r) return afail(a, FDTD_E_INVALID, "a design needs values");
+  a->ctx = ctx;
+  a->steps = steps;
+  a->segment = segment + (segment & 1);  // even: every checkpoint has the same current copy
+  a->nseg = (int)((steps + a->segment - 1) / a->segment);
+  InstanceView v;
+  if (int q = fdtd_instance_view(ctx, &v)) return afail(a, q, "%s", fdtd_last_error(ctx));
+  a->precision = v.precision;
+  a->N = v.N;
+  a->psi_e_len = v.psi_e_len;
+  a->psi_h_len = v.psi_h_len;
+  if (v.media) return afail(a, FDTD_E_INVALID, "the adjoint does not step dispersive media");
+  std::vector<long long> design(count);
+  for (int64_t d = 0; d < count; d++) {
+    if (component[d] < 0 || component[d] > 1 || r[d] < 0 || r[d] >= v.N)
+      return afail(a, FDTD_E_INVALID, "design value %lld is not an E_x or E_y value of the grid",
+                   (long long)d);
+    design[d] = (long long)component[d] * v.N + r[d];
+  }
+  // design values clear of the CPMLs and the electric sources: there the derivative of the new
+  // E by cb is the curl alone
+  for (const fdtd_injection &x : *v.inj)
+    if (x.field == 0)
+      for (long long d : design)
+        if ((long long)x.component * v.N + x.r == d)
+          return afail(a, FDTD_E_INVALID, "a design value carries an electric source");
+  for (long long d : design) {
+    const long long rr = d % v.N;
+    const int x = (int)(rr % v.n[0]), y = (int)(rr / v.n[0]);
+    if ((!v.periodic[0] && (x < v.low[0] || x >= v.n[0] - v.high[0])) ||
+        (!v.periodic[1] && (y < v.low[1] || y >= v.n[1] - v.high[1])))
+      return afail(a, FDTD_E_INVALID, "design value (%d, %d) is in a CPML", x, y);
+  }
+  a->ndesign = count;
+  const size_t E = v.precision == 64 ? 8 : 4;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  a->ckpt_bytes = up(2 * v.N * E) + up(v.N * E) + up(v.psi_h_len * E) + up(v.psi_e_len * E);
+  const long long pe = (v.psi_e_len + 63) / 64 * 64, ph = (v.psi_h_len + 63) / 64 * 64;
+  if (int q = amalloc(a, (void **)&a->d_design, count * 8)) return q;
+  if (int q = amalloc(a, &a->d_K, (size_t)a->segment * count * E)) return q;
+  if (int q = amalloc(a, (void **)&a->d_grad, count * 8)) return q;
+  if (int q = amalloc(a, (void **)&a->d_gsums, std::max<long long>(v.nsums, 1) * 16)) return q;
+  if (int q = amalloc(a, (void **)&a->d_phase, (size_t)a->segment * std::max(v.nslots, 1) * 16))
+    return q;
+  if (int q = amalloc(a, &a->d_ckpt, (size_t)(a->nseg + 1) * a->ckpt_bytes)) return q;
+  if (int q = amalloc(a, &a->d_adj, (size_t)2 * (3 * v.N + pe + ph) * E)) return q;
+  ATRY(a, cudaMemcpy(a->d_design, design.data(), count * 8, cudaMemcpyHostToDevice));
+  fdtd_ctx *one[1] = {ctx};
+  if (int q = fdtd_batch_create(1, one, &a->batch))
+    return afail(a, q, "%s", fdtd_batch_last_error(a->batch));
+  fdtd_batch_set_tile(a->batch, 64, 8);
+  return 0;
+}
+
+const char *fdtd_adjoint_last_error(const fdtd_adjoint *a) {
+  return a ? a->error.c_str() : "no adjoint";
+}
+
+int fdtd_adjoint_forward(fdtd_adjoint *a, int64_t first_step) {
+  if (!a || !a->batch) return FDTD_E_INVALID;
+  return forward_impl(a, first_step);
+}
+
+int fdtd_adjoint_backward(fdtd_adjoint *a, const double *grad_sums, double *grad_cb) {
+  if (!a || !a->batch || !grad_cb) return FDTD_E_INVALID;
+  if (!a->forward_done) return afail(a, FDTD_E_STATE, "run the forward steps before the adjoint");
+  return a->precision == 64 ? backward_impl<double>(a, grad_sums, grad_cb)
+                            : backward_impl<float>(a, grad_sums, grad_cb);
+}
+
+void fdtd_adjoint_destroy(fdtd_adjoint *a) {
+  if (!a) return;
+  fdtd_batch_destroy(a->batch);
+  for (void *p : a->allocs) cudaFree(p);
+  delete a;
 }
 
 }  // extern "C"

@@ -2914,6 +2914,8 @@ int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
     v->psi_h[p] = c->psi_h[p];
   }
   v->psi_e = c->psi_e;
+  v->psi_h_len = c->psi_h_len;
+  v->psi_e_len = c->psi_e_len;
   v->ca = c->lossless ? nullptr : c->ca;
   v->cb = c->cb;
   v->fe = c->fe;
@@ -2930,6 +2932,7 @@ int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
   v->omega = c->d_omega;
   v->slot_field = c->d_slot_field;
   v->sums = c->sums;
+  v->nsums = c->nvalues > 0 ? c->nsums : 0;
   v->nprobes = c->nprobes;
   v->probes = c->d_probes;
   v->media = c->media;

@@ -14,6 +14,7 @@
 
 #include "photonoxide_fdtd.h"
 #include "photonoxide_sim.h"
+#include "photonoxide_adjoint.h"
 #include "photonoxide_batch.h"
 #include "portable.h"
 
@@ -597,6 +598,83 @@ struct pxs_sim {
         }
     }
     return total * g.d[b] * g.d[c];
+  }
+
+  // Where value `at` of (field, comp) at frequency f is in the transforms laid end to end (the
+  // layout of pxs_transforms and fdtd_read_dft), as a complex index, or -1.
+  int64_t locate(size_t s0, size_t s1, int field, int comp, const int64_t at[3], int f) const {
+    int64_t base = 0;
+    for (size_t q = 0; q < s1; q++) {
+      const Series &s = series[q];
+      if (q >= s0 && s.field == field && s.comp == comp) {
+        bool in = true;
+        for (int a = 0; a < 3; a++)
+          if (at[a] < s.lo[a] || at[a] >= s.lo[a] + s.len[a]) in = false;
+        if (in) {
+          int64_t o = ((at[2] - s.lo[2]) * s.len[1] + (at[1] - s.lo[1])) * s.len[0] + at[0] - s.lo[0];
+          return base + f * s.volume() + o;
+        }
+      }
+      base += (int64_t)s.sums.size() / 2;
+    }
+    return -1;
+  }
+
+  // The derivative of face_flux(F, f) by the real and imaginary parts of each transform sum,
+  // times `scale`, added into grad (complex interleaved, the layout of pxs_transforms). The flux
+  // is bilinear: sum of w sign Re(m conj(h)) with m the mean of E over the two node planes.
+  void face_flux_grad(const FluxFace &F, int f, double scale, double *grad) const {
+    int b = first_of(F.axis), c = second_of(F.axis);
+    auto lo_of = [&](int along) {
+      int sl = along == b ? 0 : 1;
+      return F.win[sl][0] < 0 ? (int64_t)0 : F.win[sl][0];
+    };
+    auto hi_of = [&](int along) {
+      int sl = along == b ? 0 : 1;
+      return F.win[sl][0] < 0 ? g.n[along] : F.win[sl][1] + 1;
+    };
+    auto weight = [&](int along, int64_t m, bool half) {
+      int sl = along == b ? 0 : 1;
+      if (F.win[sl][0] < 0) return 1.0;
+      int64_t lo = F.win[sl][0], hi = F.win[sl][1];
+      if (half) return (lo < m && m < hi) ? 1.0 : ((m == lo || m == hi) ? 0.5 : 0.0);
+      return (lo < m && m <= hi) ? 1.0 : 0.0;
+    };
+    const double area = g.d[b] * g.d[c] * scale;
+    const int comps[2] = {b, c}, hs[2] = {c, b};
+    const double signs[2] = {0.5, -0.5};
+    for (int t = 0; t < 2; t++)
+      for (int64_t v = lo_of(c); v < hi_of(c); v++)
+        for (int64_t u = lo_of(b); u < hi_of(b); u++) {
+          double w = weight(b, u, comps[t] == b) * weight(c, v, comps[t] == c);
+          if (w == 0.0) continue;
+          int64_t at[3];
+          at[F.axis] = F.plane;
+          at[b] = u;
+          at[c] = v;
+          double lr = 0, li = 0, hr = 0, hi2 = 0, er = 0, ei = 0;
+          const int64_t il = locate(F.series0, F.series0 + 4, 0, comps[t], at, f);
+          const int64_t ih = locate(F.series0, F.series0 + 4, 1, hs[t], at, f);
+          value(F.series0, F.series0 + 4, 0, comps[t], at, f, &lr, &li);
+          value(F.series0, F.series0 + 4, 1, hs[t], at, f, &hr, &hi2);
+          at[F.axis] = F.plane + 1;
+          const int64_t ie = locate(F.series0, F.series0 + 4, 0, comps[t], at, f);
+          value(F.series0, F.series0 + 4, 0, comps[t], at, f, &er, &ei);
+          const double k = w * signs[t] * area;
+          const double mr = 0.5 * (lr + er), mi = 0.5 * (li + ei);
+          if (il >= 0) {
+            grad[2 * il] += 0.5 * k * hr;
+            grad[2 * il + 1] += 0.5 * k * hi2;
+          }
+          if (ie >= 0) {
+            grad[2 * ie] += 0.5 * k * hr;
+            grad[2 * ie + 1] += 0.5 * k * hi2;
+          }
+          if (ih >= 0) {
+            grad[2 * ih] += k * mr;
+            grad[2 * ih + 1] += k * mi;
+          }
+        }
   }
 
   int check_frequencies(int nf, const double *freqs) {
@@ -1262,6 +1340,84 @@ void pxs_batch_destroy(pxs_batch *b) {
   if (!b) return;
   fdtd_batch_destroy(b->batch);
   delete b;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// The adjoint (photonoxide_adjoint.h) at the level of this API, and the flux's derivative by the
+// transform sums that feeds it.
+
+struct pxs_adjoint {
+  std::string error;
+  pxs_sim *sim = nullptr;
+  fdtd_adjoint *adj = nullptr;
+  int64_t steps = 0;
+};
+
+extern "C" {
+
+int pxs_flux_gradient(pxs_sim *s, int32_t n, int32_t f, double scale, double *grad) {
+  if (n < 0 || n >= (int32_t)s->fluxes.size()) return s->fail(FDTD_E_INVALID, "no flux monitor %d", n);
+  if (int r = s->pull_sums()) return r;
+  const auto &faces = s->fluxes[n];
+  int nf = (int)(s->series[faces[0].series0].sums.size() / 2 / s->series[faces[0].series0].volume());
+  if (f < 0 || f >= nf) return s->fail(FDTD_E_INVALID, "flux monitor %d has no frequency %d", n, f);
+  for (auto &F : faces) s->face_flux_grad(F, f, F.sign * scale, grad);
+  return 0;
+}
+
+int pxs_adjoint_create(pxs_sim *s, int64_t steps, int32_t segment, int64_t count,
+                       const int32_t *component, const int64_t *r, pxs_adjoint **out) {
+  if (!out) return FDTD_E_INVALID;
+  pxs_adjoint *a = new pxs_adjoint();
+  *out = a;
+  if (!s) {
+    a->error = "no simulation";
+    return FDTD_E_INVALID;
+  }
+  a->sim = s;
+  a->steps = steps;
+  if (int q = s->prepare()) {
+    a->error = s->error;
+    return q;
+  }
+  int q = fdtd_adjoint_create(s->ctx, steps, segment, count, component, r, &a->adj);
+  if (q) a->error = fdtd_adjoint_last_error(a->adj);
+  return q;
+}
+
+const char *pxs_adjoint_last_error(const pxs_adjoint *a) { return a ? a->error.c_str() : "no adjoint"; }
+
+int pxs_adjoint_forward(pxs_adjoint *a) {
+  if (!a || !a->adj) return FDTD_E_INVALID;
+  pxs_sim *s = a->sim;
+  if (int q = s->prepare()) {
+    a->error = s->error;
+    return q;
+  }
+  if (int q = fdtd_adjoint_forward(a->adj, s->steps)) {
+    a->error = fdtd_adjoint_last_error(a->adj);
+    return q;
+  }
+  if (int q = s->finish(a->steps)) {
+    a->error = s->error;
+    return q;
+  }
+  return 0;
+}
+
+int pxs_adjoint_backward(pxs_adjoint *a, const double *grad_sums, double *grad_cb) {
+  if (!a || !a->adj) return FDTD_E_INVALID;
+  int q = fdtd_adjoint_backward(a->adj, grad_sums, grad_cb);
+  if (q) a->error = fdtd_adjoint_last_error(a->adj);
+  return q;
+}
+
+void pxs_adjoint_destroy(pxs_adjoint *a) {
+  if (!a) return;
+  fdtd_adjoint_destroy(a->adj);
+  delete a;
 }
 
 }  // extern "C"

@@ -16,6 +16,7 @@ struct InstanceView {
   double dt, step[3];
   int parity;  // which copy of E, H and H's psi is current
   void *e[2], *h[2], *psi_h[2], *psi_e;
+  long long psi_h_len, psi_e_len;  // values in each copy of H's psi and in E's
   const void *ca;  // null: lossless
   const void *cb, *fe, *fh, *coefs;
   pxf::SlabEntry table[2][3][3][2];
@@ -29,6 +30,7 @@ struct InstanceView {
   const double *omega;
   const int *slot_field;
   double *sums;
+  long long nsums;  // complex sums
   int nprobes;
   const long long *probes;
   bool media;
