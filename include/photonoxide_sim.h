@@ -103,6 +103,9 @@ int pxs_batch_set_tile(pxs_batch *b, int32_t width, int32_t height);
 int64_t pxs_batch_launches(const pxs_batch *b);
 void pxs_batch_destroy(pxs_batch *b);
 
+/* The dispersive media's size: out[0] E values in a medium, out[1] their poles in total. */
+int pxs_media_counts(const pxs_sim *s, int64_t *out);
+
 /* The derivative of pxs_flux(s, n)'s value at frequency f by the real and imaginary parts of
  * every transform sum, times scale, ADDED into grad (pxs_transforms' layout, complex
  * interleaved). No counterpart in the reference, whose adjoint sources come from its own terms
@@ -119,6 +122,28 @@ const char *pxs_adjoint_last_error(const pxs_adjoint *a);
 int pxs_adjoint_forward(pxs_adjoint *a);
 int pxs_adjoint_backward(pxs_adjoint *a, const double *grad_sums, double *grad_cb);
 void pxs_adjoint_destroy(pxs_adjoint *a);
+
+/* Serving: a resident loop (its own thread) that admits submitted simulations in arrival order
+ * while its slots (max_active) and device-memory budget (an estimate per job) allow, keeps them on
+ * the device and steps them together `chunk` steps at a time -- the 2D TE ones in one batch, the
+ * others each on its own stream, concurrently. A finished job's fields, probes and transforms are
+ * read back to its simulation and its device memory freed. A submitted simulation belongs to the
+ * server until its job ends: the caller must not use it meanwhile. No counterpart in the reference.
+ * Job states: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled. */
+typedef struct pxs_server pxs_server;
+int pxs_server_create(size_t hbm_budget, int32_t max_active, int64_t chunk, pxs_server **out);
+const char *pxs_server_last_error(const pxs_server *sv);
+/* returns the job's id (> 0) or a negative status */
+int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps);
+/* the job's state; times (may be NULL): submitted, started, finished (steady clock, seconds) */
+int pxs_server_poll(pxs_server *sv, int64_t id, double *times);
+int pxs_server_wait(pxs_server *sv, int64_t id);
+int pxs_server_cancel(pxs_server *sv, int64_t id);
+/* out[0] cell-updates taken, out[1] chunks stepped, out[2] device bytes admitted now */
+int pxs_server_stats(pxs_server *sv, double *out);
+/* stops the loop (between chunks) and frees the server; jobs still running are left released or
+ * not as the loop left them */
+void pxs_server_destroy(pxs_server *sv);
 
 #ifdef __cplusplus
 }

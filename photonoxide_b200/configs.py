@@ -143,3 +143,49 @@ def psi_values(grid: Grid3d, boundaries: Boundaries) -> int:
         if hasattr(e, "low"):
             total += 4 * (e.low + e.high) * (grid.cells() // grid.n(a))
     return total
+
+
+def te_design(nx: int, ny: int, precision: int = 32, steps: int = 6000, segment: int = 500,
+              design_cells: int = 100, h: float = 0.02, bandwidth: float = 0.3):
+    """Configuration 4, one instance: a 2D TE grid of nx x ny cells of 20 nm, 12-cell CPMLs, an
+    input Si strip (0.5 um) from the left CPML into a design region of design_cells^2 cells at
+    the centre and an output strip from it to the right CPML, all in SiO2. A Gaussian-profile
+    current on E_y across the input strip carries a pulse centred on 1550 nm (``bandwidth`` c/um
+    wide, so that it has passed within the run); flux monitor 0 sits across the output strip
+    (the arm) at 1550 nm. Returns the adjoint's TeProblem (design permittivities
+    eps in [1.444^2, 3.48^2] are the variables)."""
+    from .adjoint import Design2d, TeProblem
+    from .fdtd import Simulation, average
+
+    g = Grid3d(nx, ny, 1, h, h, h, -0.5 * nx * h, -0.5 * ny * h, -h / 2)
+    half = 0.5 * design_cells * h
+    boxes = (Boxes(N_SIO2 ** 2)
+             .add((-INF, -0.25, -INF), (-half, 0.25, INF), N_SI ** 2)
+             .add((half, -0.25, -INF), (INF, 0.25, INF), N_SI ** 2))
+    background = average(g, boxes)
+    d0x, d0y = nx // 2 - design_cells // 2, ny // 2 - design_cells // 2
+    design = Design2d(d0x, d0y, design_cells, design_cells)
+    src_x = 12 + 25
+    mon_x = nx - 12 - 25
+    jc = ny // 2
+    span = int(round(1.0 / h))  # the monitor's window: 1 um either side of the strip
+
+    def build(eps, prec):
+        s = Simulation(g, eps, Boundaries.cpml_2d(12), 0.5, precision=prec)
+        values = []
+        for j in range(jc - 25, jc + 26):
+            y = (j + 0.5 - ny / 2) * h
+            values.append((Axis.Y, (src_x, j, 0), complex(math.exp(-(y / 0.25) ** 2))))
+        s.add_current(Current(Field.E, values, Waveform.pulse(1.0 / 1.55, bandwidth)))
+        window = ((max(jc - span, 13), min(jc + span, ny - 14)), None)  # all of z
+        s.add_flux(FluxPlane(Axis.X, mon_x, window), [1.0 / 1.55])
+        return s
+
+    return TeProblem(g, background, design, build, steps, precision=precision, segment=segment)
+
+
+def te_design_sides(count: int = 64, seed: int = 0, lo: int = 256, hi: int = 1024):
+    """The instances' sides (nx, ny), log-uniform in [lo, hi] cells, seeded."""
+    rng = np.random.default_rng(seed)
+    return [tuple(int(v) for v in np.exp(rng.uniform(np.log(lo), np.log(hi), 2)))
+            for _ in range(count)]

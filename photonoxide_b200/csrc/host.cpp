@@ -4,12 +4,17 @@
 // through the engine's C ABI (photonoxide_fdtd.h). Compiled without floating-point contraction,
 // so every table is the reference's bits.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "photonoxide_fdtd.h"
@@ -520,6 +525,66 @@ struct pxs_sim {
     if (int r = prepare()) return r;
     if (int r = fdtd_run(ctx, count, steps)) return fail(r, "%s", fdtd_last_error(ctx));
     return finish(count);
+  }
+
+  // Everything the device holds brought to the host (fields, psi, transforms; the probes are
+  // read after each run), then the engine and its device memory released. A later run makes a
+  // new engine from the host's copies.
+  int release() {
+    if (!ctx) return 0;
+    if (int r = pull()) return r;
+    if (int r = pull_sums()) return r;
+    fdtd_destroy(ctx);
+    ctx = nullptr;
+    configured = false;
+    device_fresh = false;
+    return 0;
+  }
+
+  // An upper estimate of the device memory the engine takes (fdtd_create and the set_* calls):
+  // two copies of E and H, cb (and ca when lossy), psi (H's twice), the transforms' ring of 64
+  // steps and sums, and the media's state.
+  size_t device_bytes() const {
+    const size_t E = precision == 64 ? 8 : 4;
+    const double n = (double)N();
+    double values = 15.0 * n;
+    bool lossless = true;
+    for (int c = 0; c < 3 && lossless; c++)
+      for (int64_t r = 0; r < N(); r++)
+        if (ca[c][r] != (cb[c][r] == 0.0 ? 0.0 : 1.0)) {
+          lossless = false;
+          break;
+        }
+    if (!lossless) values += 3.0 * n;
+    for (const SlabInfo &sl : slabs) {
+      double rows = n / (double)g.n[sl.axis];
+      double width = sl.axis == 0 ? (double)(sl.count + 8) : (double)sl.count;
+      values += (sl.field == 1 ? 2.0 : 1.0) * (width * rows + 16.0);
+    }
+    double extra = 0.0;
+    for (const Series &se : series) {
+      double nf = se.volume() > 0 ? (double)se.sums.size() / 2.0 / (double)se.volume() : 0.0;
+      extra += (double)se.volume() * (64.0 * E + 8.0 * 3 + 16.0 * nf);
+    }
+    extra += 64.0 * (double)members.size();
+    return (size_t)((values * (double)E + extra) * 1.05) + (16u << 20);
+  }
+
+  // Whether the batch (photonoxide_batch.h) can step this simulation: 2D, TE fields and sources,
+  // no media.
+  bool te() const {
+    if (g.n[2] != 1 || !periodic(2) || !groups.empty()) return false;
+    for (const auto *list : {&points, &currents})
+      for (const fdtd_injection &x : *list)
+        if ((x.field == 0) == (x.component == 2)) return false;
+    const int64_t n = N();
+    if (!e.empty())
+      for (int64_t r = 0; r < n; r++)
+        if (e[2 * n + r] != 0.0) return false;
+    if (!h.empty())
+      for (int64_t r = 0; r < 2 * n; r++)
+        if (h[r] != 0.0) return false;
+    return true;
   }
 
   // After `count` steps on the device (fdtd_run or a batch): the count, the probes' values.
@@ -1357,6 +1422,15 @@ struct pxs_adjoint {
 
 extern "C" {
 
+int pxs_media_counts(const pxs_sim *s, int64_t *out) {
+  out[0] = out[1] = 0;
+  for (const MediaGroup &G : s->groups) {
+    out[0] += (int64_t)G.comp.size();
+    out[1] += (int64_t)G.comp.size() * (int64_t)(G.poles.size() / 3);
+  }
+  return 0;
+}
+
 int pxs_flux_gradient(pxs_sim *s, int32_t n, int32_t f, double scale, double *grad) {
   if (n < 0 || n >= (int32_t)s->fluxes.size()) return s->fail(FDTD_E_INVALID, "no flux monitor %d", n);
   if (int r = s->pull_sums()) return r;
@@ -1418,6 +1492,324 @@ void pxs_adjoint_destroy(pxs_adjoint *a) {
   if (!a) return;
   fdtd_adjoint_destroy(a->adj);
   delete a;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Serving: a resident loop that admits simulations (jobs) under a device-memory budget, keeps
+// the admitted ones on the device and steps them together, chunk by chunk: the 2D TE jobs in one
+// batch (one launch per step for all of them), the others each on its own stream, all in flight
+// at once. A job that has taken its steps is read back to the host and its device memory freed,
+// which admits the next. No counterpart in the reference (one Simulation at a time).
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+enum { JOB_QUEUED = 0, JOB_RUNNING = 1, JOB_DONE = 2, JOB_FAILED = 3, JOB_CANCELLED = 4 };
+
+struct ServerJob {
+  int64_t id = 0;
+  pxs_sim *sim = nullptr;
+  int64_t steps = 0, done = 0;
+  int state = JOB_QUEUED;
+  bool te = false, prepared = false;
+  size_t bytes = 0;
+  double submitted = 0, started = 0, finished = 0;
+  std::string error;
+};
+
+}  // namespace
+
+struct pxs_server {
+  std::string error;
+  size_t budget = 0, used = 0;
+  int max_active = 64;
+  int64_t chunk = 500;
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<ServerJob *> queue;
+  std::vector<ServerJob *> active;
+  std::map<int64_t, ServerJob *> jobs;
+  int64_t next_id = 1;
+  bool stop = false;
+  std::thread loop;
+  // the loop's own
+  fdtd_batch *batch = nullptr;
+  std::vector<ServerJob *> batch_jobs;
+  double cell_updates = 0.0;
+  int64_t chunks = 0;
+
+  void finish_job(ServerJob *j, int state, const std::string &why) {
+    // called with mu held
+    j->state = state;
+    j->error = why;
+    j->finished = now_s();
+    used -= j->bytes;
+  }
+
+  void run_loop() {
+    cudaSetDevice(device);
+    for (;;) {
+      std::vector<ServerJob *> admitted;
+      {
+        std::unique_lock<std::mutex> lock(mu);
+        cv.wait(lock, [&] { return stop || !queue.empty() || !active.empty(); });
+        if (stop) break;
+        // admission in arrival order, while slots and memory last
+        while (!queue.empty() && (int)active.size() < max_active) {
+          ServerJob *j = queue.front();
+          if (j->bytes > budget) {
+            queue.pop_front();
+            j->state = JOB_FAILED;
+            j->error = "the job needs more device memory than the whole budget";
+            j->finished = now_s();
+            cv.notify_all();
+            continue;
+          }
+          if (used + j->bytes > budget) break;
+          queue.pop_front();
+          used += j->bytes;
+          j->state = JOB_RUNNING;
+          j->started = now_s();
+          active.push_back(j);
+          admitted.push_back(j);
+        }
+      }
+      for (ServerJob *j : admitted) {
+        if (int r = j->sim->prepare()) {
+          std::lock_guard<std::mutex> lock(mu);
+          finish_job(j, JOB_FAILED, j->sim->error.empty() ? "setup failed" : j->sim->error);
+          (void)r;
+        } else {
+          j->prepared = true;
+        }
+      }
+      std::vector<ServerJob *> te, other;
+      {
+        std::lock_guard<std::mutex> lock(mu);
+        std::vector<ServerJob *> keep;
+        for (ServerJob *j : active) {
+          if (j->state == JOB_RUNNING && j->prepared) {
+            keep.push_back(j);
+            (j->te ? te : other).push_back(j);
+          } else if (j->state == JOB_CANCELLED && j->prepared) {
+            j->sim->release();
+          }
+        }
+        active = keep;
+        cv.notify_all();
+      }
+      if (te.empty() && other.empty()) continue;
+      // the others: each its own chunk on its own stream
+      std::vector<int64_t> took(other.size(), 0);
+      for (size_t q = 0; q < other.size(); q++) {
+        ServerJob *j = other[q];
+        took[q] = std::min(chunk, j->steps - j->done);
+        if (fdtd_run_async(j->sim->ctx, took[q], j->sim->steps)) {
+          std::string why = fdtd_last_error(j->sim->ctx);
+          std::lock_guard<std::mutex> lock(mu);
+          j->sim->release();
+          finish_job(j, JOB_FAILED, why);
+          took[q] = -1;
+        }
+      }
+      // the 2D TE jobs: one batch (remade when its members change), as many steps as the job
+      // nearest its end still needs (none overshoots)
+      int64_t te_took = 0;
+      if (!te.empty()) {
+        if (te != batch_jobs) {
+          fdtd_batch_destroy(batch);
+          batch = nullptr;
+          std::vector<fdtd_ctx *> ctxs;
+          for (ServerJob *j : te) ctxs.push_back(j->sim->ctx);
+          if (fdtd_batch_create((int32_t)ctxs.size(), ctxs.data(), &batch)) {
+            std::string why = fdtd_batch_last_error(batch);
+            fdtd_batch_destroy(batch);
+            batch = nullptr;
+            batch_jobs.clear();
+            std::lock_guard<std::mutex> lock(mu);
+            for (ServerJob *j : te) {
+              j->sim->release();
+              finish_job(j, JOB_FAILED, why);
+            }
+            te.clear();
+          } else {
+            fdtd_batch_set_tile(batch, 32, 16);
+            batch_jobs = te;
+          }
+        }
+        if (!te.empty()) {
+          te_took = chunk;
+          std::vector<int64_t> first;
+          for (ServerJob *j : te) {
+            te_took = std::min(te_took, j->steps - j->done);
+            first.push_back(j->sim->steps);
+          }
+          if (fdtd_batch_run(batch, te_took, first.data())) {
+            std::string why = fdtd_batch_last_error(batch);
+            std::lock_guard<std::mutex> lock(mu);
+            for (ServerJob *j : te) {
+              j->sim->release();
+              finish_job(j, JOB_FAILED, why);
+            }
+            te.clear();
+            te_took = 0;
+          }
+        }
+      }
+      for (size_t q = 0; q < other.size(); q++)
+        if (took[q] > 0) fdtd_synchronize(other[q]->sim->ctx);
+      // bookkeeping; finished jobs read back and their memory freed
+      std::lock_guard<std::mutex> lock(mu);
+      chunks++;
+      auto advance = [&](ServerJob *j, int64_t n) {
+        if (j->state != JOB_RUNNING) return;
+        j->sim->finish(n);
+        j->done += n;
+        cell_updates += (double)n * (double)j->sim->N();
+        if (j->done >= j->steps) {
+          int r = j->sim->release();
+          finish_job(j, r ? JOB_FAILED : JOB_DONE, r ? j->sim->error : std::string());
+        }
+      };
+      for (size_t q = 0; q < other.size(); q++)
+        if (took[q] > 0) advance(other[q], took[q]);
+      for (ServerJob *j : te) advance(j, te_took);
+      std::vector<ServerJob *> keep;
+      for (ServerJob *j : active) {
+        if (j->state == JOB_RUNNING) keep.push_back(j);
+        else if (j->state == JOB_CANCELLED && j->prepared) j->sim->release();
+      }
+      active = keep;
+      cv.notify_all();
+    }
+    fdtd_batch_destroy(batch);
+    batch = nullptr;
+  }
+};
+
+extern "C" {
+
+int pxs_server_create(size_t hbm_budget, int32_t max_active, int64_t chunk, pxs_server **out) {
+  if (!out) return FDTD_E_INVALID;
+  pxs_server *sv = new pxs_server();
+  *out = sv;
+  if (hbm_budget == 0 || max_active <= 0 || chunk <= 0) {
+    sv->error = "a server needs a budget, slots and a chunk of steps";
+    return FDTD_E_INVALID;
+  }
+  sv->budget = hbm_budget;
+  sv->max_active = max_active;
+  sv->chunk = chunk;
+  cudaGetDevice(&sv->device);
+  sv->loop = std::thread([sv] { sv->run_loop(); });
+  return 0;
+}
+
+const char *pxs_server_last_error(const pxs_server *sv) { return sv ? sv->error.c_str() : "no server"; }
+
+int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps) {
+  if (!sv || !s || steps <= 0) return FDTD_E_INVALID;
+  ServerJob *j = new ServerJob();
+  j->sim = s;
+  j->steps = steps;
+  j->te = s->te();
+  j->bytes = s->device_bytes();
+  j->submitted = now_s();
+  std::lock_guard<std::mutex> lock(sv->mu);
+  for (auto &kv : sv->jobs)
+    if (kv.second->sim == s && kv.second->state <= JOB_RUNNING) {
+      delete j;
+      sv->error = "that simulation is already a job of this server";
+      return FDTD_E_INVALID;
+    }
+  j->id = sv->next_id++;
+  sv->jobs[j->id] = j;
+  sv->queue.push_back(j);
+  sv->cv.notify_all();
+  return j->id;
+}
+
+// The job's state (0 queued, 1 running, 2 done, 3 failed, 4 cancelled) and its times (seconds
+// on one steady clock: submitted, started, finished; 0 while not reached).
+int pxs_server_poll(pxs_server *sv, int64_t id, double *times) {
+  if (!sv) return FDTD_E_INVALID;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end()) {
+    sv->error = "no such job";
+    return FDTD_E_INVALID;
+  }
+  ServerJob *j = it->second;
+  if (times) {
+    times[0] = j->submitted;
+    times[1] = j->started;
+    times[2] = j->finished;
+  }
+  if (j->state == JOB_FAILED) sv->error = j->error;
+  return j->state;
+}
+
+int pxs_server_wait(pxs_server *sv, int64_t id) {
+  if (!sv) return FDTD_E_INVALID;
+  std::unique_lock<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end()) {
+    sv->error = "no such job";
+    return FDTD_E_INVALID;
+  }
+  ServerJob *j = it->second;
+  sv->cv.wait(lock, [&] { return j->state >= JOB_DONE || sv->stop; });
+  if (j->state == JOB_FAILED) sv->error = j->error;
+  return j->state;
+}
+
+int pxs_server_cancel(pxs_server *sv, int64_t id) {
+  if (!sv) return FDTD_E_INVALID;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->jobs.find(id);
+  if (it == sv->jobs.end()) return FDTD_E_INVALID;
+  ServerJob *j = it->second;
+  if (j->state == JOB_QUEUED) {
+    sv->queue.erase(std::find(sv->queue.begin(), sv->queue.end(), j));
+    j->state = JOB_CANCELLED;
+    j->finished = now_s();
+  } else if (j->state == JOB_RUNNING) {
+    // the loop releases it between chunks
+    sv->used -= j->bytes;
+    j->bytes = 0;
+    j->state = JOB_CANCELLED;
+    j->finished = now_s();
+  }
+  sv->cv.notify_all();
+  return 0;
+}
+
+// Totals so far: cell-updates taken, chunks stepped, device bytes admitted now.
+int pxs_server_stats(pxs_server *sv, double *out) {
+  if (!sv || !out) return FDTD_E_INVALID;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  out[0] = sv->cell_updates;
+  out[1] = (double)sv->chunks;
+  out[2] = (double)sv->used;
+  return 0;
+}
+
+void pxs_server_destroy(pxs_server *sv) {
+  if (!sv) return;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+    sv->cv.notify_all();
+  }
+  if (sv->loop.joinable()) sv->loop.join();
+  for (auto &kv : sv->jobs) delete kv.second;
+  delete sv;
 }
 
 }  // extern "C"
