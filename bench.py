@@ -101,6 +101,19 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def aggregate(ms, steps, cells, dist=None, device="cpu"):
+    """The slowest rank's time of a timed region (every rank steps its own replica of the grid,
+    so the job ends when the last one does) and the whole job's rate in Gcell-updates/s."""
+    world = 1
+    if dist is not None and dist.is_initialized():
+        import torch
+        world = dist.get_world_size()
+        t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, world * steps * cells / (ms / 1e3) / 1e9
+
+
 def cpu_baseline(eps, target_seconds=15.0):
     """The oracle (f64, all host threads) on the same MMI problem, timed over a bounded number
     of steps (about 10-30 s of CPU work)."""
@@ -174,10 +187,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="mmi", choices=sorted(["mmi"] + list(WORKLOADS)),
+                    help="mmi: the 3D MMI step (this benchmark's line); the others measure the "
+                         "remaining configurations, one JSON line each")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload != "mmi":
+        return WORKLOADS[args.workload](args)
 
     import torch
     import torch.distributed as dist
@@ -224,11 +242,7 @@ def main():
     kernel_ms, kernel_n = eng.profile_read()
     eng.profile(False)
     launches = eng.launches()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps * cells / (ms / 1e3) / 1e9
+    ms, value = aggregate(ms, args.steps, cells, dist if world > 1 else None, "cuda")
 
     # end to end through the C ABI: host (pinned) buffers in, the run, the results back
     N = cells
@@ -252,11 +266,7 @@ def main():
     eng.synchronize()
     wall = time.perf_counter() - wall0
     e2e_ms = max(e0.elapsed_time(e1), 0.0)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * args.steps * cells / (e2e_ms / 1e3) / 1e9
+    e2e_ms, e2e_value = aggregate(e2e_ms, args.steps, cells, dist if world > 1 else None, "cuda")
     h2d = (3 * N + 6 * N) * 8 / args.steps
     d2h = (6 * N * 8 + 16 * nsums) / args.steps
 
@@ -296,6 +306,269 @@ def main():
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# -- the other configurations -----------------------------------------------------------------
+# Each prints one JSON line. Timings of whole runs through the Python API are wall-clock around
+# a synchronized run (host work included); the kernel-level figures come from CUDA events.
+
+def _rel_l2(a, b):
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    n = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a))
+
+
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t0
+
+
+def workload_strip2d(args):
+    """Configuration 1: the 2D TE strip, 4000 steps, f32 on the GPU against f64 (the engine's
+    f64, which is the oracle's bits): relative L2 of the probe's time series and of |DFT| over the
+    plane at 21 wavelengths."""
+    from photonoxide_b200 import configs
+    from photonoxide_b200.fdtd import Simulation
+    s32, info = configs.strip_2d(Simulation, 32)
+    s64, _ = configs.strip_2d(Simulation, 64)
+    steps = info["steps"]
+    s32.run(args.warmup)
+    _, dt = _timed(lambda: s32.run(steps - args.warmup))
+    s64.run(steps)
+    cells = s32.grid.cells()
+    line = {"metric": "FDTD Gcell-updates/s (2D TE strip 400x200, 21-wavelength plane DFT)",
+            "value": (steps - args.warmup) * cells / dt / 1e9, "unit": UNIT, "n_gpus": 1,
+            "steps": steps - args.warmup, "warmup": args.warmup, "dtype": "f32",
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "2D TE Si strip 0.5 um in SiO2, 400x200 at 20 nm, CPML 12, "
+                                   "H_z line source, 4000 steps, DFT of the whole plane at 21 "
+                                   "wavelengths", "cells": cells, "l2": "L2-resident"},
+            "parity_vs_f64": {"probe_rel_l2": _rel_l2(s32.probe(info["probe"]), s64.probe(info["probe"])),
+                              "dft_abs_rel_l2": _rel_l2(np.abs(s32.transforms()),
+                                                        np.abs(s64.transforms())),
+                              "tolerance": 1e-4}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_mmi_parity(args):
+    """Configuration 2 at full size: 20000 steps of the MMI in f32 and in f64 (the engine's f64,
+    the oracle's bits): the arms' flux spectra (|dT| relative to the largest flux) and the probe's
+    time series (relative L2)."""
+    from photonoxide_b200 import configs
+    from photonoxide_b200.fdtd import Simulation
+    s32, info = configs.mmi_3d(Simulation, 32)
+    s64, _ = configs.mmi_3d(Simulation, 64)
+    steps = int(os.environ.get("PHOTONOXIDE_MMI_STEPS", info["steps"]))
+    _, t32 = _timed(lambda: s32.run(steps))
+    _, t64 = _timed(lambda: s64.run(steps))
+    f32 = np.array([s32.flux(n) for n in info["fluxes"]])
+    f64 = np.array([s64.flux(n) for n in info["fluxes"]])
+    scale = float(np.max(np.abs(f64)))
+    line = {"metric": "MMI f32 vs f64 over a full run", "steps": steps, "dtype": "f32",
+            "value": float(np.max(np.abs(f32 - f64)) / scale), "unit": "max |dT| / max T",
+            "higher_is_better": False, "data": "synthetic",
+            "probe_rel_l2": _rel_l2(s32.probe(info["probe"]), s64.probe(info["probe"])),
+            "seconds": {"f32": t32, "f64": t64}, "tolerance": 1e-4,
+            "config": {"workload": "3D MMI 600x200x100, CPML 10, 2 arm flux planes x 51 "
+                                   "wavelengths", "cells": info["cells"]}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_dispersive(args):
+    """Configuration 3: 256x256x128 with Drude and two-pole Lorentz boxes, the ADE fused into the
+    E update; kernel time by CUDA events, algorithmic bytes 60 B/cell + 8 B/psi value + 8 B per
+    dispersive value + 16 B per pole of it."""
+    import ctypes as C
+    import torch
+    from photonoxide_b200 import configs
+    from photonoxide_b200.engine import Engine
+    from photonoxide_b200.fdtd import Simulation, library
+    from photonoxide_b200.types import Boundaries
+    s, info = configs.dispersive_3d(Simulation, 7, 32)
+    steps = args.steps
+    s.run(args.warmup)
+    eng = Engine(s.engine())
+    stream = torch.cuda.ExternalStream(eng.stream())
+    clocks = Clocks(0)
+    torch.cuda.synchronize()
+    eng.profile(True)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    eng.run_async(steps, s.steps)
+    b.record(stream)
+    eng.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b)
+    kms, kn = eng.profile_read()
+    eng.profile(False)
+    counts = (C.c_int64 * 2)()
+    library().pxs_media_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    library().pxs_media_counts(s._h, counts)
+    psi = configs.psi_values(s.grid, Boundaries.with_cpml(10))
+    bytes_step = 60 * info["cells"] + 8 * psi + 8 * counts[0] + 16 * counts[1]
+    peak, kind = peaks()
+    achieved = bytes_step / (kms / max(kn, 1) / 1e3) / 1e9
+    line = {"metric": "FDTD Gcell-updates/s (3D dispersive 256x256x128)",
+            "value": steps * info["cells"] / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": 1,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps, "dtype": "f32",
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "256x256x128 at 10 nm, Drude (wp 1.37e16 rad/s, gamma 1e14/s) "
+                                   "and 2-pole Lorentz boxes, 12% fill, CPML 10",
+                       "cells": info["cells"], "dispersive_values": counts[0],
+                       "poles": counts[1], "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": kind,
+                         "bytes_per_launch": bytes_step,
+                         "kernel_ms_per_launch": kms / max(kn, 1)},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _te_instances(count, seed=0, precision=32):
+    from photonoxide_b200 import configs
+    rng = np.random.default_rng(seed + 1)
+    sims = []
+    for (nx, ny) in configs.te_design_sides(count, seed):
+        p = configs.te_design(nx, ny, precision=precision)
+        eps = configs.N_SIO2 ** 2 + rng.uniform(0, 1, (100, 100)) * (configs.N_SI ** 2 - configs.N_SIO2 ** 2)
+        sims.append(p.simulation(eps))
+    return sims
+
+
+def workload_batch(args):
+    """Configuration 4, forward: 64 uneven 2D TE instances (sides log-uniform 256-1024 cells) with
+    100x100 design regions, 6000 steps, batched (one persistent launch per step for all, CUDA-
+    graph chunks, tile shape by timing) against the same instances run one at a time."""
+    from photonoxide_b200.batch import Batch
+    steps = 6000
+    sims = _te_instances(64)
+    cells = sum(s.grid.cells() for s in sims)
+    B = Batch(sims)
+    B.run(416)  # the tile shape's trial chunks
+    _, tb = _timed(lambda: B.run(steps))
+    alone = _te_instances(64)
+    for s in alone:
+        s.run(3)
+    _, ta = _timed(lambda: [s.run(steps) for s in alone])
+    line = {"metric": "batched 2D TE Gcell-updates/s vs one at a time (64 instances)",
+            "value": steps * cells / tb / 1e9, "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "dtype": "f32", "higher_is_better": True, "data": "synthetic",
+            "one_at_a_time": steps * cells / ta / 1e9,
+            "speedup": ta / tb, "tile": list(B.tile),
+            "config": {"workload": "64 2D TE instances, sides log-uniform 256-1024 at 20 nm, "
+                                   "100x100 random design, CPML 12, flux monitor at 1550 nm",
+                       "cells": cells}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_adjoint(args):
+    """Configuration 4, gradient: one instance's flux at 1550 nm through the arm, d/d(density) of
+    its 100x100 design (Gaussian blur sigma 2 px, eps in [1.444^2, 3.48^2]) by the time-reversed
+    adjoint (6000 steps, checkpoints every 500), against central differences on 16 seeded pixels
+    (delta 1e-3) in f64; and the f32 gradient against the f64 one."""
+    import torch
+    from photonoxide_b200 import configs
+    from photonoxide_b200.adjoint import central_differences, transmission
+    nx, ny = configs.te_design_sides(64)[0]
+    e0, e1 = configs.N_SIO2 ** 2, configs.N_SI ** 2
+    rho = np.random.default_rng(11).uniform(0, 1, (100, 100))
+    out = {}
+    for prec in (32, 64):
+        p = configs.te_design(nx, ny, precision=prec)
+        r = torch.tensor(rho, requires_grad=True)
+        t, tf = _timed(lambda: transmission(r, p, e0, e1))
+        _, tbk = _timed(lambda: t[0].backward())
+        out[prec] = (p, r.grad.numpy().copy(), tf, tbk, float(t[0].detach()))
+    p64, g64 = out[64][0], out[64][1]
+
+    def f(x):
+        with torch.no_grad():
+            return float(transmission(torch.tensor(x), p64, e0, e1)[0])
+    pixels = np.random.default_rng(5).choice(rho.size, 16, replace=False)
+    fd = central_differences(f, rho, pixels, 1e-3)
+    ga = g64.reshape(-1)[pixels]
+    line = {"metric": "adjoint gradient vs central differences (max relative error, 16 pixels)",
+            "value": float(np.max(np.abs(ga - fd)) / np.max(np.abs(fd))), "unit": "relative",
+            "higher_is_better": False, "dtype": "f64", "data": "synthetic", "steps": 6000,
+            "rel_l2": _rel_l2(ga, fd), "tolerance": 1e-3,
+            "f32_vs_f64_gradient_rel_l2": _rel_l2(out[32][1], g64),
+            "seconds": {"f32_forward": out[32][2], "f32_backward": out[32][3],
+                        "f64_forward": out[64][2], "f64_backward": out[64][3]},
+            "flux": out[64][4],
+            "config": {"workload": f"2D TE {nx}x{ny} at 20 nm, 100x100 design, 6000 steps, "
+                                   "segments of 500", "cells": nx * ny}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_serving(args):
+    """Configuration 5, scaled to minutes: a seeded Poisson stream of jobs (20/s; 70% 2D, 30% 3D;
+    cells log-uniform 1e4-2e6; steps 200-2000; 1-4 Si boxes in SiO2; 1-51 DFT wavelengths) served
+    by the resident loop (150 GB budget, continuous admission) against the same jobs run one at a
+    time in arrival order: p50/p99 latency and aggregate Gcell-updates/s. Each job's host set-up
+    (permittivity averaging, tables) is made before the stream starts, for both arms: the
+    comparison is of the device's work."""
+    import torch
+    from photonoxide_b200.serving import Server, job_stream, make_job
+    count = int(os.environ.get("PHOTONOXIDE_SERVING_JOBS", "60"))
+    specs = job_stream(count, rate=20.0, seed=5, cells=(1e4, 2e6), steps=(200, 2000))
+    work = sum(int(np.prod(sp.n)) * sp.steps for sp in specs)
+    # one at a time, in arrival order: each job run and its results read back
+    sims = [make_job(sp) for sp in specs]
+    durations = []
+    for sp, s in zip(specs, sims):
+        def one():
+            s.run(sp.steps)
+            s.transforms()
+        _, d = _timed(one)
+        durations.append(d)
+    t, lat1 = 0.0, []
+    for sp, d in zip(specs, durations):
+        t = max(t, sp.arrival) + d
+        lat1.append(t - sp.arrival)
+    span1 = t - specs[0].arrival
+    # served: submitted at their arrival times
+    sims = [make_job(sp) for sp in specs]
+    torch.cuda.synchronize()
+    with Server(hbm_budget=150e9, max_active=64, chunk=500) as server:
+        start = time.perf_counter()
+        jobs = []
+        for sp, s in zip(specs, sims):
+            delay = sp.arrival - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            jobs.append(server.submit(s, sp.steps))
+        for j in jobs:
+            j.wait()
+        span = time.perf_counter() - start - specs[0].arrival
+        lat = [j.latency() for j in jobs]
+    line = {"metric": "served FDTD jobs: aggregate Gcell-updates/s and p99 latency",
+            "value": work / span / 1e9, "unit": UNIT, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "jobs": count,
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "one_at_a_time": {"value": work / span1 / 1e9,
+                              "latency_s": {"p50": float(np.percentile(lat1, 50)),
+                                            "p99": float(np.percentile(lat1, 99))}},
+            "speedup": span1 / span,
+            "config": {"workload": "Poisson stream, 20 jobs/s, 70% 2D / 30% 3D, cells "
+                                   "log-uniform 1e4-2e6 (scaled from 1e5-5e7), steps 200-2000 "
+                                   "(scaled from 2000-20000), 150 GB budget; host set-up before "
+                                   "the stream", "cell_updates": work}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+WORKLOADS = {"strip2d": workload_strip2d, "mmi_parity": workload_mmi_parity,
+             "dispersive": workload_dispersive, "batch": workload_batch,
+             "adjoint": workload_adjoint, "serving": workload_serving}
 
 
 def configs_eps(sim):
