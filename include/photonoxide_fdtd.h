@@ -33,6 +33,7 @@ extern "C" {
 #define FDTD_E_BUDGET (-3)  /* the problem needs more HBM than the context's budget */
 #define FDTD_E_STATE (-4)   /* a call out of order (e.g. a run before the fields are there) */
 #define FDTD_E_TIMEOUT (-5) /* a device-side wait gave up (persistent/served kernels) */
+#define FDTD_E_GROWING (-6) /* the fields grew again after the sources ended (Error::Growing) */
 
 typedef struct fdtd_ctx fdtd_ctx;
 

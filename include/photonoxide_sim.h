@@ -78,6 +78,15 @@ int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const doub
 int pxs_run(pxs_sim *s, int64_t steps);
 double pxs_dt(const pxs_sim *s);
 int64_t pxs_steps(const pxs_sim *s);
+/* Simulation::time (src/fdtd.rs:887-889): steps x dt */
+double pxs_time(const pxs_sim *s);
+/* Simulation::run_until (src/fdtd.rs:1161-1167) */
+int pxs_run_until(pxs_sim *s, double time);
+/* Simulation::run_until_decayed (src/fdtd/monitors.rs:742-838): *decayed 1 when the probes'
+ * |F|^2 stayed within `fraction` of its peak over a block of `interval`, 0 at `limit`;
+ * FDTD_E_GROWING (growing: time, checks, factor) when the fields grow again after the sources. */
+int pxs_run_until_decayed(pxs_sim *s, int32_t count, const int32_t *probes, double fraction,
+                          double interval, double limit, int32_t *decayed, double *growing);
 int pxs_get_field(pxs_sim *s, int32_t field, int32_t comp, double *out);
 int pxs_set_field(pxs_sim *s, int32_t field, int32_t comp, const double *in);
 /* probe n's values, one per step since it was added; returns the count (out may be NULL) */

@@ -63,6 +63,8 @@ struct MediaArgs {
   const int *gpoles;  // per group: its pole count
   const T *gpole;     // per group x maxpoles x 3: alpha, xi, gamma
   T two_dt;
+  const long long *place;  // per member: its value (component * N + r); members in value order
+  long long members;
 };
 
 template <typename T>
@@ -1249,8 +1251,9 @@ __device__ __forceinline__ void slab4x(const StepArgs<T> &A, const SlabEntry &s,
   if (write) st4(psi_out, nw);
 }
 
-// The CPML of one field at a lane's four places: each slab's psi read first, then the slabs in
-// the reference's order for each component (src/fdtd/kernel.rs:525-579: along x, y, z).
+// The CPML of one field at a lane's four places, slab by slab in the reference's order for each
+// component (src/fdtd/kernel.rs:525-579: along x, y, z): each slab's psi row read, updated and
+// written before the next, so that only one row is live at a time.
 template <typename T, int FIELD>
 __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int mxb, int sx,
                                       bool xmixed, const bool inx[4], bool zs, int sy, bool write,
@@ -1258,47 +1261,42 @@ __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int m
                                       bool xdiv_fallback_ok) {
   const int nx = A.n[0], ny = A.n[1];
   const long long plane = (long long)nx * ny;
-  const long long rowat = (long long)my * nx + mxb;
   const T *pin = FIELD == 1 ? A.psi_h_in : A.psi_e;
   T *pout = FIELD == 1 ? A.psi_h_out : A.psi_e;
-  // the slabs: c = 0 along y (+) and z (-); c = 1 along x (-) and z (+); c = 2 along x (+) and y (-)
-  SlabEntry sy0{}, sz0{}, sx1{}, sz1{}, sx2{}, sy2{};
-  Vec4<T> py0, pz0, px1, pz1, px2, py2;
-  long long ay0 = 0, az0 = 0, ax1 = 0, az1 = 0, ax2 = 0, ay2 = 0;
-  if (sy >= 0) {
-    sy0 = A.slab[FIELD][0][1][sy];
-    sy2 = A.slab[FIELD][2][1][sy];
-    if (sy0.count) { ay0 = sy0.psi + ((long long)k * sy0.count + (my - sy0.from)) * nx + mxb; py0 = ld4(pin + ay0); }
-    if (sy2.count) { ay2 = sy2.psi + ((long long)k * sy2.count + (my - sy2.from)) * nx + mxb; py2 = ld4(pin + ay2); }
-  }
-  if (zs) {
-    const int side = k < A.low[2] ? 0 : 1;
-    sz0 = A.slab[FIELD][0][2][side];
-    sz1 = A.slab[FIELD][1][2][side];
-    if (sz0.count) { az0 = sz0.psi + (long long)(k - sz0.from) * plane + rowat; pz0 = ld4(pin + az0); }
-    if (sz1.count) { az1 = sz1.psi + (long long)(k - sz1.from) * plane + rowat; pz1 = ld4(pin + az1); }
-  }
-  if (sx >= 0 && !xmixed) {
-    sx1 = A.slab[FIELD][1][0][sx];
-    sx2 = A.slab[FIELD][2][0][sx];
-    const long long rx = ((long long)k * ny + my);
-    if (sx1.count) { ax1 = sx1.psi + rx * sx1.pw + (mxb - sx1.pf); px1 = ld4(pin + ax1); }
-    if (sx2.count) { ax2 = sx2.psi + rx * sx2.pw + (mxb - sx2.pf); px2 = ld4(pin + ax2); }
-  }
   const T one = T(1), minus = T(-1);
   const T zero4[4] = {T(0), T(0), T(0), T(0)};
-  const T *cb0 = FIELD == 1 ? zero4 : cbv[0];
-  const T *cb1 = FIELD == 1 ? zero4 : cbv[1];
-  const T *cb2 = FIELD == 1 ? zero4 : cbv[2];
-  // component x: y then z
-  if (sy0.count) slab4_loaded<T, FIELD>(A, pout + ay0, py0, sy0, my - sy0.from, A.step[1], one, diff[0][1], v[0], cb0, write);
-  if (sz0.count) slab4_loaded<T, FIELD>(A, pout + az0, pz0, sz0, k - sz0.from, A.step[2], minus, diff[0][2], v[0], cb0, write);
-  // component y: x then z
-  if (sx1.count) slab4x<T, FIELD>(A, sx1, pout + ax1, px1, mxb, inx, minus, diff[1][0], v[1], cb1, write);
-  if (sz1.count) slab4_loaded<T, FIELD>(A, pout + az1, pz1, sz1, k - sz1.from, A.step[2], one, diff[1][2], v[1], cb1, write);
-  // component z: x then y
-  if (sx2.count) slab4x<T, FIELD>(A, sx2, pout + ax2, px2, mxb, inx, one, diff[2][0], v[2], cb2, write);
-  if (sy2.count) slab4_loaded<T, FIELD>(A, pout + ay2, py2, sy2, my - sy2.from, A.step[1], minus, diff[2][1], v[2], cb2, write);
+  const int zside = zs ? (k < A.low[2] ? 0 : 1) : 0;
+  const bool xs = sx >= 0 && !xmixed;
+  // along y at (k, my): rows of nx
+  auto y_slab = [&](int c, T sign, const T d[4], T w[4], const T *cb) {
+    const SlabEntry &s = A.slab[FIELD][c][1][sy];
+    if (!s.count) return;
+    const long long at = s.psi + ((long long)k * s.count + (my - s.from)) * nx + mxb;
+    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, my - s.from, A.step[1], sign, d, w, cb,
+                           write);
+  };
+  auto z_slab = [&](int c, T sign, const T d[4], T w[4], const T *cb) {
+    const SlabEntry &s = A.slab[FIELD][c][2][zside];
+    if (!s.count) return;
+    const long long at = s.psi + (long long)(k - s.from) * plane + (long long)my * nx + mxb;
+    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, k - s.from, A.step[2], sign, d, w, cb,
+                           write);
+  };
+  auto x_slab = [&](int c, T sign, const T d[4], T w[4], const T *cb) {
+    const SlabEntry &s = A.slab[FIELD][c][0][sx];
+    if (!s.count) return;
+    const long long at = s.psi + ((long long)k * ny + my) * s.pw + (mxb - s.pf);
+    slab4x<T, FIELD>(A, s, pout + at, ld4(pin + at), mxb, inx, sign, d, w, cb, write);
+  };
+  // component x: y (+) then z (-)
+  if (sy >= 0) y_slab(0, one, diff[0][1], v[0], FIELD == 1 ? zero4 : cbv[0]);
+  if (zs) z_slab(0, minus, diff[0][2], v[0], FIELD == 1 ? zero4 : cbv[0]);
+  // component y: x (-) then z (+)
+  if (xs) x_slab(1, minus, diff[1][0], v[1], FIELD == 1 ? zero4 : cbv[1]);
+  if (zs) z_slab(1, one, diff[1][2], v[1], FIELD == 1 ? zero4 : cbv[1]);
+  // component z: x (+) then y (-)
+  if (xs) x_slab(2, one, diff[2][0], v[2], FIELD == 1 ? zero4 : cbv[2]);
+  if (sy >= 0) y_slab(2, minus, diff[2][1], v[2], FIELD == 1 ? zero4 : cbv[2]);
   (void)xdiv_fallback_ok;
 }
 
@@ -2006,6 +2004,36 @@ void launch_staged(fdtd_ctx *c, const StepArgs<T> &A) {
   kernel<<<ctas, NT, smem, c->stream>>>(A, total, ctas);
 }
 
+// The dispersive media's ADE update (src/fdtd/media.rs:661-705) as a pass of its own over the
+// members, after the step kernel has written E (curl, slabs and currents): the same arithmetic
+// as the kernels' fused MEDIA branch, reading E^n from the step's input copy and the updated E
+// from its output, one member a thread in value order.
+template <typename T>
+__global__ void media_kernel(StepArgs<T> A) {
+  const MediaArgs<T> &M = A.media;
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= M.members) return;
+  const long long at = M.place[q];
+  const int g = M.group[q];
+  const int np = M.gpoles[g];
+  const T before = M.before[q];
+  T rest = M.gchi[g] * before;
+  const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+  T *cur = M.current + q * M.maxpoles;
+  T *prev = M.previous + q * M.maxpoles;
+  for (int p = 0; p < np; p++)
+    rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
+  const T next = A.e_out[at] + M.scale[q] * rest;
+  const T slope = (next - before) / M.two_dt;
+  for (int p = 0; p < np; p++) {
+    const T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
+    prev[p] = cur[p];
+    cur[p] = jn;
+  }
+  M.before[q] = A.e_in[at];
+  A.e_out[at] = next;
+}
+
 template <typename T>
 void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
   if (c->quad) {
@@ -2015,13 +2043,11 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
       cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       kernel<<<grid, quad::THREADS, smem, c->stream>>>(A);
     };
-    if (c->media) {
-      if (c->lossless) go(quad_kernel<T, false, true>);
-      else go(quad_kernel<T, true, true>);
-    } else {
-      if (c->lossless) go(quad_kernel<T, false, false>);
-      else go(quad_kernel<T, true, false>);
-    }
+    // media: the step without them, then their pass over the members
+    if (c->lossless) go(quad_kernel<T, false, false>);
+    else go(quad_kernel<T, true, false>);
+    if (c->media)
+      media_kernel<T><<<(unsigned)((A.media.members + 255) / 256), 256, 0, c->stream>>>(A);
     return;
   }
   if (c->row) {
@@ -2118,7 +2144,7 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
       } else {
         launch_step<T>(c, A);
       }
-      c->launches++;
+      c->launches += (c->quad && c->media) ? 2 : 1;
       c->parity = 1 - c->parity;
       long long gathered = c->nvalues + c->nprobes;
       if (gathered > 0) {
@@ -2666,25 +2692,36 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
   std::vector<int> member(3 * c->N, -1), group(members);
   std::vector<double> scale(members), gchi(ngroups), gpole((size_t)ngroups * maxp * 3, 0.0);
   std::vector<int> gpoles(ngroups);
-  long long m = 0;
+  // members numbered in value order, so a pass over them reads the fields in order
+  struct In { long long at; int g; double scale; };
+  std::vector<In> all;
+  all.reserve(members);
   for (int g = 0; g < ngroups; g++) {
     const fdtd_media_group &G = groups[g];
     gchi[g] = G.chi;
     gpoles[g] = G.npoles;
     for (int p = 0; p < G.npoles; p++)
       for (int q = 0; q < 3; q++) gpole[((size_t)g * maxp + p) * 3 + q] = G.poles[3 * p + q];
-    for (long long v = 0; v < G.count; v++, m++) {
+    for (long long v = 0; v < G.count; v++) {
       if (G.component[v] < 0 || G.component[v] > 2 || G.r[v] < 0 || G.r[v] >= c->N)
         return fail(c, FDTD_E_INVALID, "a medium's value is outside the grid");
-      long long at = G.component[v] * c->N + G.r[v];
-      if (member[at] >= 0) return fail(c, FDTD_E_INVALID, "a value is in two media");
-      member[at] = (int)m;
-      group[m] = g;
-      scale[m] = G.scale[v];
+      all.push_back(In{G.component[v] * c->N + G.r[v], g, G.scale[v]});
     }
+  }
+  std::sort(all.begin(), all.end(), [](const In &a, const In &b) { return a.at < b.at; });
+  std::vector<long long> place(members);
+  for (long long m = 0; m < members; m++) {
+    if (member[all[m].at] >= 0) return fail(c, FDTD_E_INVALID, "a value is in two media");
+    member[all[m].at] = (int)m;
+    group[m] = all[m].g;
+    scale[m] = all[m].scale;
+    place[m] = all[m].at;
   }
   size_t E = c->elem;
   void *d_member, *d_group, *d_scale, *d_before, *d_cur, *d_prev, *d_gchi, *d_gpoles, *d_gpole;
+  void *d_place;
+  if (int r = alloc(c, &d_place, members * 8)) return r;
+  CUDA_TRY(c, cudaMemcpy(d_place, place.data(), members * 8, cudaMemcpyHostToDevice));
   if (int r = alloc(c, &d_member, member.size() * 4)) return r;
   if (int r = alloc(c, &d_group, members * 4)) return r;
   if (int r = alloc(c, &d_scale, members * E)) return r;
@@ -2718,6 +2755,8 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
     M.gpoles = (const int *)d_gpoles;
     M.gpole = (const TT *)d_gpole;
     M.two_dt = (TT)(2.0 * c->dt);
+    M.place = (const long long *)d_place;
+    M.members = members;
   };
   if (c->precision == 64) fillm(c->md);
   else fillm(c->mf);

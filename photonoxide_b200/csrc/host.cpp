@@ -1233,6 +1233,113 @@ int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const doub
 }
 
 int pxs_run(pxs_sim *s, int64_t steps) { return s->run(steps); }
+
+double pxs_time(const pxs_sim *s) { return (double)s->steps * s->dt; }
+
+// Simulation::run_until (src/fdtd.rs:1161-1167): the steps that bring the time to `time`.
+int pxs_run_until(pxs_sim *s, double time) {
+  int64_t count = 0;
+  while ((double)(s->steps + count) * s->dt < time) count++;
+  return s->run(count);
+}
+
+namespace {
+
+// Growth (src/fdtd/monitors.rs:663-717): the fields rising at each of the last `needed` checks,
+// to 1e3 times their level before the first of them.
+struct Growth {
+  size_t needed;
+  double start = 0.0, last = 0.0;
+  size_t rises = 0;
+  explicit Growth(size_t n) : needed(n) {}
+  static Growth after(double pulse_end, double check) {
+    return Growth(std::max<size_t>((size_t)std::ceil(pulse_end / check) + 1, 4));
+  }
+  bool check(double level, double *factor) {
+    if (last > 0.0 && level > last) {
+      if (rises == 0) start = last;
+      rises++;
+    } else {
+      rises = 0;
+    }
+    last = level;
+    if (rises >= needed && level >= 1e3 * start) {
+      *factor = level / start;
+      return true;
+    }
+    return false;
+  }
+};
+
+// When the last source ends (monitors.rs:719-740): a pulse 6 widths after its peak; false for a
+// continuous wave, which never ends. No source: 0.
+bool sources_end(const pxs_sim *s, double *end) {
+  *end = 0.0;
+  for (const fdtd_waveform &w : s->waves) {
+    if (w.kind == 0) *end = std::max(*end, w.p[2] + 6.0 * w.p[1]);
+    else if (w.kind == 1) *end = std::max(*end, w.p[1] + 6.0 * w.p[0]);
+    else return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+// Simulation::run_until_decayed (src/fdtd/monitors.rs:742-838): blocks of `interval` until, over
+// a whole block, |F|^2 at every probe has stayed at or below `fraction` of its largest since the
+// probe was added (*decayed = 1), or the time reaches `limit` (*decayed = 0). After the sources
+// end it watches for late growth: FDTD_E_GROWING, with growing[0..2] = the time, the checks in a
+// row and the factor.
+int pxs_run_until_decayed(pxs_sim *s, int32_t count, const int32_t *probes, double fraction,
+                          double interval, double limit, int32_t *decayed, double *growing) {
+  if (count <= 0 || !probes || !(fraction > 0.0 && fraction < 1.0) ||
+      !(std::isfinite(interval) && interval > 0.0) || !std::isfinite(limit))
+    return s->fail(FDTD_E_INVALID,
+                   "running until the fields decay needs probes, a fraction in (0, 1), a positive "
+                   "interval and a finite limit, got %d probes, %g, %g and %g",
+                   count, fraction, interval, limit);
+  for (int q = 0; q < count; q++)
+    if (probes[q] < 0 || probes[q] >= (int32_t)s->probes.size())
+      return s->fail(FDTD_E_INVALID, "no probe %d", probes[q]);
+  *decayed = 0;
+  double end = 0.0;
+  const bool ends = sources_end(s, &end);
+  Growth growth = Growth::after(end, interval);
+  while (pxs_time(s) < limit) {
+    const size_t from = s->probes[probes[0]].values.size();
+    const double began = pxs_time(s);
+    if (int r = pxs_run_until(s, std::min(began + interval, limit))) return r;
+    bool all = true;
+    double level = 0.0;
+    for (int q = 0; q < count; q++) {
+      const std::vector<double> &v = s->probes[probes[q]].values;
+      double peak = 0.0, recent = 0.0;
+      for (size_t m = 0; m < v.size(); m++) {
+        peak = std::max(peak, v[m] * v[m]);
+        if (m >= std::min(from, v.size())) recent = std::max(recent, v[m] * v[m]);
+      }
+      if (!(peak > 0.0 && recent <= fraction * peak)) all = false;
+      level = std::max(level, recent);
+    }
+    if (all) {
+      *decayed = 1;
+      return 0;
+    }
+    double factor = 0.0;
+    if (ends && began >= end && growth.check(level, &factor)) {
+      if (growing) {
+        growing[0] = pxs_time(s);
+        growing[1] = (double)growth.needed;
+        growing[2] = factor;
+      }
+      return s->fail(FDTD_E_GROWING,
+                     "the fields grew again, and the run stopped at %.0f um/c: |field|^2 at the "
+                     "probes rose at %zu checks in a row, to %.1e times its level before",
+                     pxs_time(s), growth.needed, factor);
+    }
+  }
+  return 0;
+}
 double pxs_dt(const pxs_sim *s) { return s->dt; }
 int64_t pxs_steps(const pxs_sim *s) { return s->steps; }
 

@@ -22,7 +22,7 @@ from typing import Optional
 import numpy as np
 
 from .types import (Boxes, Current, Dipole, Dispersive, Field, FluxPlane, GpuError, Grid3d,
-                    InvalidValue, Source)
+                    Growing, InvalidValue, Source)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libphotonoxide_fdtd.so")
@@ -30,6 +30,7 @@ LIB_PATH = os.path.join(HERE, "libphotonoxide_fdtd.so")
 FDTD_E_INVALID = -1
 FDTD_E_GPU = -2
 FDTD_E_BUDGET = -3
+FDTD_E_GROWING = -6
 
 _lib = None
 
@@ -81,6 +82,10 @@ def library():
         x.pxs_tables.argtypes = [P, I32, DP]
         x.pxs_tables.restype = I64
         x.pxs_engine.argtypes = [P]
+        x.pxs_time.argtypes = [P]
+        x.pxs_time.restype = D
+        x.pxs_run_until.argtypes = [P, D]
+        x.pxs_run_until_decayed.argtypes = [P, I32, I32P, D, D, D, I32P, DP]
         x.pxs_engine.restype = P
         _lib = x
     return _lib
@@ -252,12 +257,31 @@ class Simulation:
     def step(self):
         self.run(1)
 
-    def run_until(self, time: float):
-        """``Simulation::run_until`` (``src/fdtd.rs:1161-1167``)."""
-        count = 0
-        while (self.steps + count) * self.dt < time:
-            count += 1
-        self.run(count)
+    def time(self) -> float:
+        """``Simulation::time``: steps x dt (um/c)."""
+        return float(library().pxs_time(self._h))
+
+    def run_until(self, time: float) -> "Simulation":
+        """``Simulation::run_until`` (src/fdtd.rs:1161-1167): the steps that bring the time to
+        ``time``."""
+        self._check(library().pxs_run_until(self._h, float(time)))
+        return self
+
+    def run_until_decayed(self, probes, fraction: float, interval: float, limit: float) -> bool:
+        """``Simulation::run_until_decayed`` (src/fdtd/monitors.rs:742-838): runs in blocks of
+        ``interval`` until |F|^2 at every probe stayed within ``fraction`` of its peak over a
+        block (True) or the time reaches ``limit`` (False). Raises :class:`Growing` when the
+        fields grow again after the sources end."""
+        ps = (C.c_int32 * len(probes))(*[int(p) for p in probes])
+        done = C.c_int32(0)
+        info = (C.c_double * 3)()
+        code = library().pxs_run_until_decayed(self._h, len(probes), ps, float(fraction),
+                                               float(interval), float(limit), C.byref(done), info)
+        if code == FDTD_E_GROWING:
+            raise Growing(library().pxs_last_error(self._h).decode(), info[0], int(info[1]),
+                          info[2])
+        self._check(code)
+        return bool(done.value)
 
     @property
     def dt(self) -> float:
@@ -266,9 +290,6 @@ class Simulation:
     @property
     def steps(self) -> int:
         return library().pxs_steps(self._h)
-
-    def time(self) -> float:
-        return self.steps * self.dt
 
     def _field(self, field, component) -> np.ndarray:
         out = np.empty(self.grid.cells())

@@ -53,6 +53,15 @@ class GpuError(RuntimeError):
     """A device failure or a problem the device can't hold: ``Error::Gpu`` (``src/error.rs:49``)."""
 
 
+class Growing(RuntimeError):
+    """The fields grew again after the sources ended and the run stopped: ``Error::Growing``
+    (``src/error.rs:59-69``)."""
+
+    def __init__(self, message, time_um=float("nan"), checks=0, factor=float("nan")):
+        super().__init__(message)
+        self.time_um, self.checks, self.factor = time_um, checks, factor
+
+
 @dataclass(frozen=True)
 class Grid3d:
     """nx x ny x nz cells of dx x dy x dz um, the lowest corner at (x0, y0, z0)."""
