@@ -187,6 +187,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--edges", default="cpml", choices=["cpml", "walls", "periodic"],
+                    help="the MMI grid's edges: cpml (the configuration) or, to compare the "
+                         "step's cost without CPMLs, walls or periodic sides")
     ap.add_argument("--workload", default="mmi", choices=sorted(["mmi"] + list(WORKLOADS)),
                     help="mmi: the 3D MMI step (this benchmark's line); the others measure the "
                          "remaining configurations, one JSON line each")
@@ -217,7 +220,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    sim, info = configs.mmi_3d(Simulation)
+    sim, info = configs.mmi_3d(Simulation, edges=args.edges)
     cells = info["cells"]
     sim.run(args.warmup)  # the first run uploads and configures; then warm
     eng = Engine(sim.engine())

@@ -120,6 +120,12 @@ int fdtd_upload_fields(fdtd_ctx *ctx, const double *e, const double *h, const do
  * first call on a device looks the array up (call it before any stream capture); calls that
  * overlap on the GPU share the array and race. */
 int fdtd_upload_fields_static(fdtd_ctx *ctx, const double *e, const double *h);
+
+/* Which axes' CPML differences are divided by the grid step through a reciprocal product with
+ * one correction (out[axis] = 1) rather than a division: in f32 the engine compares that form
+ * with division for every finite float at creation and uses it only where every result is the
+ * same bits. No counterpart in the reference (its WGSL divides). */
+int fdtd_fast_division(const fdtd_ctx *ctx, int32_t out[3]);
 /* Resident::download (resident.rs:402-413). Any pointer may be NULL to skip it. */
 int fdtd_download_fields(fdtd_ctx *ctx, double *e, double *h, double *const *psi);
 

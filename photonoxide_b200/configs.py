@@ -21,8 +21,8 @@ import math
 
 import numpy as np
 
-from .types import (INF, Axis, Boundaries, Boxes, Current, Dispersive, Field, FluxPlane, Grid3d,
-                    Pole, Source, Waveform)
+from .types import (INF, Axis, Boundaries, Boxes, Cpml, Current, Dispersive, Field, FluxPlane,
+                    Grid3d, Periodic, Pole, Source, Waveform)
 
 N_SI = 3.48
 N_SIO2 = 1.444
@@ -64,12 +64,16 @@ def mmi_geometry() -> Boxes:
     return geo
 
 
-def mmi_3d(cls, precision: int = 32, steps: int = 20000, frequencies: int = 51, **kw):
-    """Configuration 2: returns (simulation, info)."""
+def mmi_3d(cls, precision: int = 32, steps: int = 20000, frequencies: int = 51,
+           edges: str = "cpml", **kw):
+    """Configuration 2: returns (simulation, info). ``edges`` "walls" or "periodic" replaces the
+    CPMLs (for comparing the step's cost without them; not the configuration)."""
     h = 0.02
     g = Grid3d(600, 200, 100, h, h, h, -6.0, -2.0, -1.0)
+    b = {"cpml": Boundaries.with_cpml(10), "walls": Boundaries.walls(),
+         "periodic": Boundaries(Periodic(), Periodic(), Periodic(), Cpml())}[edges]
     # Courant 0.9: the reference job's default (src/job/fdtd.rs:523)
-    s = cls(g, mmi_geometry(), Boundaries.with_cpml(10), 0.9, precision=precision, **kw)
+    s = cls(g, mmi_geometry(), b, 0.9, precision=precision, **kw)
     # a Gaussian-profile E_y current across the input guide, 0.5 um in from the CPML
     i = 10 + 25
     values = []

@@ -45,6 +45,9 @@ struct TeInst {
   int nx, ny, px, py;  // sizes, periodic flags
   long long N;
   T dt, sx, sy;        // the step's dt and the grid steps along x and y, as the kernel rounds them
+  T inv_sx, inv_sy;    // 1/step rounded, and whether div_by_step's product form is checked
+  double rd_x, rd_y;   // 1/step in double
+  int fast_x, fast_y;
   double dt64;
   T *e[2], *h[2], *psi_h[2];
   T *psi_e;
@@ -81,9 +84,11 @@ __device__ __forceinline__ bool in_slab(const SlabEntry &s, int m) {
 // psi <- b psi + a (d/h), then H -= dt (sign psi) or E += cb (sign psi) (slab4 in engine.cu)
 template <typename T>
 __device__ __forceinline__ T slab_h(const TeInst<T> &I, const SlabEntry &s, int m, long long at,
-                                    const T *pin, T *pout, bool own, T diff, T h, T sign, T v) {
+                                    const T *pin, T *pout, bool own, T diff, int axis, T sign,
+                                    T v) {
   const T b = I.coefs[s.coef + (m - s.from)], a = I.coefs[s.coef + s.count + (m - s.from)];
-  T d = diff / h;
+  T d = axis == 0 ? div_by_step(diff, I.sx, I.inv_sx, I.rd_x, I.fast_x)
+                  : div_by_step(diff, I.sy, I.inv_sy, I.rd_y, I.fast_y);
   T nw = b * pin[at] + a * d;
   if (own) pout[at] = nw;
   T u = sign * nw;
@@ -91,9 +96,10 @@ __device__ __forceinline__ T slab_h(const TeInst<T> &I, const SlabEntry &s, int 
 }
 template <typename T>
 __device__ __forceinline__ T slab_e(const TeInst<T> &I, const SlabEntry &s, int m, long long at,
-                                    T *psi, T diff, T h, T sign, T cbv, T v) {
+                                    T *psi, T diff, int axis, T sign, T cbv, T v) {
   const T b = I.coefs[s.coef + (m - s.from)], a = I.coefs[s.coef + s.count + (m - s.from)];
-  T d = diff / h;
+  T d = axis == 0 ? div_by_step(diff, I.sx, I.inv_sx, I.rd_x, I.fast_x)
+                  : div_by_step(diff, I.sy, I.inv_sy, I.rd_y, I.fast_y);
   T nw = b * psi[at] + a * d;
   psi[at] = nw;
   T u = sign * nw;
@@ -142,14 +148,14 @@ __global__ void __launch_bounds__(THREADS) te_step_kernel(
           const SlabEntry &s = I.hx[side];
           if (in_slab(s, mx))
             hz = slab_h(I, s, mx, s.psi + (long long)my * s.pw + (mx - s.pf), pin, pout, own, dxEy,
-                        I.sx, T(1), hz);
+                        0, T(1), hz);
         }
         if (!I.py) {
           const int side = my < ny / 2 ? 0 : 1;
           const SlabEntry &s = I.hy[side];
           if (in_slab(s, my))
             hz = slab_h(I, s, my, s.psi + (long long)(my - s.from) * nx + mx, pin, pout, own, dyEx,
-                        I.sy, T(-1), hz);
+                        1, T(-1), hz);
         }
       }
       sh[q] = hz;
@@ -202,14 +208,14 @@ __global__ void __launch_bounds__(THREADS) te_step_kernel(
           const int side = y < ny / 2 ? 0 : 1;
           const SlabEntry &s = I.ey[side];
           if (in_slab(s, y))
-            nex = slab_e(I, s, y, s.psi + (long long)(y - s.from) * nx + x, I.psi_e, dyHz, I.sy,
+            nex = slab_e(I, s, y, s.psi + (long long)(y - s.from) * nx + x, I.psi_e, dyHz, 1,
                          T(1), cbx, nex);
         }
         if (!I.px) {
           const int side = x < nx / 2 ? 0 : 1;
           const SlabEntry &s = I.ex[side];
           if (in_slab(s, x))
-            ney = slab_e(I, s, x, s.psi + (long long)y * s.pw + (x - s.pf), I.psi_e, dxHz, I.sx,
+            ney = slab_e(I, s, x, s.psi + (long long)y * s.pw + (x - s.pf), I.psi_e, dxHz, 0,
                          T(-1), cby, ney);
         }
         eout[r] = nex;
@@ -722,6 +728,12 @@ int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vect
     I.dt64 = v.dt;
     I.sx = (T)v.step[0];
     I.sy = (T)v.step[1];
+    I.inv_sx = (T)v.inv_step[0];
+    I.inv_sy = (T)v.inv_step[1];
+    I.fast_x = v.fast_div[0];
+    I.rd_x = 1.0 / (double)I.sx;
+    I.rd_y = 1.0 / (double)I.sy;
+    I.fast_y = v.fast_div[1];
     for (int p = 0; p < 2; p++) {
       I.e[p] = (T *)v.e[p];
       I.h[p] = (T *)v.h[p];

@@ -94,4 +94,43 @@ struct SeriesDev {
   int slot0;         // its phases' slot for frequency 0
 };
 
+// x / h with h a grid step, the quotient IEEE division gives. In f32, where `fast` (set only
+// after the engine has compared it with division for every finite float x, see
+// verify_division_kernel), by Markstein's correction of the reciprocal product (P. Markstein,
+// IBM J. Res. Dev. 34(1), 1990): q0 = x r with r = 1/h rounded, the remainder e = x - q0 h exact
+// by a fused multiply-add, q = q0 + e r rounded once. The remainder is exact only while it does
+// not underflow, so |x| below 2^-90 is first scaled by 2^64 and the quotient scaled back (both
+// exact while the quotient is a normal number); zero gives x r (its sign kept); a subnormal
+// quotient is x times 1/h in double, rounded to float; a quotient that overflows takes the
+// division. In f64 always the division.
+#ifdef __CUDA_ARCH__
+// Out of line, so that the rare inputs' division is a call the common path branches over, not a
+// sequence issued (predicated off) at every use.
+static __device__ __noinline__ float div_rare(float x, float h) { return x / h; }
+#define PXF_DIV_RARE(x, h) div_rare(x, h)
+#else
+#define PXF_DIV_RARE(x, h) ((x) / (h))
+#endif
+__host__ __device__ __forceinline__ float div_by_step(float x, float h, float r, double rd,
+                                                      int fast) {
+  if (fast) {
+    const float ax = fabsf(x);
+    const bool tiny = ax < 0x1p-90f;
+    const float sx = x * (tiny ? 0x1p64f : 1.0f);
+    const float q0 = sx * r;
+    const float e = fmaf(-q0, h, sx);
+    const float q = fmaf(e, r, q0) * (tiny ? 0x1p-64f : 1.0f);
+    const float aq = fabsf(q);
+    if (aq >= 0x1p-126f && aq <= 3.40282347e38f) return q;  // a normal quotient
+    if (x == 0.0f) return x * r;
+    // a subnormal quotient: the product with 1/h in double, rounded once to float, carries
+    // 53 bits for the at most 23 the result keeps
+    if (aq < 0x1p-126f) return (float)((double)x * rd);
+  }
+  return PXF_DIV_RARE(x, h);
+}
+__host__ __device__ __forceinline__ double div_by_step(double x, double h, double, double, int) {
+  return x / h;
+}
+
 }  // namespace pxf

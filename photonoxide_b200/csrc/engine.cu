@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -75,6 +76,9 @@ struct StepArgs {
   int low[3], high[3];
   T dt;
   T step[3];
+  T inv_step[3];    // 1/step rounded, for div_by_step
+  double inv_step64[3];  // 1/step in double, for div_by_step's subnormal quotients
+  int fast_div[3];  // div_by_step's product form checked for this step
   const T *fe;  // kappa/h at the nodes: x | y | z
   const T *fh;  // at the halves
   const T *e_in;
@@ -127,7 +131,7 @@ __device__ inline T slab_update(const StepArgs<T> &A, const SlabEntry *s, int c,
   else if (w == 1) { lj = q; dy = s->count; }
   else lk = q;
   long long p = s->psi + ((long long)lk * dy + lj) * dx + li;
-  T d = diff / A.step[w];
+  T d = div_by_step(diff, A.step[w], A.inv_step[w], A.inv_step64[w], A.fast_div[w]);
   T b = A.coefs[s->coef + q], a = A.coefs[s->coef + s->count + q];
   T old = FIELD == 1 ? A.psi_h_in[p] : A.psi_e[p];
   T psi = b * old + a * d;
@@ -731,7 +735,7 @@ __device__ __forceinline__ T slab_apply(const StepArgs<T> &A, const SlabEntry s,
   else if (w == 1) { lj = q; dy = s.count; }
   else lk = q;
   long long p = s.psi + ((long long)lk * dy + lj) * dx + li;
-  T d = diff / A.step[w];
+  T d = div_by_step(diff, A.step[w], A.inv_step[w], A.inv_step64[w], A.fast_div[w]);
   T b = A.coefs[s.coef + q], a = A.coefs[s.coef + s.count + q];
   T old = FIELD == 1 ? A.psi_h_in[p] : A.psi_e[p];
   T psi = b * old + a * d;
@@ -1196,13 +1200,13 @@ __device__ __forceinline__ void st4(T *p, const Vec4<T> &r) {
 // then H -= dt (sign psi) or E += cb (sign psi), each value as slab_update does
 template <typename T, int FIELD>
 __device__ __forceinline__ void slab4(const StepArgs<T> &A, T *psi_out, const T *psi_in, T b, T a,
-                                      T hstep, T sign, const T diff[4], T v[4], const T cbv[4],
+                                      int axis, T sign, const T diff[4], T v[4], const T cbv[4],
                                       bool write) {
   Vec4<T> old = ld4(psi_in);
   Vec4<T> nw;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    T d = diff[j] / hstep;
+    T d = div_by_step(diff[j], A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
     nw.v[j] = b * old.v[j] + a * d;
     T u = sign * nw.v[j];
     if (FIELD == 1) v[j] = v[j] - A.dt * u;
@@ -1214,13 +1218,13 @@ __device__ __forceinline__ void slab4(const StepArgs<T> &A, T *psi_out, const T 
 // slab4 with the psi row already read
 template <typename T, int FIELD>
 __device__ __forceinline__ void slab4_loaded(const StepArgs<T> &A, T *psi_out, const Vec4<T> &old,
-                                             const SlabEntry &s, int q, T hstep, T sign,
+                                             const SlabEntry &s, int q, int axis, T sign,
                                              const T diff[4], T v[4], const T cbv[4], bool write) {
   const T b = A.coefs[s.coef + q], a = A.coefs[s.coef + s.count + q];
   Vec4<T> nw;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    T d = diff[j] / hstep;
+    T d = div_by_step(diff[j], A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
     nw.v[j] = b * old.v[j] + a * d;
     T u = sign * nw.v[j];
     if (FIELD == 1) v[j] = v[j] - A.dt * u;
@@ -1241,7 +1245,7 @@ __device__ __forceinline__ void slab4x(const StepArgs<T> &A, const SlabEntry &s,
     nw.v[j] = old.v[j];
     if (in[j]) {
       const int q = x + j - s.from;
-      T d = diff[j] / A.step[0];
+      T d = div_by_step(diff[j], A.step[0], A.inv_step[0], A.inv_step64[0], A.fast_div[0]);
       nw.v[j] = A.coefs[s.coef + q] * old.v[j] + A.coefs[s.coef + s.count + q] * d;
       T u = sign * nw.v[j];
       if (FIELD == 1) v[j] = v[j] - A.dt * u;
@@ -1272,14 +1276,14 @@ __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int m
     const SlabEntry &s = A.slab[FIELD][c][1][sy];
     if (!s.count) return;
     const long long at = s.psi + ((long long)k * s.count + (my - s.from)) * nx + mxb;
-    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, my - s.from, A.step[1], sign, d, w, cb,
+    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, my - s.from, 1, sign, d, w, cb,
                            write);
   };
   auto z_slab = [&](int c, T sign, const T d[4], T w[4], const T *cb) {
     const SlabEntry &s = A.slab[FIELD][c][2][zside];
     if (!s.count) return;
     const long long at = s.psi + (long long)(k - s.from) * plane + (long long)my * nx + mxb;
-    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, k - s.from, A.step[2], sign, d, w, cb,
+    slab4_loaded<T, FIELD>(A, pout + at, ld4(pin + at), s, k - s.from, 2, sign, d, w, cb,
                            write);
   };
   auto x_slab = [&](int c, T sign, const T d[4], T w[4], const T *cb) {
@@ -1779,6 +1783,20 @@ __global__ void widen_kernel(const T *in, double *out, long long n) {
 
 using namespace pxf;
 
+// For every finite float x: whether div_by_step's product form (reciprocal r) gives x / h's
+// bits. Sets *bad if any x differs. 2^32 values, a few milliseconds on a B200.
+__global__ void verify_division_kernel(float h, float r, double rd, int *bad) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  int found = 0;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+       i < (1ULL << 32); i += stride) {
+    const float x = __uint_as_float((unsigned)i);
+    if (!isfinite(x)) continue;
+    if (__float_as_uint(div_by_step(x, h, r, rd, 1)) != __float_as_uint(x / h)) found = 1;
+  }
+  if (found) atomicOr(bad, 1);
+}
+
 // ------------------------------------------------------------------------------------------
 // The context: the device state of one simulation.
 
@@ -1797,6 +1815,8 @@ struct fdtd_ctx {
   int periodic[3], low[3], high[3];
   double dt;
   double step[3];
+  double inv_step[3] = {0, 0, 0};  // 1/step as the kernels round it
+  int fast_div[3] = {0, 0, 0};     // div_by_step's product form checked for this step
   size_t budget = 0, used = 0;
   cudaStream_t stream = nullptr;
   std::vector<void *> allocations;
@@ -1960,6 +1980,9 @@ StepArgs<T> step_args(fdtd_ctx *c) {
     A.low[a] = c->low[a];
     A.high[a] = c->high[a];
     A.step[a] = (T)c->step[a];
+    A.inv_step[a] = (T)c->inv_step[a];
+    A.inv_step64[a] = 1.0 / (double)(T)c->step[a];
+    A.fast_div[a] = c->fast_div[a];
   }
   A.N = c->N;
   A.dt = (T)c->dt;
@@ -2084,6 +2107,40 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
     if (c->lossless) go(step_kernel<T, false, false>);
     else go(step_kernel<T, true, false>);
   }
+}
+
+// Whether div_by_step's product form equals division for grid step h on this device, checked
+// once per (device, step) and remembered.
+int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
+  static std::mutex mu;
+  static std::map<std::pair<int, unsigned>, int> seen;
+  int dev = 0;
+  CUDA_TRY(c, cudaGetDevice(&dev));
+  unsigned hb, rb;
+  memcpy(&hb, &h, 4);
+  memcpy(&rb, &r, 4);
+  const auto key = std::make_pair(dev, hb ^ (rb * 2654435761u));
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = seen.find(key);
+    if (it != seen.end()) {
+      *ok = it->second;
+      return 0;
+    }
+  }
+  int *bad = nullptr;
+  CUDA_TRY(c, cudaMalloc(&bad, 4));
+  CUDA_TRY(c, cudaMemsetAsync(bad, 0, 4, c->stream));
+  verify_division_kernel<<<c->sms * 8, 256, 0, c->stream>>>(h, r, 1.0 / (double)h, bad);
+  int found = 1;
+  cudaError_t err = cudaMemcpyAsync(&found, bad, 4, cudaMemcpyDeviceToHost, c->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
+  cudaFree(bad);
+  if (err != cudaSuccess) return fail(c, FDTD_E_GPU, "checking the division: %s", cudaGetErrorString(err));
+  *ok = found ? 0 : 1;
+  std::lock_guard<std::mutex> lock(mu);
+  seen[key] = *ok;
+  return 0;
 }
 
 // Empty source tables: every bucket empty.
@@ -2284,6 +2341,17 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   }
   c->sms = sms;
+  // the slabs' d/h: in f32 by the product form where it is checked to give division's bits
+  for (int a = 0; a < 3; a++) {
+    if (c->precision == 64) {
+      c->inv_step[a] = 1.0 / c->step[a];
+      c->fast_div[a] = 0;
+      continue;
+    }
+    const float h = (float)c->step[a], r = (float)(1.0 / (double)h);
+    c->inv_step[a] = r;
+    if (int q = division_checked(c, h, r, &c->fast_div[a])) return q;
+  }
   {
     const char *force = getenv("PHOTONOXIDE_FDTD_KERNEL");
     // the quad kernel takes four places along x at once: nx a multiple of 4, and no group of
@@ -2954,6 +3022,10 @@ int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
   }
   v->psi_e = c->psi_e;
   v->psi_h_len = c->psi_h_len;
+  for (int a = 0; a < 3; a++) {
+    v->inv_step[a] = c->inv_step[a];
+    v->fast_div[a] = c->fast_div[a];
+  }
   v->psi_e_len = c->psi_e_len;
   v->ca = c->lossless ? nullptr : c->ca;
   v->cb = c->cb;
@@ -3003,6 +3075,12 @@ void fdtd_instance_advance(fdtd_ctx *c, long long steps) {
   if (!c) return;
   if (steps & 1) c->parity = 1 - c->parity;
   if (c->nprobes > 0) c->recorded += steps;
+}
+
+int fdtd_fast_division(const fdtd_ctx *c, int32_t out[3]) {
+  if (!c || !out) return FDTD_E_INVALID;
+  for (int a = 0; a < 3; a++) out[a] = c->fast_div[a];
+  return 0;
 }
 
 int fdtd_instance_fail(fdtd_ctx *c, int code, const char *what) {

@@ -14,6 +14,8 @@ struct InstanceView {
   long long N;
   int periodic[3], low[3], high[3];
   double dt, step[3];
+  double inv_step[3];  // 1/step as the kernels round it
+  int fast_div[3];     // div_by_step's product form checked for the step
   int parity;  // which copy of E, H and H's psi is current
   void *e[2], *h[2], *psi_h[2], *psi_e;
   long long psi_h_len, psi_e_len;  // values in each copy of H's psi and in E's

@@ -171,3 +171,24 @@ def test_dispersive_media_bit_for_bit(precision, n):
     for x, y in zip(fields(p), fields(o)):
         assert np.array_equal(x, y), relative(x, y)
     assert np.array_equal(p.probe(pp), o.probe(op))
+
+
+@pytest.mark.parametrize("h", [0.02, 0.04, 0.05])
+def test_fast_division_is_checked_and_on(h):
+    """The slabs' d/h in f32 goes through the product form only where the engine found it equal to
+    division for every finite float; for the steps these tests use (and the MMI's 20 nm) it is,
+    so the bit-for-bit tests above run through it. In f64 the division stays."""
+    import ctypes
+    from photonoxide_b200.fdtd import library
+    flags = {}
+    for precision in (32, 64):
+        s = Simulation(Grid3d.centred((24, 20, 12), h), Boxes(1.0), Boundaries.with_cpml(3), 0.9,
+                       precision=precision)
+        s.run(1)
+        out = (ctypes.c_int32 * 3)()
+        lib = library()
+        lib.fdtd_fast_division.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+        assert lib.fdtd_fast_division(s.engine(), out) == 0
+        flags[precision] = list(out)
+    assert flags[32] == [1, 1, 1]
+    assert flags[64] == [0, 0, 0]
