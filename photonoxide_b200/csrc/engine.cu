@@ -1166,7 +1166,10 @@ struct Smem {
   static constexpr int E_SLOT = 3 * ER * EW;             // E of one plane
   static constexpr int HB_SLOT = 3 * WARPS * ROW + 3 * RW * ROW;  // H(k) rows, cb(k) rows
   static constexpr int X = 2 * WARPS * ROW;              // H_x, H_z exchange
-  static constexpr size_t BYTES = sizeof(T) * (3 * (size_t)E_SLOT + 2 * (size_t)HB_SLOT + X);
+  // the x CPML's b and a at the row's places: [field][component y, z][b, a][ROW] (0 outside)
+  static constexpr int XC = 2 * 2 * 2 * ROW;
+  static constexpr size_t BYTES =
+      sizeof(T) * (3 * (size_t)E_SLOT + 2 * (size_t)HB_SLOT + X + XC);
 };
 }  // namespace quad
 
@@ -1236,17 +1239,18 @@ __device__ __forceinline__ void slab4_loaded(const StepArgs<T> &A, T *psi_out, c
 // The same along x, where each place has its own coefficients and only the places `in` the slab
 // change (the psi row is padded to whole vectors; the other places keep their psi).
 template <typename T, int FIELD>
-__device__ __forceinline__ void slab4x(const StepArgs<T> &A, const SlabEntry &s, T *psi_out,
-                                       const Vec4<T> &old, int x, const bool in[4], T sign,
+__device__ __forceinline__ void slab4x(const StepArgs<T> &A, const T *xb4, const T *xa4,
+                                       T *psi_out, const Vec4<T> &old, const bool in[4], T sign,
                                        const T diff[4], T v[4], const T cbv[4], bool write) {
+  // xb4, xa4: b and a at the lane's four places (the CTA's table)
+  const Vec4<T> bb = ld4(xb4), aa = ld4(xa4);
   Vec4<T> nw;
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     nw.v[j] = old.v[j];
     if (in[j]) {
-      const int q = x + j - s.from;
       T d = div_by_step(diff[j], A.step[0], A.inv_step[0], A.inv_step64[0], A.fast_div[0]);
-      nw.v[j] = A.coefs[s.coef + q] * old.v[j] + A.coefs[s.coef + s.count + q] * d;
+      nw.v[j] = bb.v[j] * old.v[j] + aa.v[j] * d;
       T u = sign * nw.v[j];
       if (FIELD == 1) v[j] = v[j] - A.dt * u;
       else v[j] = v[j] + cbv[j] * u;
@@ -1262,7 +1266,8 @@ template <typename T, int FIELD>
 __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int mxb, int sx,
                                       bool xmixed, const bool inx[4], bool zs, int sy, bool write,
                                       T v[3][4], const T diff[3][3][4], const T cbv[3][4],
-                                      bool xdiv_fallback_ok) {
+                                      const T *xc) {
+  // xc: the CTA's x coefficient table at this lane's first place (quad::Smem::XC)
   const int nx = A.n[0], ny = A.n[1];
   const long long plane = (long long)nx * ny;
   const T *pin = FIELD == 1 ? A.psi_h_in : A.psi_e;
@@ -1290,7 +1295,8 @@ __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int m
     const SlabEntry &s = A.slab[FIELD][c][0][sx];
     if (!s.count) return;
     const long long at = s.psi + ((long long)k * ny + my) * s.pw + (mxb - s.pf);
-    slab4x<T, FIELD>(A, s, pout + at, ld4(pin + at), mxb, inx, sign, d, w, cb, write);
+    const T *t = xc + ((FIELD * 2 + (c - 1)) * 2) * quad::ROW;
+    slab4x<T, FIELD>(A, t, t + quad::ROW, pout + at, ld4(pin + at), inx, sign, d, w, cb, write);
   };
   // component x: y (+) then z (-)
   if (sy >= 0) y_slab(0, one, diff[0][1], v[0], FIELD == 1 ? zero4 : cbv[0]);
@@ -1301,7 +1307,6 @@ __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int m
   // component z: x (+) then y (-)
   if (xs) x_slab(2, one, diff[2][0], v[2], FIELD == 1 ? zero4 : cbv[2]);
   if (sy >= 0) y_slab(2, minus, diff[2][1], v[2], FIELD == 1 ? zero4 : cbv[2]);
-  (void)xdiv_fallback_ok;
 }
 
 template <typename T, bool LOSSY, bool MEDIA>
@@ -1321,6 +1326,22 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const int kbeg = blockIdx.y * A.zchunk, kend = min(kbeg + A.zchunk, nz);
   if (kbeg >= nz) return;
   const long long plane = (long long)nx * ny;
+  T *sXC = sX + S::X;                                // quad::Smem::XC
+  // the x CPML's coefficients at the row's places, once (read after the prologue's barrier)
+  for (int q = threadIdx.x; q < S::XC; q += THREADS) {
+    const int at = q % ROW, ba = (q / ROW) % 2, c = 1 + (q / (2 * ROW)) % 2, f = q / (4 * ROW);
+    const int gx = x0 - VEC + at;
+    T val = T(0);
+    if (!A.periodic[0] && gx >= 0 && gx < nx) {
+      const int side = gx < A.low[0] ? 0 : (gx >= nx - A.high[0] ? 1 : -1);
+      if (side >= 0) {
+        const SlabEntry &e = A.slab[f][c][0][side];
+        if (e.count && gx >= e.from && gx < e.from + e.count)
+          val = A.coefs[e.coef + ba * e.count + (gx - e.from)];
+      }
+    }
+    sXC[q] = val;
+  }
 
   // -- this lane's four places along x, this warp's row
   const int xb = x0 - VEC + VEC * lane;  // the first of the four
@@ -1489,7 +1510,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
           {{dxEz[0], dxEz[1], dxEz[2], dxEz[3]}, {T(0), T(0), T(0), T(0)}, {dzEx[0], dzEx[1], dzEx[2], dzEx[3]}},
           {{dxEy[0], dxEy[1], dxEy[2], dxEy[3]}, {dyEx[0], dyEx[1], dyEx[2], dyEx[3]}, {T(0), T(0), T(0), T(0)}}};
       const T nocb[3][4] = {};
-      cpml4<T, 1>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, ow, hn, diff, nocb, true);
+      cpml4<T, 1>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, ow, hn, diff, nocb, sXC + VEC * lane);
     }
     // beyond a wall H is zero (E's back differences read zero there)
 #pragma unroll
@@ -1620,7 +1641,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
                              {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
                              {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
-        cpml4<T, 0>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, true, en, diff, cbs, true);
+        cpml4<T, 0>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, true, en, diff, cbs, sXC + VEC * lane);
       }
       // the electric currents (src/fdtd.rs:1375-1387)
       const int bucket = tile * nz + k;
