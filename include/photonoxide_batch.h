@@ -29,7 +29,9 @@ int fdtd_batch_create(int32_t count, fdtd_ctx *const *ctxs, fdtd_batch **out);
 const char *fdtd_batch_last_error(const fdtd_batch *batch);
 /* `steps` steps of every grid; grid i's first step has index first_steps[i] (its step count so
  * far, as fdtd_run's first_step), all 0 when first_steps is NULL. The first run of a batch whose
- * tile shape is not set times each shape on chunks of these steps and keeps the fastest. */
+ * tile shape is not set times each shape on chunks of these steps and keeps the fastest. Returns
+ * once the steps are queued: each context's stream waits for them, so its later calls (reads,
+ * runs, fdtd_synchronize) come after. */
 int fdtd_batch_run(fdtd_batch *batch, int64_t steps, const int64_t *first_steps);
 /* The tile shape in use (0 x 0 before the first run chooses one). */
 int fdtd_batch_tile(const fdtd_batch *batch, int32_t *width, int32_t *height);

@@ -148,7 +148,8 @@ int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps);
 int pxs_server_poll(pxs_server *sv, int64_t id, double *times);
 int pxs_server_wait(pxs_server *sv, int64_t id);
 int pxs_server_cancel(pxs_server *sv, int64_t id);
-/* out[0] cell-updates taken, out[1] chunks stepped, out[2] device bytes admitted now */
+/* out[0] cell-updates taken, out[1] rounds stepped, out[2] device bytes admitted now, out[3..5]
+ * the loop's seconds queuing work, setting up and reading back jobs, waiting for the device */
 int pxs_server_stats(pxs_server *sv, double *out);
 /* stops the loop (between chunks) and frees the server; jobs still running are left released or
  * not as the loop left them */

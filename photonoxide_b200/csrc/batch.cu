@@ -16,7 +16,8 @@
 // E_y on its cells, adds the electric sources, and writes both to the other copy of the fields.
 // Steps run in chunks of G: the source waveforms and transform phases of a chunk are evaluated
 // first (f64, the reference's exp and sincos), the chunk's step launches follow, each with a
-// launch that adds the new values into the f64 transform sums in time order. A chunk is captured
+// launch that copies the monitored values into a ring; at the chunk's end one launch adds the
+// ring into the f64 transform sums in time order. A chunk is captured
 // once as a CUDA graph and replayed. The tile shape is chosen by timing: the first run tries each
 // shape on a chunk of real steps (every shape gives the same bits) and keeps the fastest.
 #include <cuda_runtime.h>
@@ -75,6 +76,7 @@ struct TeInst {
 struct RecItem {
   int inst, kind;
   long long index;
+  long long col;  // a transform value's column in the ring
 };
 
 __device__ __forceinline__ bool in_slab(const SlabEntry &s, int m) {
@@ -289,11 +291,11 @@ __global__ void te_phase_kernel(const TeInst<T> *insts, const int2 *items, int n
   phase[o + 1] = sn * I.dt64;
 }
 
-// After step m of the chunk: each transform value's sums += F e^{i w t} dt (f64, time order),
-// each probe's value into its record row.
+// After step m of the chunk: each transform value into row m of the ring, each probe's value
+// into its record row.
 template <typename T>
 __global__ void te_record_kernel(const TeInst<T> *insts, const RecItem *items, long long nitems,
-                                 const double *phase, int nslots_total, int m) {
+                                 T *ring, long long nring, int m) {
   long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nitems) return;
   const RecItem it = items[q];
@@ -305,17 +307,36 @@ __global__ void te_record_kernel(const TeInst<T> *insts, const RecItem *items, l
     I.rows[(long long)m * I.nprobes + it.index] = (double)f[w & ((1LL << 62) - 1)];
     return;
   }
-  const long long v = it.index;
-  const long long w = I.where[v];
+  const long long w = I.where[it.index];
   const T *f = (w >> 62) ? I.h[now] : I.e[now];
-  const double x = (double)f[w & ((1LL << 62) - 1)];
+  ring[(long long)m * nring + it.col] = f[w & ((1LL << 62) - 1)];
+}
+
+// After a chunk's `count` steps: each transform value's sums += sum over the ring's rows of
+// F e^{i w t} dt, f64, in time order (dft_kernel in engine.cu).
+template <typename T>
+__global__ void te_contract_kernel(const TeInst<T> *insts, const RecItem *items, long long nitems,
+                                   const T *ring, long long nring, const double *phase,
+                                   int nslots_total, int count) {
+  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nitems) return;
+  const RecItem it = items[q];
+  if (it.kind != 0) return;
+  const TeInst<T> &I = insts[it.inst];
+  const long long v = it.index;
   const SeriesDev s = I.series[I.value_series[v]];
   const long long o = v - s.value0;
-  const double *ph = phase + 2 * ((long long)m * nslots_total + I.slot0 + s.slot0);
   for (int k = 0; k < s.nf; k++) {
     double *acc = I.sums + 2 * (s.sum0 + (long long)k * s.volume + o);
-    acc[0] = acc[0] + x * ph[2 * k];
-    acc[1] = acc[1] + x * ph[2 * k + 1];
+    double re = acc[0], im = acc[1];
+    const double *ph = phase + 2 * ((long long)I.slot0 + s.slot0 + k);
+    for (int m = 0; m < count; m++) {
+      const double x = (double)ring[(long long)m * nring + it.col];
+      re = re + x * ph[2 * (long long)m * nslots_total];
+      im = im + x * ph[2 * (long long)m * nslots_total + 1];
+    }
+    acc[0] = re;
+    acc[1] = im;
   }
 }
 
@@ -627,6 +648,8 @@ struct fdtd_batch {
   double *d_waves_h = nullptr, *d_waves_e = nullptr, *d_phase = nullptr;
   RecItem *d_rec = nullptr;
   long long nrec = 0;
+  void *d_ring = nullptr;  // G rows of the transform values
+  long long nring = 0;
   int blocks = 0;
   int *d_bad = nullptr;  // the TE check's flag
   // for the adjoint's recomputation: transforms and probes off, and after each step the E curl
@@ -660,7 +683,7 @@ int bfail(fdtd_batch *b, int code, const char *fmt, ...) {
 void free_tables(fdtd_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
-  for (void *p : b->allocs) cudaFree(p);
+  for (void *p : b->allocs) cudaFreeAsync(p, b->stream);  // after the batch's work so far
   b->allocs.clear();
 }
 
@@ -683,16 +706,18 @@ int upload_vec(fdtd_batch *b, V **dst, const std::vector<V> &v) {
   *dst = nullptr;
   size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(V);
   void *p = nullptr;
-  BTRY(b, cudaMalloc(&p, bytes));
+  BTRY(b, cudaMallocAsync(&p, bytes, b->stream));  // stream-ordered: no device-wide sync
   b->allocs.push_back(p);
-  if (!v.empty()) BTRY(b, cudaMemcpy(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  if (!v.empty())
+    BTRY(b, cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, b->stream));
   *dst = static_cast<V *>(p);
   return 0;
 }
 int zeros(fdtd_batch *b, double **dst, size_t n) {
   void *p = nullptr;
-  BTRY(b, cudaMalloc(&p, std::max<size_t>(n, 1) * 8));
+  BTRY(b, cudaMallocAsync(&p, std::max<size_t>(n, 1) * 8, b->stream));
   b->allocs.push_back(p);
+  BTRY(b, cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * 8, b->stream));
   *dst = static_cast<double *>(p);
   return 0;
 }
@@ -714,6 +739,7 @@ int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vect
   std::vector<int> point;
   std::vector<int2> wave_items, slot_items;
   std::vector<RecItem> rec;
+  long long nring = 0;
   int bucket = 0, slots = 0;
   for (size_t i = 0; i < views.size(); i++) {
     const InstanceView &v = views[i];
@@ -855,8 +881,8 @@ int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vect
     I.nslots = v.nvalues > 0 ? v.nslots : 0;
     for (int s = 0; s < I.nslots; s++) slot_items.push_back(make_int2((int)i, s));
     slots += I.nslots;
-    for (long long q = 0; q < v.nvalues; q++) rec.push_back(RecItem{(int)i, 0, q});
-    for (int p = 0; p < v.nprobes; p++) rec.push_back(RecItem{(int)i, 1, p});
+    for (long long q = 0; q < v.nvalues; q++) rec.push_back(RecItem{(int)i, 0, q, nring++});
+    for (int p = 0; p < v.nprobes; p++) rec.push_back(RecItem{(int)i, 1, p, -1});
   }
   b->ntiles = (int)tile_inst.size();
   b->nwaves_total = (int)waves.size();
@@ -879,6 +905,13 @@ int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vect
   if (int r = zeros(b, &b->d_waves_h, (size_t)G * std::max(b->nwaves_total, 1) * 2)) return r;
   if (int r = zeros(b, &b->d_waves_e, (size_t)G * std::max(b->nwaves_total, 1) * 2)) return r;
   if (int r = zeros(b, &b->d_phase, (size_t)G * std::max(b->nslots_total, 1) * 2)) return r;
+  b->nring = nring;
+  {
+    double *ring = nullptr;
+    if (int r = zeros(b, &ring, ((size_t)G * std::max<long long>(nring, 1) * sizeof(T) + 7) / 8))
+      return r;
+    b->d_ring = ring;
+  }
   b->shape = sh;
   return 0;
 }
@@ -940,7 +973,7 @@ void enqueue(fdtd_batch *b, int count) {
     b->launches++;
     if (b->nrec > 0 && b->record) {
       te_record_kernel<T><<<(unsigned)((b->nrec + 255) / 256), 256, 0, b->stream>>>(
-          insts, b->d_rec, b->nrec, b->d_phase, b->nslots_total, m);
+          insts, b->d_rec, b->nrec, (T *)b->d_ring, b->nring, m);
       b->launches++;
     }
     if (b->ndesign > 0) {
@@ -948,6 +981,12 @@ void enqueue(fdtd_batch *b, int count) {
           insts, b->d_design, b->ndesign, (T *)b->d_K, b->k_first, m);
       b->launches++;
     }
+  }
+  if (b->nring > 0 && b->record) {
+    te_contract_kernel<T><<<(unsigned)((b->nrec + 127) / 128), 128, 0, b->stream>>>(
+        insts, b->d_rec, b->nrec, (const T *)b->d_ring, b->nring, b->d_phase, b->nslots_total,
+        count);
+    b->launches++;
   }
   te_advance_kernel<T><<<(n + 127) / 128, 128, 0, b->stream>>>(insts, n, count);
   b->launches++;
@@ -1063,7 +1102,8 @@ int run_impl(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
     BTRY(b, cudaStreamWaitEvent(views[i].stream, b->done, 0));
     fdtd_instance_advance(b->ctxs[i], steps);
   }
-  BTRY(b, cudaStreamSynchronize(b->stream));
+  // no wait here: each context's stream waits for the batch's work (the event), so its later
+  // calls see the steps; the batch's next run orders after them on the batch's stream
   return 0;
 }
 
@@ -1136,6 +1176,7 @@ void fdtd_batch_destroy(fdtd_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   free_tables(b);
+  if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->done) cudaEventDestroy(b->done);
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->t1) cudaEventDestroy(b->t1);

@@ -1926,10 +1926,13 @@ int alloc(fdtd_ctx *c, void **p, size_t bytes) {
   if (c->budget && c->used + bytes > c->budget)
     return fail(c, FDTD_E_BUDGET, "%zu MB more would exceed the HBM budget of %zu MB",
                 bytes >> 20, c->budget >> 20);
-  cudaError_t e = cudaMalloc(p, bytes);
+  // stream-ordered, so that engines made and freed while others run (a serving loop) don't
+  // synchronize the device; the stream's work so far is waited for before the memory is used
+  cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return fail(c, FDTD_E_GPU, "cudaMalloc of %zu MB: %s", bytes >> 20, cudaGetErrorString(e));
+    return fail(c, FDTD_E_GPU, "cudaMallocAsync of %zu MB: %s", bytes >> 20, cudaGetErrorString(e));
   }
   c->used += bytes;
   c->allocations.push_back(*p);
@@ -1939,7 +1942,16 @@ void release(fdtd_ctx *c, void *p) {
   if (!p) return;
   auto it = std::find(c->allocations.begin(), c->allocations.end(), p);
   if (it != c->allocations.end()) c->allocations.erase(it);
-  cudaFree(p);
+  cudaFreeAsync(p, c->stream);
+}
+
+// A copy between host and device ordered on the engine's stream and finished before returning:
+// the engine's memory is stream-ordered, so no copy may run on another stream (a legacy-stream
+// copy still in flight could land in memory the stream has since freed).
+cudaError_t copy(fdtd_ctx *c, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
 }
 
 template <typename T>
@@ -2150,13 +2162,13 @@ int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
     }
   }
   int *bad = nullptr;
-  CUDA_TRY(c, cudaMalloc(&bad, 4));
+  CUDA_TRY(c, cudaMallocAsync(&bad, 4, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(bad, 0, 4, c->stream));
   verify_division_kernel<<<c->sms * 8, 256, 0, c->stream>>>(h, r, 1.0 / (double)h, bad);
   int found = 1;
   cudaError_t err = cudaMemcpyAsync(&found, bad, 4, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(bad, c->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(c->stream);
-  cudaFree(bad);
   if (err != cudaSuccess) return fail(c, FDTD_E_GPU, "checking the division: %s", cudaGetErrorString(err));
   *ok = found ? 0 : 1;
   std::lock_guard<std::mutex> lock(mu);
@@ -2173,8 +2185,8 @@ int empty_sources(fdtd_ctx *c) {
   c->hbucket = c->ebucket = nullptr;
   if (int r = alloc(c, (void **)&c->hbucket, nb * 4)) return r;
   if (int r = alloc(c, (void **)&c->ebucket, nb * 4)) return r;
-  CUDA_TRY(c, cudaMemcpy(c->hbucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->ebucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->hbucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->ebucket, zero.data(), nb * 4, cudaMemcpyHostToDevice));
   return 0;
 }
 
@@ -2421,8 +2433,11 @@ void fdtd_destroy(fdtd_ctx *c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (cudaEvent_t ev : c->events) cudaEventDestroy(ev);
-  for (void *p : c->allocations) cudaFree(p);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream) {
+    for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
   delete c;
 }
 
@@ -2620,14 +2635,14 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   if (int r = alloc(c, (void **)&c->hgroups, groups[1].size() * sizeof(Group))) return r;
   if (int r = alloc(c, (void **)&c->egroups, groups[0].size() * sizeof(Group))) return r;
   if (int r = alloc(c, (void **)&c->entries, ordered_entries.size() * sizeof(Entry))) return r;
-  CUDA_TRY(c, cudaMemcpy(c->hbucket, buckets[1].data(), nb * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->ebucket, buckets[0].data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->hbucket, buckets[1].data(), nb * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->ebucket, buckets[0].data(), nb * 4, cudaMemcpyHostToDevice));
   if (!groups[1].empty())
-    CUDA_TRY(c, cudaMemcpy(c->hgroups, groups[1].data(), groups[1].size() * sizeof(Group), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->hgroups, groups[1].data(), groups[1].size() * sizeof(Group), cudaMemcpyHostToDevice));
   if (!groups[0].empty())
-    CUDA_TRY(c, cudaMemcpy(c->egroups, groups[0].data(), groups[0].size() * sizeof(Group), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->egroups, groups[0].data(), groups[0].size() * sizeof(Group), cudaMemcpyHostToDevice));
   if (!ordered_entries.empty())
-    CUDA_TRY(c, cudaMemcpy(c->entries, ordered_entries.data(), ordered_entries.size() * sizeof(Entry), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->entries, ordered_entries.data(), ordered_entries.size() * sizeof(Entry), cudaMemcpyHostToDevice));
   c->nwaves = nwaves;
   if (nwaves > 0) {
     std::vector<Wave> w(nwaves);
@@ -2642,8 +2657,8 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
     if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * nwaves * 16)) return r;
     if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * nwaves * 16)) return r;
     c->wave_batch = K;
-    CUDA_TRY(c, cudaMemcpy(c->d_waves, w.data(), nwaves * sizeof(Wave), cudaMemcpyHostToDevice));
-    CUDA_TRY(c, cudaMemcpy(c->d_point, point.data(), nwaves * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->d_waves, w.data(), nwaves * sizeof(Wave), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->d_point, point.data(), nwaves * sizeof(int), cudaMemcpyHostToDevice));
   }
   return 0;
 }
@@ -2666,7 +2681,7 @@ int fdtd_set_probes(fdtd_ctx *c, int32_t n, const int32_t *field, const int32_t 
   c->nprobes = n;
   if (n > 0) {
     if (int rr = alloc(c, (void **)&c->d_probes, n * 8)) return rr;
-    CUDA_TRY(c, cudaMemcpy(c->d_probes, w.data(), n * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, copy(c, c->d_probes, w.data(), n * 8, cudaMemcpyHostToDevice));
   }
   return 0;
 }
@@ -2750,12 +2765,12 @@ int fdtd_set_dft(fdtd_ctx *c, int32_t nseries, const fdtd_series *series, int32_
   if (int r = alloc(c, (void **)&c->sums, sums * 16)) return r;
   if (int r = alloc(c, &c->ring, K * values * c->elem)) return r;
   if (int r = alloc(c, (void **)&c->phase, K * omega.size() * 16)) return r;
-  CUDA_TRY(c, cudaMemcpy(c->d_where, where.data(), values * 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->d_value_series, value_series.data(), values * 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->d_series, sd.data(), nseries * sizeof(SeriesDev), cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->d_omega, omega.data(), omega.size() * 8, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(c->d_slot_field, slot_field.data(), slot_field.size() * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemset(c->sums, 0, sums * 16));
+  CUDA_TRY(c, copy(c, c->d_where, where.data(), values * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->d_value_series, value_series.data(), values * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->d_series, sd.data(), nseries * sizeof(SeriesDev), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->d_omega, omega.data(), omega.size() * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, c->d_slot_field, slot_field.data(), slot_field.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemsetAsync(c->sums, 0, sums * 16, c->stream));
   // the source waves' batch must match the ring's
   if (c->nwaves > 0 && c->wave_batch < K) {
     release(c, c->waves_h);
@@ -2810,7 +2825,7 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
   void *d_member, *d_group, *d_scale, *d_before, *d_cur, *d_prev, *d_gchi, *d_gpoles, *d_gpole;
   void *d_place;
   if (int r = alloc(c, &d_place, members * 8)) return r;
-  CUDA_TRY(c, cudaMemcpy(d_place, place.data(), members * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, d_place, place.data(), members * 8, cudaMemcpyHostToDevice));
   if (int r = alloc(c, &d_member, member.size() * 4)) return r;
   if (int r = alloc(c, &d_group, members * 4)) return r;
   if (int r = alloc(c, &d_scale, members * E)) return r;
@@ -2820,15 +2835,15 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
   if (int r = alloc(c, &d_gchi, ngroups * E)) return r;
   if (int r = alloc(c, &d_gpoles, ngroups * 4)) return r;
   if (int r = alloc(c, &d_gpole, gpole.size() * E)) return r;
-  CUDA_TRY(c, cudaMemcpy(d_member, member.data(), member.size() * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(d_group, group.data(), members * 4, cudaMemcpyHostToDevice));
-  CUDA_TRY(c, cudaMemcpy(d_gpoles, gpoles.data(), ngroups * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, d_member, member.data(), member.size() * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, d_group, group.data(), members * 4, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, copy(c, d_gpoles, gpoles.data(), ngroups * 4, cudaMemcpyHostToDevice));
   if (int r = upload(c, d_scale, scale.data(), members)) return r;
   if (int r = upload(c, d_gchi, gchi.data(), ngroups)) return r;
   if (int r = upload(c, d_gpole, gpole.data(), (long long)gpole.size())) return r;
-  CUDA_TRY(c, cudaMemset(d_before, 0, members * E));
-  CUDA_TRY(c, cudaMemset(d_cur, 0, members * maxp * E));
-  CUDA_TRY(c, cudaMemset(d_prev, 0, members * maxp * E));
+  CUDA_TRY(c, cudaMemsetAsync(d_before, 0, members * E, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(d_cur, 0, members * maxp * E, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(d_prev, 0, members * maxp * E, c->stream));
   auto fillm = [&](auto &M) {
     using T = typename std::remove_pointer<decltype(M.scale)>::type;
     using TT = typename std::remove_const<T>::type;
@@ -2880,7 +2895,7 @@ int fdtd_read_probes(fdtd_ctx *c, double *out, int64_t capacity, int64_t *steps)
   long long n = c->recorded * c->nprobes;
   if (capacity < n) return fail(c, FDTD_E_INVALID, "%lld values need room for %lld", n, (long long)capacity);
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  CUDA_TRY(c, cudaMemcpy(out, c->record, n * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy(c, out, c->record, n * 8, cudaMemcpyDeviceToHost));
   c->recorded = 0;
   return 0;
 }
@@ -2892,9 +2907,9 @@ int fdtd_read_dft(fdtd_ctx *c, double *sums, int64_t count) {
   if (c->nsums == 0) return 0;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   std::vector<double> tmp(2 * c->nsums);
-  CUDA_TRY(c, cudaMemcpy(tmp.data(), c->sums, c->nsums * 16, cudaMemcpyDeviceToHost));
+  CUDA_TRY(c, copy(c, tmp.data(), c->sums, c->nsums * 16, cudaMemcpyDeviceToHost));
   for (long long q = 0; q < 2 * c->nsums; q++) sums[q] += tmp[q];
-  CUDA_TRY(c, cudaMemset(c->sums, 0, c->nsums * 16));
+  CUDA_TRY(c, cudaMemsetAsync(c->sums, 0, c->nsums * 16, c->stream));
   return 0;
 }
 

@@ -1650,6 +1650,8 @@ struct pxs_server {
   std::vector<ServerJob *> batch_jobs;
   double cell_updates = 0.0;
   int64_t chunks = 0;
+  double launch_s = 0.0, host_s = 0.0, wait_s = 0.0;  // the loop's time: queuing, set-up and
+                                                       // read-back, waiting for the device
 
   void finish_job(ServerJob *j, int state, const std::string &why) {
     // called with mu held
@@ -1661,11 +1663,12 @@ struct pxs_server {
 
   void run_loop() {
     cudaSetDevice(device);
+    std::vector<ServerJob *> finished;  // stepped to their end; read back in the next round
     for (;;) {
-      std::vector<ServerJob *> admitted;
+      std::vector<ServerJob *> admitted, te, other;
       {
         std::unique_lock<std::mutex> lock(mu);
-        cv.wait(lock, [&] { return stop || !queue.empty() || !active.empty(); });
+        cv.wait(lock, [&] { return stop || !queue.empty() || !active.empty() || !finished.empty(); });
         if (stop) break;
         // admission in arrival order, while slots and memory last
         while (!queue.empty() && (int)active.size() < max_active) {
@@ -1686,64 +1689,43 @@ struct pxs_server {
           active.push_back(j);
           admitted.push_back(j);
         }
-      }
-      for (ServerJob *j : admitted) {
-        if (int r = j->sim->prepare()) {
-          std::lock_guard<std::mutex> lock(mu);
-          finish_job(j, JOB_FAILED, j->sim->error.empty() ? "setup failed" : j->sim->error);
-          (void)r;
-        } else {
-          j->prepared = true;
-        }
-      }
-      std::vector<ServerJob *> te, other;
-      {
-        std::lock_guard<std::mutex> lock(mu);
+        // this round's work: the admitted jobs already set up
         std::vector<ServerJob *> keep;
         for (ServerJob *j : active) {
-          if (j->state == JOB_RUNNING && j->prepared) {
+          if (j->state == JOB_RUNNING) {
             keep.push_back(j);
-            (j->te ? te : other).push_back(j);
+            if (j->prepared) (j->te ? te : other).push_back(j);
           } else if (j->state == JOB_CANCELLED && j->prepared) {
             j->sim->release();
           }
         }
         active = keep;
-        cv.notify_all();
       }
-      if (te.empty() && other.empty()) continue;
-      // the others: each its own chunk on its own stream
+      const double t0 = now_s();
+      // launch: the others each on its own stream, the 2D TE jobs as one batch (remade when its
+      // members change), as many steps as the batch's job nearest its end still needs
       std::vector<int64_t> took(other.size(), 0);
+      std::vector<std::pair<ServerJob *, std::string>> failed;
       for (size_t q = 0; q < other.size(); q++) {
         ServerJob *j = other[q];
         took[q] = std::min(chunk, j->steps - j->done);
         if (fdtd_run_async(j->sim->ctx, took[q], j->sim->steps)) {
-          std::string why = fdtd_last_error(j->sim->ctx);
-          std::lock_guard<std::mutex> lock(mu);
-          j->sim->release();
-          finish_job(j, JOB_FAILED, why);
+          failed.push_back({j, fdtd_last_error(j->sim->ctx)});
           took[q] = -1;
         }
       }
-      // the 2D TE jobs: one batch (remade when its members change), as many steps as the job
-      // nearest its end still needs (none overshoots)
       int64_t te_took = 0;
       if (!te.empty()) {
         if (te != batch_jobs) {
           fdtd_batch_destroy(batch);
           batch = nullptr;
+          batch_jobs.clear();
           std::vector<fdtd_ctx *> ctxs;
           for (ServerJob *j : te) ctxs.push_back(j->sim->ctx);
           if (fdtd_batch_create((int32_t)ctxs.size(), ctxs.data(), &batch)) {
-            std::string why = fdtd_batch_last_error(batch);
+            for (ServerJob *j : te) failed.push_back({j, fdtd_batch_last_error(batch)});
             fdtd_batch_destroy(batch);
             batch = nullptr;
-            batch_jobs.clear();
-            std::lock_guard<std::mutex> lock(mu);
-            for (ServerJob *j : te) {
-              j->sim->release();
-              finish_job(j, JOB_FAILED, why);
-            }
             te.clear();
           } else {
             fdtd_batch_set_tile(batch, 32, 16);
@@ -1758,42 +1740,70 @@ struct pxs_server {
             first.push_back(j->sim->steps);
           }
           if (fdtd_batch_run(batch, te_took, first.data())) {
-            std::string why = fdtd_batch_last_error(batch);
-            std::lock_guard<std::mutex> lock(mu);
-            for (ServerJob *j : te) {
-              j->sim->release();
-              finish_job(j, JOB_FAILED, why);
-            }
+            for (ServerJob *j : te) failed.push_back({j, fdtd_batch_last_error(batch)});
             te.clear();
             te_took = 0;
           }
         }
       }
+      const double t1 = now_s();
+      // while the device steps: the last round's finished jobs read back (their own streams),
+      // the newly admitted ones set up
+      for (ServerJob *j : finished) {
+        const int r = j->sim->release();
+        std::lock_guard<std::mutex> lock(mu);
+        finish_job(j, r ? JOB_FAILED : JOB_DONE, r ? j->sim->error : std::string());
+        cv.notify_all();
+      }
+      finished.clear();
+      for (ServerJob *j : admitted) {
+        if (j->sim->prepare()) {
+          std::lock_guard<std::mutex> lock(mu);
+          j->sim->release();
+          finish_job(j, JOB_FAILED, j->sim->error.empty() ? "setup failed" : j->sim->error);
+        } else {
+          j->prepared = true;
+        }
+      }
+      const double t2 = now_s();
+      // the round's steps done
       for (size_t q = 0; q < other.size(); q++)
         if (took[q] > 0) fdtd_synchronize(other[q]->sim->ctx);
-      // bookkeeping; finished jobs read back and their memory freed
+      for (ServerJob *j : te) fdtd_synchronize(j->sim->ctx);
+      const double t3 = now_s();
       std::lock_guard<std::mutex> lock(mu);
-      chunks++;
+      launch_s += t1 - t0;
+      host_s += t2 - t1;
+      wait_s += t3 - t2;
+      if (!other.empty() || !te.empty()) chunks++;
+      for (auto &f : failed) {
+        if (f.first->state != JOB_RUNNING) continue;
+        f.first->sim->release();
+        finish_job(f.first, JOB_FAILED, f.second);
+      }
       auto advance = [&](ServerJob *j, int64_t n) {
         if (j->state != JOB_RUNNING) return;
         j->sim->finish(n);
         j->done += n;
         cell_updates += (double)n * (double)j->sim->N();
-        if (j->done >= j->steps) {
-          int r = j->sim->release();
-          finish_job(j, r ? JOB_FAILED : JOB_DONE, r ? j->sim->error : std::string());
-        }
+        if (j->done >= j->steps) finished.push_back(j);
       };
       for (size_t q = 0; q < other.size(); q++)
         if (took[q] > 0) advance(other[q], took[q]);
       for (ServerJob *j : te) advance(j, te_took);
       std::vector<ServerJob *> keep;
       for (ServerJob *j : active) {
-        if (j->state == JOB_RUNNING) keep.push_back(j);
+        const bool done = std::find(finished.begin(), finished.end(), j) != finished.end();
+        if (j->state == JOB_RUNNING && !done) keep.push_back(j);
         else if (j->state == JOB_CANCELLED && j->prepared) j->sim->release();
       }
       active = keep;
       cv.notify_all();
+    }
+    for (ServerJob *j : finished) {
+      j->sim->release();
+      std::lock_guard<std::mutex> lock(mu);
+      finish_job(j, JOB_DONE, std::string());
     }
     fdtd_batch_destroy(batch);
     batch = nullptr;
@@ -1897,13 +1907,17 @@ int pxs_server_cancel(pxs_server *sv, int64_t id) {
   return 0;
 }
 
-// Totals so far: cell-updates taken, chunks stepped, device bytes admitted now.
+// Totals so far: cell-updates taken, rounds stepped, device bytes admitted now, and the loop's
+// seconds queuing work, setting up and reading back jobs (while the device steps), waiting.
 int pxs_server_stats(pxs_server *sv, double *out) {
   if (!sv || !out) return FDTD_E_INVALID;
   std::lock_guard<std::mutex> lock(sv->mu);
   out[0] = sv->cell_updates;
   out[1] = (double)sv->chunks;
   out[2] = (double)sv->used;
+  out[3] = sv->launch_s;
+  out[4] = sv->host_s;
+  out[5] = sv->wait_s;
   return 0;
 }
 

@@ -97,9 +97,10 @@ class Server:
         return job
 
     def stats(self) -> dict:
-        out = (C.c_double * 3)()
+        out = (C.c_double * 6)()
         _lib().pxs_server_stats(self._h, out)
-        return {"cell_updates": out[0], "chunks": int(out[1]), "bytes_admitted": out[2]}
+        return {"cell_updates": out[0], "chunks": int(out[1]), "bytes_admitted": out[2],
+                "launch_s": out[3], "host_s": out[4], "wait_s": out[5]}
 
     def close(self):
         h = getattr(self, "_h", None)
