@@ -142,8 +142,10 @@ void pxs_adjoint_destroy(pxs_adjoint *a);
 typedef struct pxs_server pxs_server;
 int pxs_server_create(size_t hbm_budget, int32_t max_active, int64_t chunk, pxs_server **out);
 const char *pxs_server_last_error(const pxs_server *sv);
-/* returns the job's id (> 0) or a negative status */
-int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps);
+/* returns the job's id (> 0) or a negative status. keep_fields 0: when the job ends only its
+ * transforms, fluxes and probes come back (the fields are dropped with the device memory;
+ * reading them or running the simulation again then refuses with FDTD_E_STATE). */
+int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps, int32_t keep_fields);
 /* the job's state; times (may be NULL): submitted, started, finished (steady clock, seconds) */
 int pxs_server_poll(pxs_server *sv, int64_t id, double *times);
 int pxs_server_wait(pxs_server *sv, int64_t id);

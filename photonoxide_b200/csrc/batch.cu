@@ -659,6 +659,15 @@ struct fdtd_batch {
   long long ndesign = 0;
   void *d_K = nullptr;
   long long k_first = 0;
+  // the tables and graph stay good for the next run while every member is as the last run left
+  // it: the same generation (no engine call since), step index and current copy
+  bool reusable = false;
+  bool cap_record = true;
+  long long per_chunk = 0;  // the graph's kernels
+  std::vector<unsigned long long> gens;
+  std::vector<int64_t> next_first;
+  std::vector<int> next_parity;
+  std::vector<cudaEvent_t> member_ev;
 };
 
 namespace {
@@ -992,8 +1001,86 @@ void enqueue(fdtd_batch *b, int count) {
   b->launches++;
 }
 
+// The run's steps from `done` on with the current tables: whole chunks by the captured graph
+// (captured now if there is none), the rest launched; then the members' streams wait for them.
+template <typename T>
+int finish_run(fdtd_batch *b, int64_t steps, int64_t done, const std::vector<InstanceView> &views) {
+  const int n = (int)b->ctxs.size();
+  const int64_t full = (steps - done) / G;
+  if (full > 0) {
+    if (!b->graph) {
+      // one chunk captured as a graph, replayed
+      cudaGraph_t g = nullptr;
+      const long long before = b->launches;
+      BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue<T>(b, G);
+      cudaError_t err = cudaStreamEndCapture(b->stream, &g);
+      if (err != cudaSuccess)
+        return bfail(b, FDTD_E_GPU, "cudaStreamEndCapture: %s", cudaGetErrorString(err));
+      b->per_chunk = b->launches - before;
+      b->launches = before;
+      err = cudaGraphInstantiate(&b->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (err != cudaSuccess)
+        return bfail(b, FDTD_E_GPU, "cudaGraphInstantiate: %s", cudaGetErrorString(err));
+    }
+    for (int64_t c = 0; c < full; c++) {
+      BTRY(b, cudaGraphLaunch(b->graph, b->stream));
+      b->launches += b->per_chunk;
+    }
+    done += full * G;
+  }
+  if (done < steps) enqueue<T>(b, (int)(steps - done));
+  BTRY(b, cudaGetLastError());
+  BTRY(b, cudaEventRecord(b->done, b->stream));
+  for (int i = 0; i < n; i++) {
+    BTRY(b, cudaStreamWaitEvent(views[i].stream, b->done, 0));
+    fdtd_instance_advance(b->ctxs[i], steps);
+  }
+  // no wait here: each context's stream waits for the batch's work (the event), so its later
+  // calls see the steps; the batch's next run orders after them on the batch's stream
+  return 0;
+}
+
+// A run whose members are all as the last run left them: its tables and graph serve again, the
+// members' streams ordered before it by events (no host waits, no checks, no rebuild).
+template <typename T>
+int run_again(fdtd_batch *b, int64_t steps, const int64_t *first_steps, bool *ran) {
+  *ran = false;
+  const int n = (int)b->ctxs.size();
+  if (!b->reusable || b->record != b->cap_record || b->ndesign > 0 || (int)b->gens.size() != n)
+    return 0;
+  std::vector<InstanceView> views(n);
+  for (int i = 0; i < n; i++) {
+    if (fdtd_instance_view(b->ctxs[i], &views[i])) return 0;
+    const InstanceView &v = views[i];
+    if (v.generation != b->gens[i] || v.parity != b->next_parity[i] || v.nprobes > 0 ||
+        (first_steps ? first_steps[i] : 0) != b->next_first[i])
+      return 0;
+  }
+  while ((int)b->member_ev.size() < n) {
+    cudaEvent_t ev;
+    BTRY(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->member_ev.push_back(ev);
+  }
+  for (int i = 0; i < n; i++) {
+    BTRY(b, cudaEventRecord(b->member_ev[i], views[i].stream));
+    BTRY(b, cudaStreamWaitEvent(b->stream, b->member_ev[i], 0));
+  }
+  if (int r = finish_run<T>(b, steps, 0, views)) return r;
+  for (int i = 0; i < n; i++) {
+    b->next_first[i] += steps;
+    b->next_parity[i] = (int)((b->next_parity[i] + steps) & 1);
+  }
+  *ran = true;
+  return 0;
+}
+
 template <typename T>
 int run_impl(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
+  bool ran = false;
+  if (int r = run_again<T>(b, steps, first_steps, &ran)) return r;
+  if (ran) return 0;
   const int n = (int)b->ctxs.size();
   std::vector<InstanceView> views(n);
   std::vector<int64_t> first(n);
@@ -1073,37 +1160,18 @@ int run_impl(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
     }
   }
   if (int r = rebuild(b->shape)) return r;
-  const int64_t full = (steps - done) / G;
-  if (full > 0) {
-    // one chunk captured as a graph, replayed
-    cudaGraph_t g = nullptr;
-    const long long before = b->launches;
-    BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue<T>(b, G);
-    cudaError_t err = cudaStreamEndCapture(b->stream, &g);
-    if (err != cudaSuccess)
-      return bfail(b, FDTD_E_GPU, "cudaStreamEndCapture: %s", cudaGetErrorString(err));
-    const long long per_chunk = b->launches - before;
-    b->launches = before;
-    err = cudaGraphInstantiate(&b->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (err != cudaSuccess)
-      return bfail(b, FDTD_E_GPU, "cudaGraphInstantiate: %s", cudaGetErrorString(err));
-    for (int64_t c = 0; c < full; c++) {
-      BTRY(b, cudaGraphLaunch(b->graph, b->stream));
-      b->launches += per_chunk;
-    }
-    done += full * G;
-  }
-  if (done < steps) enqueue<T>(b, (int)(steps - done));
-  BTRY(b, cudaGetLastError());
-  BTRY(b, cudaEventRecord(b->done, b->stream));
+  b->reusable = false;
+  if (int r = finish_run<T>(b, steps, done, views)) return r;
+  b->reusable = true;
+  b->cap_record = b->record;
+  b->gens.assign(n, 0);
+  b->next_first.assign(n, 0);
+  b->next_parity.assign(n, 0);
   for (int i = 0; i < n; i++) {
-    BTRY(b, cudaStreamWaitEvent(views[i].stream, b->done, 0));
-    fdtd_instance_advance(b->ctxs[i], steps);
+    b->gens[i] = views[i].generation;
+    b->next_first[i] = (first_steps ? first_steps[i] : 0) + steps;
+    b->next_parity[i] = (int)((views[i].parity + steps) & 1);
   }
-  // no wait here: each context's stream waits for the batch's work (the event), so its later
-  // calls see the steps; the batch's next run orders after them on the batch's stream
   return 0;
 }
 
@@ -1158,6 +1226,7 @@ int fdtd_batch_tile(const fdtd_batch *b, int32_t *width, int32_t *height) {
 
 int fdtd_batch_set_tile(fdtd_batch *b, int32_t width, int32_t height) {
   if (!b) return FDTD_E_INVALID;
+  b->reusable = false;
   if (width == 0 && height == 0) {
     b->shape = -1;
     return 0;
@@ -1180,6 +1249,7 @@ void fdtd_batch_destroy(fdtd_batch *b) {
   if (b->done) cudaEventDestroy(b->done);
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->t1) cudaEventDestroy(b->t1);
+  for (cudaEvent_t ev : b->member_ev) cudaEventDestroy(ev);
   if (b->d_bad) cudaFree(b->d_bad);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;

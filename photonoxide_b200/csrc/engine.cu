@@ -1719,10 +1719,13 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 // The waveforms of a batch of steps, in f64 (src/fdtd.rs:329-423): for step m of the batch, w
 // at H's time t = (first+m) dt and at E's t + dt/2, 2 doubles each per emitter.
 // point[e]: 1 if emitter e is a point source (w.at), else 0 (complex_at)
+// base: the batch's first step index in device memory (a captured batch), or null (first).
 __global__ void waves_kernel(const Wave *waves, const int *point, int nw, long long first,
-                             int batch, double dt, double *out_h, double *out_e) {
+                             const long long *base, int batch, double dt, double *out_h,
+                             double *out_e) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nw * batch) return;
+  if (base) first = *base;
   int m = q / nw, e = q % nw;
   double t = (double)(first + m) * dt;
   double half = t + 0.5 * dt;
@@ -1754,9 +1757,11 @@ __global__ void gather_kernel(const T *e, const T *h, const long long *where, in
 // e^{i w t} dt for each step of the batch and each (monitor, field, frequency) slot
 // (src/fdtd/monitors.rs:178-183): E at te = (first+m+1) dt, H at te - dt/2.
 __global__ void phase_kernel(const double *omega, const int *slot_field, int nslots,
-                             long long first, int batch, double dt, double *out) {
+                             long long first, const long long *base, int batch, double dt,
+                             double *out) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nslots * batch) return;
+  if (base) first = *base;
   int m = q / nslots, s = q % nslots;
   double te = (double)(first + m + 1) * dt;
   double t = slot_field[s] ? te - 0.5 * dt : te;
@@ -1765,6 +1770,9 @@ __global__ void phase_kernel(const double *omega, const int *slot_field, int nsl
   out[2 * (long long)q] = cs * dt;
   out[2 * (long long)q + 1] = sn * dt;
 }
+
+// Sets a captured batch's first step index.
+__global__ void set_base_kernel(long long *base, long long first) { *base = first; }
 
 // sums[f][v] += sum_m ring[m][v] * phase[m][slot(f)], m in time order, f64 (monitors.rs:185-206).
 template <typename T>
@@ -1887,6 +1895,19 @@ struct fdtd_ctx {
   void *ring = nullptr;
   double *phase = nullptr;
   int ring_k = 0;
+  // every call that changes what the device holds or how it is laid out moves this on (a batch
+  // reuses its tables while its members' generations stay as it left them)
+  unsigned long long generation = 0;
+  // what a captured batch of steps bakes in (buffers, tables, kernels) changes only with these
+  // calls: the sources, probes, transforms, media and coefficients' set-up
+  unsigned long long layout = 0;
+  // K steps captured as a graph, one per current copy at the batch's start; their layout
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  unsigned long long graph_layout[2] = {0, 0};
+  long long graph_kernels[2] = {0, 0};
+  long long *d_base = nullptr;  // the captured batch's first step index
+  bool capturing = false;
+  bool warmed = false;  // a batch has run directly (lazily set kernel attributes are set)
   // the sources as last set (the batch builds its own tables from them)
   std::vector<fdtd_waveform> src_waves;
   std::vector<fdtd_injection> src_inj;
@@ -2096,7 +2117,8 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
     dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
     const size_t smem = quad::Smem<T>::BYTES;
     auto go = [&](auto kernel) {
-      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (!c->capturing)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       kernel<<<grid, quad::THREADS, smem, c->stream>>>(A);
     };
     // media: the step without them, then their pass over the members
@@ -2130,7 +2152,8 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
   dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
   const size_t smem = plain_smem_bytes<T>();
   auto go = [&](auto kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (!c->capturing)
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kernel<<<grid, NT, smem, c->stream>>>(A);
   };
   if (c->media) {
@@ -2207,13 +2230,13 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
     c->record = nr;
     c->record_cap = cap;
   }
-  long long done = 0;
-  while (done < steps) {
-    int batch = (int)std::min<long long>(K, steps - done);
+  // one batch of `batch` steps from step index first + at (or *base when captured)
+  auto enqueue_batch = [&](int batch, long long at, const long long *base) {
     if (c->nwaves > 0) {
       int total = c->nwaves * batch;
       waves_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(
-          c->d_waves, c->d_point, c->nwaves, first + done, batch, c->dt, c->waves_h, c->waves_e);
+          c->d_waves, c->d_point, c->nwaves, first + at, base, batch, c->dt, c->waves_h,
+          c->waves_e);
       c->launches++;
     }
     for (int m = 0; m < batch; m++) {
@@ -2239,7 +2262,7 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
       long long gathered = c->nvalues + c->nprobes;
       if (gathered > 0) {
         T *row = c->nvalues ? (T *)c->ring + (long long)m * c->nvalues : nullptr;
-        double *rec = c->nprobes ? c->record + (c->recorded + done + m) * c->nprobes : nullptr;
+        double *rec = c->nprobes ? c->record + (c->recorded + at + m) * c->nprobes : nullptr;
         gather_kernel<T><<<(unsigned)((gathered + 255) / 256), 256, 0, c->stream>>>(
             (const T *)c->e[c->parity], (const T *)c->h[c->parity], c->d_where, (int)c->nvalues,
             row, c->d_probes, c->nprobes, rec);
@@ -2249,12 +2272,52 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
     if (c->nvalues > 0) {
       int total = c->nslots * batch;
       phase_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(c->d_omega, c->d_slot_field,
-                                                                c->nslots, first + done, batch,
-                                                                c->dt, c->phase);
+                                                                c->nslots, first + at, base,
+                                                                batch, c->dt, c->phase);
       dft_kernel<T><<<(unsigned)((c->nvalues + 127) / 128), 128, 0, c->stream>>>(
           c->d_series, c->nseries, c->d_value_series, c->nvalues, (const T *)c->ring, batch,
           c->phase, c->nslots, c->sums);
       c->launches += 2;
+    }
+  };
+  // whole batches replay a captured graph (K even: a batch leaves the current copy as it found
+  // it), unless probes (their record rows move) or per-launch timing are asked for
+  const bool graphs = !c->profiling && c->nprobes == 0 && K % 2 == 0;
+  long long done = 0;
+  while (done < steps) {
+    const int batch = (int)std::min<long long>(K, steps - done);
+    if (graphs && batch == K && c->warmed) {
+      if (!c->d_base) {
+        if (int r = alloc(c, (void **)&c->d_base, 8)) return r;
+      }
+      const int p = c->parity;
+      if (!c->graph[p] || c->graph_layout[p] != c->layout) {
+        if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
+        c->graph[p] = nullptr;
+        cudaGraph_t g = nullptr;
+        const long long before = c->launches;
+        c->capturing = true;
+        cudaError_t err = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+        if (err == cudaSuccess) {
+          enqueue_batch(K, 0, c->d_base);
+          err = cudaStreamEndCapture(c->stream, &g);
+        }
+        c->capturing = false;
+        c->parity = p;  // the capture's bookkeeping flipped it K times
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&c->graph[p], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (err != cudaSuccess)
+          return fail(c, FDTD_E_GPU, "capturing a batch of steps: %s", cudaGetErrorString(err));
+        c->graph_kernels[p] = c->launches - before;
+        c->launches = before;
+        c->graph_layout[p] = c->layout;
+      }
+      set_base_kernel<<<1, 1, 0, c->stream>>>(c->d_base, first + done);
+      CUDA_TRY(c, cudaGraphLaunch(c->graph[p], c->stream));
+      c->launches += 1 + c->graph_kernels[p];
+    } else {
+      enqueue_batch(batch, done, nullptr);
+      c->warmed = true;
     }
     done += batch;
   }
@@ -2433,6 +2496,8 @@ void fdtd_destroy(fdtd_ctx *c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (cudaEvent_t ev : c->events) cudaEventDestroy(ev);
+  for (int p = 0; p < 2; p++)
+    if (c->graph[p]) cudaGraphExecDestroy(c->graph[p]);
   if (c->stream) {
     for (void *p : c->allocations) cudaFreeAsync(p, c->stream);
     cudaStreamSynchronize(c->stream);
@@ -2443,6 +2508,8 @@ void fdtd_destroy(fdtd_ctx *c) {
 
 int fdtd_upload_coeffs(fdtd_ctx *c, const double *ca, const double *cb) {
   if (!c || !cb) return fail(c, FDTD_E_INVALID, "cb is needed");
+  c->generation++;
+  c->layout++;
   c->lossless = ca == nullptr;
   if (ca) {
     if (!c->ca)
@@ -2456,6 +2523,7 @@ int fdtd_upload_coeffs(fdtd_ctx *c, const double *ca, const double *cb) {
 
 int fdtd_upload_fields(fdtd_ctx *c, const double *e, const double *h, const double *const *psi) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
   c->parity = 0;
   size_t E = c->elem;
   if (e) { if (int r = upload(c, c->e[0], e, 3 * c->N)) return r; }
@@ -2515,6 +2583,8 @@ int fdtd_download_fields(fdtd_ctx *c, double *e, double *h, double *const *psi) 
 int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, int64_t ninj,
                      const fdtd_injection *inj) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
+  c->layout++;
   int nx = c->n[0], ny = c->n[1], nz = c->n[2];
   std::vector<int> point(std::max(nwaves, 1), -1);
   for (int64_t q = 0; q < ninj; q++) {
@@ -2666,6 +2736,8 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
 int fdtd_set_probes(fdtd_ctx *c, int32_t n, const int32_t *field, const int32_t *component,
                     const int64_t *r) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
+  c->layout++;
   std::vector<long long> w(std::max(n, 1));
   for (int p = 0; p < n; p++) {
     if (field[p] < 0 || field[p] > 1 || component[p] < 0 || component[p] > 2 || r[p] < 0 ||
@@ -2689,6 +2761,8 @@ int fdtd_set_probes(fdtd_ctx *c, int32_t n, const int32_t *field, const int32_t 
 int fdtd_set_dft(fdtd_ctx *c, int32_t nseries, const fdtd_series *series, int32_t nmonitors,
                  const int32_t *freqs_per_monitor, const double *freqs) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
+  c->layout++;
   // phase slots: per monitor, its frequencies at E's times then at H's (resident.rs:714-730)
   std::vector<int> slot0(nmonitors + 1, 0), fcount(nmonitors, 0), fstart(nmonitors, 0);
   std::vector<double> omega;
@@ -2785,6 +2859,8 @@ int fdtd_set_dft(fdtd_ctx *c, int32_t nseries, const fdtd_series *series, int32_
 
 int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
+  c->layout++;
   long long members = 0;
   int maxp = 1;
   for (int g = 0; g < ngroups; g++) {
@@ -2869,6 +2945,7 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
 
 int fdtd_run_async(fdtd_ctx *c, int64_t steps, int64_t first_step) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
   if (steps < 0) return fail(c, FDTD_E_INVALID, "a negative number of steps");
   if (steps == 0) return 0;
   c->launches = 0;
@@ -2890,6 +2967,7 @@ int fdtd_run(fdtd_ctx *c, int64_t steps, int64_t first_step) {
 
 int fdtd_read_probes(fdtd_ctx *c, double *out, int64_t capacity, int64_t *steps) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
   if (steps) *steps = c->nprobes > 0 ? c->recorded : 0;
   if (!out || c->nprobes == 0) return 0;
   long long n = c->recorded * c->nprobes;
@@ -3000,6 +3078,7 @@ int upload_static_as(fdtd_ctx *c, double *stage, void *dst, const double *src, l
 
 extern "C" int fdtd_upload_fields_static(fdtd_ctx *c, const double *e, const double *h) {
   if (!c) return FDTD_E_INVALID;
+  c->generation++;
   if (c->N > STATIC_STAGE_VALUES)
     return fail(c, FDTD_E_INVALID,
                 "a field component of %lld values exceeds the %lld-value static staging array: "
@@ -3084,6 +3163,7 @@ int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
   v->probes = c->d_probes;
   v->media = c->media;
   v->stream = c->stream;
+  v->generation = c->generation;
   return 0;
 }
 

@@ -4,6 +4,7 @@
 // through the engine's C ABI (photonoxide_fdtd.h). Compiled without floating-point contraction,
 // so every table is the reference's bits.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -298,6 +299,7 @@ struct pxs_sim {
   std::vector<MediaGroup> groups;
   std::map<std::pair<int, int64_t>, int> members;
   bool configured = false;  // sources, probes and transforms pushed to the engine
+  bool fields_dropped = false;  // released without reading the fields back (a served job's)
   fdtd_ctx *ctx = nullptr;
 
   int64_t N() const { return g.cells(); }
@@ -520,8 +522,15 @@ struct pxs_sim {
     return push_fields();
   }
 
+  int dropped() {
+    return fail(FDTD_E_STATE, "the fields of this simulation were not kept after its served job "
+                              "(submitted with keep_fields off): its transforms, fluxes and probes "
+                              "are its results");
+  }
+
   int run(int64_t count) {
     if (count <= 0) return 0;
+    if (fields_dropped) return dropped();
     if (int r = prepare()) return r;
     if (int r = fdtd_run(ctx, count, steps)) return fail(r, "%s", fdtd_last_error(ctx));
     return finish(count);
@@ -530,9 +539,13 @@ struct pxs_sim {
   // Everything the device holds brought to the host (fields, psi, transforms; the probes are
   // read after each run), then the engine and its device memory released. A later run makes a
   // new engine from the host's copies.
-  int release() {
+  int release(bool keep_fields = true) {
     if (!ctx) return 0;
-    if (int r = pull()) return r;
+    if (keep_fields) {
+      if (int r = pull()) return r;
+    } else {
+      fields_dropped = true;  // the host's copies are stale: reading them or running refuses
+    }
     if (int r = pull_sums()) return r;
     fdtd_destroy(ctx);
     ctx = nullptr;
@@ -1344,6 +1357,7 @@ double pxs_dt(const pxs_sim *s) { return s->dt; }
 int64_t pxs_steps(const pxs_sim *s) { return s->steps; }
 
 int pxs_get_field(pxs_sim *s, int32_t field, int32_t comp, double *out) {
+  if (s->fields_dropped) return s->dropped();
   if (int r = s->pull()) return r;
   const std::vector<double> &v = field == 0 ? s->e : s->h;
   int64_t N = s->N();
@@ -1353,6 +1367,7 @@ int pxs_get_field(pxs_sim *s, int32_t field, int32_t comp, double *out) {
 }
 
 int pxs_set_field(pxs_sim *s, int32_t field, int32_t comp, const double *in) {
+  if (s->fields_dropped) return s->dropped();
   if (int r = s->pull()) return r;
   std::vector<double> &v = field == 0 ? s->e : s->h;
   int64_t N = s->N();
@@ -1616,6 +1631,25 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// f(0) .. f(count-1) on up to 8 threads (each with the device current): jobs' host work and
+// launches are independent, each on its own engine and stream.
+template <typename F>
+void parallel_for(int count, int device, F f) {
+  const int threads = std::min(count, 8);
+  if (threads <= 1) {
+    for (int i = 0; i < count; i++) f(i);
+    return;
+  }
+  std::atomic<int> next(0);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; t++)
+    pool.emplace_back([&] {
+      cudaSetDevice(device);
+      for (int i; (i = next++) < count;) f(i);
+    });
+  for (std::thread &t : pool) t.join();
+}
+
 enum { JOB_QUEUED = 0, JOB_RUNNING = 1, JOB_DONE = 2, JOB_FAILED = 3, JOB_CANCELLED = 4 };
 
 struct ServerJob {
@@ -1623,7 +1657,7 @@ struct ServerJob {
   pxs_sim *sim = nullptr;
   int64_t steps = 0, done = 0;
   int state = JOB_QUEUED;
-  bool te = false, prepared = false;
+  bool te = false, prepared = false, keep_fields = true;
   size_t bytes = 0;
   double submitted = 0, started = 0, finished = 0;
   std::string error;
@@ -1705,15 +1739,18 @@ struct pxs_server {
       // launch: the others each on its own stream, the 2D TE jobs as one batch (remade when its
       // members change), as many steps as the batch's job nearest its end still needs
       std::vector<int64_t> took(other.size(), 0);
+      std::vector<std::string> why(other.size());
       std::vector<std::pair<ServerJob *, std::string>> failed;
-      for (size_t q = 0; q < other.size(); q++) {
+      parallel_for((int)other.size(), device, [&](int q) {
         ServerJob *j = other[q];
         took[q] = std::min(chunk, j->steps - j->done);
         if (fdtd_run_async(j->sim->ctx, took[q], j->sim->steps)) {
-          failed.push_back({j, fdtd_last_error(j->sim->ctx)});
+          why[q] = fdtd_last_error(j->sim->ctx);
           took[q] = -1;
         }
-      }
+      });
+      for (size_t q = 0; q < other.size(); q++)
+        if (took[q] < 0) failed.push_back({other[q], why[q]});
       int64_t te_took = 0;
       if (!te.empty()) {
         if (te != batch_jobs) {
@@ -1749,22 +1786,30 @@ struct pxs_server {
       const double t1 = now_s();
       // while the device steps: the last round's finished jobs read back (their own streams),
       // the newly admitted ones set up
-      for (ServerJob *j : finished) {
-        const int r = j->sim->release();
+      {
+        std::vector<ServerJob *> tasks(finished);
+        tasks.insert(tasks.end(), admitted.begin(), admitted.end());
+        const size_t nfin = finished.size();
+        std::vector<int> code(tasks.size(), 0);
+        parallel_for((int)tasks.size(), device, [&](int q) {
+          ServerJob *j = tasks[q];
+          if ((size_t)q < nfin) {
+            code[q] = j->sim->release(j->keep_fields);
+          } else {
+            code[q] = j->sim->prepare();
+            if (code[q]) j->sim->release();
+          }
+        });
         std::lock_guard<std::mutex> lock(mu);
-        finish_job(j, r ? JOB_FAILED : JOB_DONE, r ? j->sim->error : std::string());
+        for (size_t q = 0; q < tasks.size(); q++) {
+          ServerJob *j = tasks[q];
+          if (q < nfin) finish_job(j, code[q] ? JOB_FAILED : JOB_DONE, code[q] ? j->sim->error : std::string());
+          else if (code[q]) finish_job(j, JOB_FAILED, j->sim->error.empty() ? "setup failed" : j->sim->error);
+          else j->prepared = true;
+        }
         cv.notify_all();
       }
       finished.clear();
-      for (ServerJob *j : admitted) {
-        if (j->sim->prepare()) {
-          std::lock_guard<std::mutex> lock(mu);
-          j->sim->release();
-          finish_job(j, JOB_FAILED, j->sim->error.empty() ? "setup failed" : j->sim->error);
-        } else {
-          j->prepared = true;
-        }
-      }
       const double t2 = now_s();
       // the round's steps done
       for (size_t q = 0; q < other.size(); q++)
@@ -1801,7 +1846,7 @@ struct pxs_server {
       cv.notify_all();
     }
     for (ServerJob *j : finished) {
-      j->sim->release();
+      j->sim->release(j->keep_fields);
       std::lock_guard<std::mutex> lock(mu);
       finish_job(j, JOB_DONE, std::string());
     }
@@ -1830,11 +1875,16 @@ int pxs_server_create(size_t hbm_budget, int32_t max_active, int64_t chunk, pxs_
 
 const char *pxs_server_last_error(const pxs_server *sv) { return sv ? sv->error.c_str() : "no server"; }
 
-int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps) {
+int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps, int32_t keep_fields) {
   if (!sv || !s || steps <= 0) return FDTD_E_INVALID;
+  if (s->fields_dropped) {
+    sv->error = s->dropped() ? s->error : std::string();
+    return FDTD_E_STATE;
+  }
   ServerJob *j = new ServerJob();
   j->sim = s;
   j->steps = steps;
+  j->keep_fields = keep_fields != 0;
   j->te = s->te();
   j->bytes = s->device_bytes();
   j->submitted = now_s();

@@ -37,6 +37,7 @@ struct InstanceView {
   const long long *probes;
   bool media;
   cudaStream_t stream;
+  unsigned long long generation;  // moves on with every change the engine's calls make
 };
 
 int fdtd_instance_view(fdtd_ctx *c, InstanceView *v);

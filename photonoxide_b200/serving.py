@@ -34,7 +34,7 @@ def _lib():
         x.pxs_server_create.argtypes = [C.c_size_t, I32, I64, C.POINTER(P)]
         x.pxs_server_last_error.argtypes = [P]
         x.pxs_server_last_error.restype = C.c_char_p
-        x.pxs_server_submit.argtypes = [P, P, I64]
+        x.pxs_server_submit.argtypes = [P, P, I64, I32]
         x.pxs_server_submit.restype = I64
         x.pxs_server_poll.argtypes = [P, I64, DP]
         x.pxs_server_wait.argtypes = [P, I64]
@@ -87,8 +87,11 @@ class Server:
             raise InvalidValue(msg)
         self.jobs: List[Job] = []
 
-    def submit(self, sim: Simulation, steps: int) -> Job:
-        id = _lib().pxs_server_submit(self._h, sim._h, int(steps))
+    def submit(self, sim: Simulation, steps: int, keep_fields: bool = True) -> Job:
+        """Queues ``steps`` steps of ``sim``. With ``keep_fields`` off only its transforms,
+        fluxes and probes come back when the job ends (its fields are dropped with the device
+        memory, which saves reading them back)."""
+        id = _lib().pxs_server_submit(self._h, sim._h, int(steps), 1 if keep_fields else 0)
         if id < 0:
             msg = _lib().pxs_server_last_error(self._h).decode()
             raise InvalidValue(msg) if id == FDTD_E_INVALID else GpuError(msg)

@@ -58,3 +58,18 @@ def test_a_job_beyond_the_budget_fails_and_a_queued_job_cancels():
         second.cancel()
         assert first.wait() == DONE
         assert second.poll()[0] == CANCELLED
+
+
+def test_a_job_without_its_fields_keeps_its_transforms():
+    sp = small_stream(1, 11)[0]
+    alone = make_job(sp)
+    alone.run(sp.steps)
+    with Server(hbm_budget=500e6, max_active=2, chunk=64) as server:
+        job = server.submit(make_job(sp), sp.steps, keep_fields=False)
+        assert job.wait() == DONE
+        assert np.array_equal(job.sim.transforms(), alone.transforms())
+        assert np.array_equal(job.sim.flux(0), alone.flux(0))
+        with pytest.raises(GpuError):
+            job.sim.e(0)
+        with pytest.raises(GpuError):
+            job.sim.run(1)
