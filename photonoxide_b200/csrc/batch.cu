@@ -651,7 +651,8 @@ struct fdtd_batch {
   void *d_ring = nullptr;  // G rows of the transform values
   long long nring = 0;
   int blocks = 0;
-  int *d_bad = nullptr;  // the TE check's flag
+  int *d_flags = nullptr;  // one TE-check flag per member
+  int flags_cap = 0;
   // for the adjoint's recomputation: transforms and probes off, and after each step the E curl
   // at the design's values into K[step - k_first][value]
   bool record = true;
@@ -1099,20 +1100,41 @@ int run_impl(fdtd_batch *b, int64_t steps, const int64_t *first_steps) {
       return bfail(b, r, "simulation %d: %s", i, fdtd_last_error(c));
     first[i] = first_steps ? first_steps[i] : 0;
     parity[i] = v.parity;
-    BTRY(b, cudaStreamSynchronize(v.stream));
-    BTRY(b, cudaMemsetAsync(b->d_bad, 0, 4, b->stream));
+  }
+  // the members' streams before the batch's (events: the host doesn't wait), then one check of
+  // every member's TM components (one flag each) and one wait for its answer
+  while ((int)b->member_ev.size() < n) {
+    cudaEvent_t ev;
+    BTRY(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->member_ev.push_back(ev);
+  }
+  if (b->flags_cap < n) {
+    if (b->d_flags) BTRY(b, cudaFreeAsync(b->d_flags, b->stream));
+    b->d_flags = nullptr;
+    BTRY(b, cudaMallocAsync(&b->d_flags, (size_t)n * 4, b->stream));
+    b->flags_cap = n;
+  }
+  BTRY(b, cudaMemsetAsync(b->d_flags, 0, (size_t)n * 4, b->stream));
+  for (int i = 0; i < n; i++) {
+    const InstanceView &v = views[i];
+    BTRY(b, cudaEventRecord(b->member_ev[i], v.stream));
+    BTRY(b, cudaStreamWaitEvent(b->stream, b->member_ev[i], 0));
     te_tm_check_kernel<T><<<(unsigned)((v.N + 255) / 256), 256, 0, b->stream>>>(
-        (const T *)v.e[v.parity], (const T *)v.h[v.parity], v.N, b->d_bad);
-    int bad = 0;
-    BTRY(b, cudaMemcpyAsync(&bad, b->d_bad, 4, cudaMemcpyDeviceToHost, b->stream));
-    BTRY(b, cudaStreamSynchronize(b->stream));
-    if (bad)
-      return bfail(b, FDTD_E_INVALID,
-                   "simulation %d has H_x, H_y or E_z values: the batch steps TE fields only", i);
+        (const T *)v.e[v.parity], (const T *)v.h[v.parity], v.N, b->d_flags + i);
     // the other copy's TM components stay zero too
     const size_t E = sizeof(T);
     BTRY(b, cudaMemsetAsync((char *)v.h[1 - v.parity], 0, 2 * v.N * E, b->stream));
     BTRY(b, cudaMemsetAsync((char *)v.e[1 - v.parity] + 2 * v.N * E, 0, v.N * E, b->stream));
+  }
+  {
+    std::vector<int> bad(n, 0);
+    BTRY(b, cudaMemcpyAsync(bad.data(), b->d_flags, (size_t)n * 4, cudaMemcpyDeviceToHost,
+                            b->stream));
+    BTRY(b, cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; i++)
+      if (bad[i])
+        return bfail(b, FDTD_E_INVALID,
+                     "simulation %d has H_x, H_y or E_z values: the batch steps TE fields only", i);
   }
   // where the device's descriptors have moved the instances to
   auto pull = [&]() -> int {
@@ -1202,7 +1224,6 @@ int fdtd_batch_create(int32_t count, fdtd_ctx *const *ctxs, fdtd_batch **out) {
   BTRY(b, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
   BTRY(b, cudaEventCreate(&b->t0));
   BTRY(b, cudaEventCreate(&b->t1));
-  BTRY(b, cudaMalloc(&b->d_bad, 4));
   return 0;
 }
 
@@ -1250,7 +1271,8 @@ void fdtd_batch_destroy(fdtd_batch *b) {
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->t1) cudaEventDestroy(b->t1);
   for (cudaEvent_t ev : b->member_ev) cudaEventDestroy(ev);
-  if (b->d_bad) cudaFree(b->d_bad);
+  if (b->d_flags) cudaFreeAsync(b->d_flags, b->stream);
+  if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
