@@ -1309,6 +1309,84 @@ __device__ __forceinline__ void cpml4(const StepArgs<T> &A, int k, int my, int m
   if (sy >= 0) y_slab(2, minus, diff[2][1], v[2], FIELD == 1 ? zero4 : cbv[2]);
 }
 
+// The x-slab places of a quad tile's rows (the same for every row of the tile), as positions
+// 0..ROW-1 of the row: where the positions hold one side's slab only, at most 16 places, p0 and
+// P and the side (0 low, 1 high); otherwise side -1.
+template <typename T>
+__device__ __forceinline__ int xslab_places(const StepArgs<T> &A, int x0, int &p0, int &P) {
+  using quad::ROW;
+  using quad::VEC;
+  if (A.periodic[0]) return -1;
+  const int nx = A.n[0];
+  const int l0 = max(0, VEC - x0), l1 = min(ROW, VEC - x0 + A.low[0]);
+  const int h0 = max(0, nx - A.high[0] - x0 + VEC), h1 = min(ROW, nx - x0 + VEC);
+  const int nl = max(0, l1 - l0), nh = max(0, h1 - h0);
+  if (nl > 0 && nh == 0 && nl <= 16) return p0 = l0, P = nl, 0;
+  if (nh > 0 && nl == 0 && nh <= 16) return p0 = h0, P = nh, 1;
+  return -1;
+}
+
+// The x CPML of one field over a warp's row, its values shared out over the lanes: the row holds
+// the slab's places p0 .. p0+P-1 (xslab_places), and lane L < 2P updates component 1 + L / P at
+// place p0 + L % P with the owning lane's x difference (shuffled in); the owner applies the
+// result (shuffled back). Each value's arithmetic and each component's order of slabs are
+// slab4x's (x before the others); only the lane that computes it differs, so that a tile whose
+// rows meet an x CPML pays for its few places once per warp, not once per place of each lane.
+// Lanes below `ownmin` own no values (E: the halo lane). Every lane of the warp calls it.
+template <typename T, int FIELD>
+__device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x0, int lane,
+                                      int ownmin, bool write, T v[3][4], const T d1[4],
+                                      const T d2[4], const T cbv[3][4], const T *xc) {
+  using quad::ROW;
+  using quad::VEC;
+  int p0 = 0, P = 0;
+  const int side = xslab_places(A, x0, p0, P);
+  const int c = lane < P ? 1 : 2;
+  const int pos = p0 + lane - (c - 1) * P;
+  const bool work = lane < 2 * P && (pos >> 2) >= ownmin;
+  const int src = work ? (pos >> 2) : lane;
+  const int jj = pos & 3;
+  T d = T(0);
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const T t1 = __shfl_sync(0xffffffffu, d1[r], src);
+    const T t2 = __shfl_sync(0xffffffffu, d2[r], src);
+    if (jj == r) d = c == 1 ? t1 : t2;
+  }
+  T u = T(0);
+  if (work) {
+    const SlabEntry &s = A.slab[FIELD][c][0][side];
+    if (s.count) {
+      const long long at = s.psi + ((long long)k * A.n[1] + my) * s.pw + (x0 - VEC + pos - s.pf);
+      const T *t = xc + ((FIELD * 2 + (c - 1)) * 2) * ROW;
+      const T b = t[pos], a = t[ROW + pos];
+      const T old = (FIELD == 1 ? A.psi_h_in : A.psi_e)[at];
+      const T q = div_by_step(d, A.step[0], A.inv_step[0], A.inv_step64[0], A.fast_div[0]);
+      const T nw = b * old + a * q;
+      u = (c == 1 ? T(-1) : T(1)) * nw;
+      if (write && (pos >> 2) >= 1) (FIELD == 1 ? A.psi_h_out : A.psi_e)[at] = nw;
+    }
+  }
+  const bool has1 = A.slab[FIELD][1][0][side].count != 0;
+  const bool has2 = A.slab[FIELD][2][0][side].count != 0;
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int q = 4 * lane + r - p0;  // this lane's place r as a worker of component 1
+    const bool mine = q >= 0 && q < P && lane >= ownmin;
+    const T g1 = __shfl_sync(0xffffffffu, u, mine ? q : lane);
+    const T g2 = __shfl_sync(0xffffffffu, u, mine ? P + q : lane);
+    if (mine) {
+      if (FIELD == 1) {
+        if (has1) v[1][r] = v[1][r] - A.dt * g1;
+        if (has2) v[2][r] = v[2][r] - A.dt * g2;
+      } else {
+        if (has1) v[1][r] = v[1][r] + cbv[1][r] * g1;
+        if (has2) v[2][r] = v[2][r] + cbv[2][r] * g2;
+      }
+    }
+  }
+}
+
 template <typename T, bool LOSSY, bool MEDIA>
 __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   using namespace quad;
@@ -1388,6 +1466,14 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
   }
   const bool any_own = ownv[0] | ownv[1] | ownv[2] | ownv[3];
+  // the row's x-slab places (the same for every warp): one side's, at most 16, are shared out
+  // over the warp's lanes (xcoop), and cpml4 takes no x slab; otherwise each lane takes its own
+  bool xco;
+  {
+    int p0, P;
+    xco = xslab_places(A, x0, p0, P) >= 0;
+  }
+  if (xco) sxl = -1;
   const T fhy = my >= 0 ? A.fh[nx + my] : T(0), fey = my >= 0 ? A.fe[nx + my] : T(0);
   int sy = -1;
   if (my >= 0 && !A.periodic[1]) {
@@ -1503,7 +1589,11 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
     // the CPML: H_x along y then z, H_y along x then z, H_z along x then y
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
-    if (rowh && mxb >= 0 && (zs | (sy >= 0) | any_x)) {
+    if (xco && rowh) {
+      const T nocb[3][4] = {};
+      xcoop<T, 1>(A, k, my, x0, lane, 0, write && w >= 1, hn, dxEz, dxEy, nocb, sXC);
+    }
+    if (rowh && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
       const bool ow = write && w >= 1 && lane >= 1;
       const T diff[3][3][4] = {
           {{T(0), T(0), T(0), T(0)}, {dyEz[0], dyEz[1], dyEz[2], dyEz[3]}, {dzEy[0], dzEy[1], dzEy[2], dzEy[3]}},
@@ -1633,7 +1723,13 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         en[2][j] = cav[2] * e[2].v[j] + cb[2].v[j] * curl2;
       }
       // the CPML: E_x along y then z, E_y along x then z, E_z along x then y
-      if (any_own && mxb >= 0 && (zs | (sy >= 0) | any_x)) {
+      if (xco && rowh) {
+        const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
+                             {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
+                             {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
+        xcoop<T, 0>(A, k, my, x0, lane, 1, true, en, dxHz, dxHy, cbs, sXC);
+      }
+      if (any_own && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
         const T diff[3][3][4] = {
             {{T(0), T(0), T(0), T(0)}, {dyHz[0], dyHz[1], dyHz[2], dyHz[3]}, {dzHy[0], dzHy[1], dzHy[2], dzHy[3]}},
             {{dxHz[0], dxHz[1], dxHz[2], dxHz[3]}, {T(0), T(0), T(0), T(0)}, {dzHx[0], dzHx[1], dzHx[2], dzHx[3]}},
@@ -2476,10 +2572,11 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   c->tiles_x = (c->n[0] + c->tile_w - 1) / c->tile_w;
   c->tiles_y = (c->n[1] + c->tile_h - 1) / c->tile_h;
   long long tiles = (long long)c->tiles_x * c->tiles_y;
-  // z cut into runs so that the CTAs fill the device about twelve times over: runs that meet a
-  // CPML take several times longer than the rest, and short runs let the scheduler balance
-  // them. Each run recomputes one plane of H, so a run is at least 4 planes long.
-  long long want = 24LL * sms;
+  // z cut into runs so that the CTAs fill the device about six times over: runs that meet a
+  // CPML take longer than the rest, and shorter runs let the scheduler balance them, while each
+  // run recomputes one plane of H (a run is at least 4 planes long). On the 3D MMI 13 runs of 8
+  // planes timed best (4 % faster than 25 of 4, 9 % than 8 of 13).
+  long long want = 12LL * sms;
   int chunks = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
   chunks = std::min(chunks, std::max(1, c->n[2] / 4));
   const char *zc = getenv("PHOTONOXIDE_FDTD_ZCHUNKS");

@@ -51,6 +51,21 @@ def test_stirred_bit_for_bit(precision, periodic, n):
 
 
 @pytest.mark.parametrize("precision", [32, 64])
+@pytest.mark.parametrize("n,cpml,periodic", [((260, 24, 23), 10, ()), ((252, 23, 22), 10, ()),
+                                             ((256, 8, 6), 15, (1, 2)), ((264, 9, 6), 20, (1, 2))])
+def test_long_rows_bit_for_bit(precision, n, cpml, periodic):
+    """Rows longer than one tile: the x CPML's places of a tile's row shared out over a warp's
+    lanes (one side's, at most 16: 10 and 11, 15 and 16 places), a high slab straddling two tiles
+    (252), and slabs of 20 and 21 places (each lane its own)."""
+    p = stirred(lambda *a: Simulation(*a, precision=precision), periodic, cpml, n)
+    o = stirred(lambda *a: OracleSimulation(*a, precision=precision), periodic, cpml, n)
+    p.run(37)
+    o.run(37)
+    for c, (x, y) in enumerate(zip(fields(p), fields(o))):
+        assert np.array_equal(x, y), (c, relative(x, y))
+
+
+@pytest.mark.parametrize("precision", [32, 64])
 def test_two_d_bit_for_bit(precision):
     """A grid one cell thick and periodic along z (Boundaries::cpml_2d), odd sizes."""
     def make(cls):
@@ -80,7 +95,8 @@ def test_closed_box_f32_bit_for_bit_over_300_steps():
 
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("two_d,n", [(False, None), (True, None), (False, (40, 21, 19)),
-                                     (True, (72, 45, 1)), (False, (96, 37, 14))])
+                                     (True, (72, 45, 1)), (False, (96, 37, 14)),
+                                     (False, (256, 21, 19))])
 def test_busy_bit_for_bit(two_d, n, precision):
     p = busy(lambda *a: Simulation(*a, precision=precision), two_d, n=n)
     o = busy(lambda *a: OracleSimulation(*a, precision=precision), two_d, n=n)
