@@ -101,6 +101,7 @@ struct StepArgs {
   const double *waves_h;  // this step's w at H's time: 2 per emitter
   const double *waves_e;  // at E's time
   int tiles_x, tiles_y, zchunk;
+  const int *order;  // quad kernel: CTA b takes run order[b] / tiles, tile order[b] % tiles
   MediaArgs<T> media;
 };
 
@@ -1399,9 +1400,11 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
   const long long N = A.N;
-  const int tile = blockIdx.x;
+  const int ntiles = A.tiles_x * A.tiles_y;
+  const int cta = A.order[blockIdx.x];  // heaviest first (quad_order)
+  const int tile = cta % ntiles;
   const int x0 = (tile % A.tiles_x) * OWNX, y0 = (tile / A.tiles_x) * RW;
-  const int kbeg = blockIdx.y * A.zchunk, kend = min(kbeg + A.zchunk, nz);
+  const int kbeg = (cta / ntiles) * A.zchunk, kend = min(kbeg + A.zchunk, nz);
   if (kbeg >= nz) return;
   const long long plane = (long long)nx * ny;
   T *sXC = sX + S::X;                                // quad::Smem::XC
@@ -1971,6 +1974,7 @@ struct fdtd_ctx {
   Wave *d_waves = nullptr;
   int *d_point = nullptr;
   int *hbucket = nullptr, *ebucket = nullptr;
+  int *order = nullptr;  // the quad kernel's CTAs, heaviest first
   Group *hgroups = nullptr, *egroups = nullptr;
   Entry *entries = nullptr;
   double *waves_h = nullptr, *waves_e = nullptr;  // batch x nwaves x 2
@@ -2157,6 +2161,7 @@ StepArgs<T> step_args(fdtd_ctx *c) {
   A.tiles_x = c->tiles_x;
   A.tiles_y = c->tiles_y;
   A.zchunk = c->zchunk;
+  A.order = c->order;
   if (sizeof(T) == 8) memcpy(&A.media, &c->md, sizeof A.media);
   else memcpy(&A.media, &c->mf, sizeof A.media);
   return A;
@@ -2210,7 +2215,7 @@ __global__ void media_kernel(StepArgs<T> A) {
 template <typename T>
 void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
   if (c->quad) {
-    dim3 grid(c->tiles_x * c->tiles_y, c->zchunks);
+    dim3 grid(c->tiles_x * c->tiles_y * c->zchunks);
     const size_t smem = quad::Smem<T>::BYTES;
     auto go = [&](auto kernel) {
       if (!c->capturing)
@@ -2293,6 +2298,43 @@ int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
   std::lock_guard<std::mutex> lock(mu);
   seen[key] = *ok;
   return 0;
+}
+
+// The quad kernel's CTAs (run r, tile t as r * tiles + t) in launch order: by an estimate of
+// their time, heaviest first, so that the CTAs that start last are short and the step, which
+// ends with its last CTA, leaves few SMs idle at its end. A plane costs 1, 1.8 in a z CPML; a
+// tile whose rows reach an x CPML 1.4 times that, and up to 1.8 times with all its rows in a y
+// CPML; a run's first, recomputed plane of H 0.6 of a plane.
+std::vector<int> quad_order(const fdtd_ctx *c) {
+  const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
+  const int tiles = c->tiles_x * c->tiles_y;
+  auto zslab = [&](int k) { return !c->periodic[2] && (k < c->low[2] || k >= nz - c->high[2]); };
+  std::vector<std::pair<double, int>> cost;
+  cost.reserve((size_t)tiles * c->zchunks);
+  for (int r = 0; r < c->zchunks; r++)
+    for (int t = 0; t < tiles; t++) {
+      const int x0 = (t % c->tiles_x) * quad::OWNX, y0 = (t / c->tiles_x) * quad::RW;
+      const bool xe = !c->periodic[0] &&
+          ((c->low[0] > 0 && x0 - quad::VEC < c->low[0]) ||
+           (c->high[0] > 0 && x0 + quad::OWNX > nx - c->high[0]));
+      int yrows = 0;
+      for (int gy = y0 - 1; gy < y0 + quad::RW; gy++)
+        if (!c->periodic[1] && gy >= 0 && gy < ny && (gy < c->low[1] || gy >= ny - c->high[1]))
+          yrows++;
+      const double f = (1.0 + 0.4 * xe) * (1.0 + 0.8 * yrows / quad::WARPS);
+      const int kbeg = r * c->zchunk, kend = std::min(kbeg + c->zchunk, nz);
+      double w = 0.0;
+      for (int k = kbeg; k < kend; k++) w += zslab(k) ? 1.8 : 1.0;
+      if (kbeg > 0) w += 0.6 * (zslab(kbeg - 1) ? 1.8 : 1.0);
+      cost.push_back({-w * f, r * tiles + t});
+    }
+  std::stable_sort(cost.begin(), cost.end(),
+                   [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+                     return a.first < b.first;
+                   });
+  std::vector<int> order(cost.size());
+  for (size_t i = 0; i < cost.size(); i++) order[i] = cost[i].second;
+  return order;
 }
 
 // Empty source tables: every bucket empty.
@@ -2584,6 +2626,11 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   chunks = std::min(chunks, c->n[2]);
   c->zchunk = (c->n[2] + chunks - 1) / chunks;
   c->zchunks = (c->n[2] + c->zchunk - 1) / c->zchunk;
+  if (c->quad) {
+    const std::vector<int> order = quad_order(c);
+    if (int r = alloc(c, (void **)&c->order, order.size() * 4)) return r;
+    CUDA_TRY(c, copy(c, c->order, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+  }
   if (int r = empty_sources(c)) return r;
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   return 0;
