@@ -68,6 +68,9 @@ struct MediaArgs {
   long long members;
 };
 
+// The quad kernel's runs of z-planes, at most this many (their starts travel with the launch).
+constexpr int quad_max_runs = 64;
+
 template <typename T>
 struct StepArgs {
   int n[3];
@@ -102,6 +105,7 @@ struct StepArgs {
   const double *waves_e;  // at E's time
   int tiles_x, tiles_y, zchunk;
   const int *order;  // quad kernel: CTA b takes run order[b] / tiles, tile order[b] % tiles
+  int runs[quad_max_runs + 1];  // quad kernel: run r is planes runs[r] .. runs[r+1]-1
   MediaArgs<T> media;
 };
 
@@ -1404,7 +1408,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const int cta = A.order[blockIdx.x];  // heaviest first (quad_order)
   const int tile = cta % ntiles;
   const int x0 = (tile % A.tiles_x) * OWNX, y0 = (tile / A.tiles_x) * RW;
-  const int kbeg = (cta / ntiles) * A.zchunk, kend = min(kbeg + A.zchunk, nz);
+  const int kbeg = A.runs[cta / ntiles], kend = A.runs[cta / ntiles + 1];
   if (kbeg >= nz) return;
   const long long plane = (long long)nx * ny;
   T *sXC = sX + S::X;                                // quad::Smem::XC
@@ -1484,6 +1488,9 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     else if (my >= ny - A.high[1]) sy = 1;
   }
   const long long rowoff = my >= 0 ? (long long)my * nx : 0;
+  // whether the tile has currents in any plane (most have none: then no plane looks them up)
+  const bool hcur = A.hbucket[(long long)tile * nz] != A.hbucket[(long long)tile * nz + nz];
+  const bool ecur = A.ebucket[(long long)tile * nz] != A.ebucket[(long long)tile * nz + nz];
 
   // -- copies: warp w copies E's row w (and the last warp also row RW+1), H's row w and cb's row
   // w-1 of a plane; lane l the chunks of its four places (lane 0 also the chunk after the row)
@@ -1611,7 +1618,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       if (!hv[j]) hn[0][j] = hn[1][j] = hn[2][j] = T(0);
     // the magnetic currents at this tile and plane, each value's entries in CPU order
     const int bucket = tile * nz + k;
-    const int g0 = A.hbucket[bucket], g1 = A.hbucket[bucket + 1];
+    const int g0 = hcur ? A.hbucket[bucket] : 0, g1 = hcur ? A.hbucket[bucket + 1] : 0;
     for (int g = g0; g < g1; g++) {
       Group gr = A.hgroups[g];
       const int gw = gr.local / ROW, gi = gr.local % ROW;
@@ -1744,7 +1751,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       }
       // the electric currents (src/fdtd.rs:1375-1387)
       const int bucket = tile * nz + k;
-      const int g0 = A.ebucket[bucket], g1 = A.ebucket[bucket + 1];
+      const int g0 = ecur ? A.ebucket[bucket] : 0, g1 = ecur ? A.ebucket[bucket + 1] : 0;
       for (int g = g0; g < g1; g++) {
         Group gr = A.egroups[g];
         const int gw = gr.local / ROW, gi = gr.local % ROW;
@@ -1975,6 +1982,7 @@ struct fdtd_ctx {
   int *d_point = nullptr;
   int *hbucket = nullptr, *ebucket = nullptr;
   int *order = nullptr;  // the quad kernel's CTAs, heaviest first
+  int runs[quad_max_runs + 1] = {};  // the quad kernel's runs of planes (quad_runs)
   Group *hgroups = nullptr, *egroups = nullptr;
   Entry *entries = nullptr;
   double *waves_h = nullptr, *waves_e = nullptr;  // batch x nwaves x 2
@@ -2162,6 +2170,7 @@ StepArgs<T> step_args(fdtd_ctx *c) {
   A.tiles_y = c->tiles_y;
   A.zchunk = c->zchunk;
   A.order = c->order;
+  for (int r = 0; r <= c->zchunks && r <= quad_max_runs; r++) A.runs[r] = c->runs[r];
   if (sizeof(T) == 8) memcpy(&A.media, &c->md, sizeof A.media);
   else memcpy(&A.media, &c->mf, sizeof A.media);
   return A;
@@ -2300,6 +2309,41 @@ int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
   return 0;
 }
 
+// The quad kernel's runs of z-planes: `count` runs (at most quad_max_runs) that never straddle the
+// edge of a z CPML, the CPMLs' planes (heavier) in runs of their own, the rest of about equal
+// length. Returns the number of runs; starts in c->runs.
+int quad_runs(fdtd_ctx *c, int count) {
+  const int nz = c->n[2];
+  const int lo = c->periodic[2] ? 0 : std::min(c->low[2], nz);
+  const int hi = c->periodic[2] ? 0 : std::min(c->high[2], nz - lo);
+  const int mid = nz - lo - hi;
+  count = std::max(1, std::min(count, quad_max_runs));
+  const int slabs = (lo > 0) + (hi > 0);
+  // the interior's runs: what is left, at least one where it has planes
+  int inner = mid > 0 ? std::max(1, std::min(mid, count - slabs)) : 0;
+  // a CPML of more than 1.5 interior runs' planes is cut into runs of about that length
+  const int len = inner > 0 ? (mid + inner - 1) / inner : std::max(lo, hi);
+  auto pieces = [&](int planes) {
+    return planes > 0 ? std::max(1, (int)((planes + 1.5 * len - 1) / (1.5 * len))) : 0;
+  };
+  int plo = pieces(lo), phi = pieces(hi);
+  while (plo + inner + phi > quad_max_runs && inner > 1) inner--;
+  while (plo + inner + phi > quad_max_runs) {
+    if (plo >= phi && plo > 1) plo--;
+    else if (phi > 1) phi--;
+    else break;
+  }
+  int n = 0;
+  c->runs[0] = 0;
+  auto cut = [&](int from, int planes, int parts) {
+    for (int q = 1; q <= parts; q++) c->runs[++n] = from + (int)((long long)planes * q / parts);
+  };
+  cut(0, lo, plo);
+  cut(lo, mid, inner);
+  cut(lo + mid, hi, phi);
+  return n;
+}
+
 // The quad kernel's CTAs (run r, tile t as r * tiles + t) in launch order: by an estimate of
 // their time, heaviest first, so that the CTAs that start last are short and the step, which
 // ends with its last CTA, leaves few SMs idle at its end. A plane costs 1, 1.8 in a z CPML; a
@@ -2322,7 +2366,7 @@ std::vector<int> quad_order(const fdtd_ctx *c) {
         if (!c->periodic[1] && gy >= 0 && gy < ny && (gy < c->low[1] || gy >= ny - c->high[1]))
           yrows++;
       const double f = (1.0 + 0.4 * xe) * (1.0 + 0.8 * yrows / quad::WARPS);
-      const int kbeg = r * c->zchunk, kend = std::min(kbeg + c->zchunk, nz);
+      const int kbeg = c->runs[r], kend = c->runs[r + 1];
       double w = 0.0;
       for (int k = kbeg; k < kend; k++) w += zslab(k) ? 1.8 : 1.0;
       if (kbeg > 0) w += 0.6 * (zslab(kbeg - 1) ? 1.8 : 1.0);
@@ -2627,6 +2671,7 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   c->zchunk = (c->n[2] + chunks - 1) / chunks;
   c->zchunks = (c->n[2] + c->zchunk - 1) / c->zchunk;
   if (c->quad) {
+    c->zchunks = quad_runs(c, chunks);
     const std::vector<int> order = quad_order(c);
     if (int r = alloc(c, (void **)&c->order, order.size() * 4)) return r;
     CUDA_TRY(c, copy(c, c->order, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
