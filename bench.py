@@ -187,9 +187,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--edges", default="cpml", choices=["cpml", "walls", "periodic"],
+    ap.add_argument("--edges", default="cpml",
+                    choices=["cpml", "walls", "periodic", "cpml-x", "cpml-y", "cpml-z"],
                     help="the MMI grid's edges: cpml (the configuration) or, to compare the "
-                         "step's cost without CPMLs, walls or periodic sides")
+                         "step's cost without CPMLs, walls or periodic sides, or the CPMLs of "
+                         "one axis only (walls elsewhere)")
     ap.add_argument("--workload", default="mmi", choices=sorted(["mmi"] + list(WORKLOADS)),
                     help="mmi: the 3D MMI step (this benchmark's line); the others measure the "
                          "remaining configurations, one JSON line each")

@@ -22,7 +22,7 @@ import math
 import numpy as np
 
 from .types import (INF, Axis, Boundaries, Boxes, Cpml, Current, Dispersive, Field, FluxPlane,
-                    Grid3d, Periodic, Pole, Source, Waveform)
+                    Grid3d, Periodic, Pml, Pole, Source, Waveform)
 
 N_SI = 3.48
 N_SIO2 = 1.444
@@ -67,11 +67,14 @@ def mmi_geometry() -> Boxes:
 def mmi_3d(cls, precision: int = 32, steps: int = 20000, frequencies: int = 51,
            edges: str = "cpml", **kw):
     """Configuration 2: returns (simulation, info). ``edges`` "walls" or "periodic" replaces the
-    CPMLs (for comparing the step's cost without them; not the configuration)."""
+    CPMLs, and "cpml-x", "cpml-y" or "cpml-z" keeps those of one axis only, walls elsewhere (for
+    comparing the step's cost without them; not the configuration)."""
     h = 0.02
     g = Grid3d(600, 200, 100, h, h, h, -6.0, -2.0, -1.0)
+    one = {f"cpml-{a}": Boundaries(*[Pml(10, 10) if a == b else Pml(0, 0) for b in "xyz"], Cpml())
+           for a in "xyz"}
     b = {"cpml": Boundaries.with_cpml(10), "walls": Boundaries.walls(),
-         "periodic": Boundaries(Periodic(), Periodic(), Periodic(), Cpml())}[edges]
+         "periodic": Boundaries(Periodic(), Periodic(), Periodic(), Cpml()), **one}[edges]
     # Courant 0.9: the reference job's default (src/job/fdtd.rs:523)
     s = cls(g, mmi_geometry(), b, 0.9, precision=precision, **kw)
     # a Gaussian-profile E_y current across the input guide, 0.5 um in from the CPML
