@@ -192,6 +192,9 @@ def main():
                     help="the MMI grid's edges: cpml (the configuration) or, to compare the "
                          "step's cost without CPMLs, walls or periodic sides, or the CPMLs of "
                          "one axis only (walls elsewhere)")
+    ap.add_argument("--batch-steps", type=int, default=6000,
+                    help="the batch workload's steps (6000: the configuration; fewer for a "
+                         "profiler's small case)")
     ap.add_argument("--workload", default="mmi", choices=sorted(["mmi"] + list(WORKLOADS)),
                     help="mmi: the 3D MMI step (this benchmark's line); the others measure the "
                          "remaining configurations, one JSON line each")
@@ -452,7 +455,7 @@ def workload_batch(args):
     100x100 design regions, 6000 steps, batched (one persistent launch per step for all, CUDA-
     graph chunks, tile shape by timing) against the same instances run one at a time."""
     from photonoxide_b200.batch import Batch
-    steps = 6000
+    steps = args.batch_steps
     sims = _te_instances(64)
     cells = sum(s.grid.cells() for s in sims)
     B = Batch(sims)

@@ -110,9 +110,11 @@ __device__ __forceinline__ T slab_e(const TeInst<T> &I, const SlabEntry &s, int 
 
 template <typename T, int TW, int TH>
 __global__ void __launch_bounds__(THREADS) te_step_kernel(
-    const TeInst<T> *insts, const int *tile_inst, int ntiles, const int *hbucket,
-    const int *ebucket, const Group *hgroups, const Group *egroups, const Entry *entries,
-    const double *waves_h, const double *waves_e, int m) {
+    const TeInst<T> *__restrict__ insts, const int *__restrict__ tile_inst, int ntiles,
+    const int *__restrict__ hbucket, const int *__restrict__ ebucket,
+    const Group *__restrict__ hgroups, const Group *__restrict__ egroups,
+    const Entry *__restrict__ entries, const double *__restrict__ waves_h,
+    const double *__restrict__ waves_e, int m) {
   constexpr int HW = TW + 1, HH = TH + 1;
   __shared__ T sh[HW * HH];  // the new H_z over the tile and the row and column below it
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
