@@ -459,7 +459,7 @@ def workload_batch(args):
     sims = _te_instances(64)
     cells = sum(s.grid.cells() for s in sims)
     B = Batch(sims)
-    B.run(416)  # the tile shape's trial chunks
+    B.run(480)  # the tile shape's trial chunks
     _, tb = _timed(lambda: B.run(steps))
     alone = _te_instances(64)
     for s in alone:

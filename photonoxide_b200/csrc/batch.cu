@@ -251,6 +251,252 @@ __global__ void __launch_bounds__(THREADS) te_step_kernel(
   }
 }
 
+// The same step with a warp per tile row and four places per lane: a tile owns 124 x 7 places;
+// warp w holds row y0-1+w (warp 0 the row below the tile, for E's back differences), lane l the
+// places x0-4+4l .. x0-1+4l (lane 0 the column before the tile), read and written 16 bytes at a
+// time where a grid's rows are (nx a multiple of 4), one value at a time otherwise. H_z goes
+// through shared memory, where the magnetic sources are added and E reads its neighbours. Each
+// value's arithmetic is te_step_kernel's; the lane's index arithmetic serves four values.
+namespace teq {
+constexpr int VEC = 4, ROW = 128, OWN = 124, RW = 7, WARPS = RW + 1;
+static_assert(WARPS * 32 == THREADS, "a warp per row");
+}  // namespace teq
+
+template <typename T>
+struct V4 {
+  T v[4];
+};
+template <typename T>
+__device__ __forceinline__ V4<T> ldv(const T *p) {
+  V4<T> r;
+  if (sizeof(T) == 4) {
+    const float4 f = *reinterpret_cast<const float4 *>(p);
+    r.v[0] = (T)f.x, r.v[1] = (T)f.y, r.v[2] = (T)f.z, r.v[3] = (T)f.w;
+  } else {
+    const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+    r.v[0] = (T)a.x, r.v[1] = (T)a.y, r.v[2] = (T)b.x, r.v[3] = (T)b.y;
+  }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stv(T *p, const T v[4]) {
+  if (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+  } else {
+    *reinterpret_cast<double2 *>(p) = make_double2((double)v[0], (double)v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2((double)v[2], (double)v[3]);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS) te_quad_kernel(
+    const TeInst<T> *__restrict__ insts, const int *__restrict__ tile_inst, int ntiles,
+    const int *__restrict__ hbucket, const int *__restrict__ ebucket,
+    const Group *__restrict__ hgroups, const Group *__restrict__ egroups,
+    const Entry *__restrict__ entries, const double *__restrict__ waves_h,
+    const double *__restrict__ waves_e, int m) {
+  using namespace teq;
+  __shared__ __align__(16) T sh[WARPS * ROW];  // the new H_z of the rows y0-1 .. y0+RW-1
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int ii = tile_inst[t];
+    const TeInst<T> &I = insts[ii];
+    const int lt = t - I.tile0;
+    const int x0 = (lt % I.tiles_x) * OWN, y0 = (lt / I.tiles_x) * RW;
+    const int nx = I.nx, ny = I.ny;
+    const long long N = I.N;
+    const int cur = (I.parity + m) & 1;
+    const T *ein = I.e[cur];
+    T *eout = I.e[1 - cur];
+    const T *hin = I.h[cur];
+    T *hout = I.h[1 - cur];
+    const T *pin = I.psi_h[cur];
+    T *pout = I.psi_h[1 - cur];
+    const bool vec = (nx & 3) == 0;  // then a lane's four places are all in the grid or none
+    const int xb = x0 - VEC + VEC * lane;
+    const int y = y0 - 1 + w;
+    const int my = y < ny ? wrap_index(y, ny, I.py) : -1;  // beyond the grid's end: H is zero
+    int mx[4];
+    bool ok[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int x = xb + j;
+      mx[j] = x < 0 ? (I.px ? x + nx : -1) : (x < nx ? x : -1);
+      ok[j] = mx[j] >= 0 && my >= 0;
+    }
+    const bool live = ok[0] | ok[1] | ok[2] | ok[3];
+    const bool own = w >= 1 && lane >= 1;
+    // the four places' values of a row (zero where a place is not in the grid)
+    auto get = [&](const T *row) {
+      V4<T> o;
+      if (vec && ok[0]) {
+        o = ldv(row + mx[0]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) o.v[j] = ok[j] ? row[mx[j]] : T(0);
+      }
+      return o;
+    };
+    const long long rrow = (long long)(my < 0 ? 0 : my) * nx;
+    // -- H_z (src/fdtd/kernel/reference.rs:14-56 with E_z, H_x, H_y zero)
+    const V4<T> ex = get(ein + rrow), ey = get(ein + N + rrow);
+    const T eynext = __shfl_down_sync(0xffffffffu, ey.v[0], 1);
+    T hz[4] = {T(0), T(0), T(0), T(0)};
+    T dxEy[4], dyEx[4];
+    if (live) {
+      const int myp = wrap_index(my + 1, ny, I.py);
+      V4<T> exn;
+      if (myp >= 0) {
+        exn = get(ein + (long long)myp * nx);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) exn.v[j] = T(0);
+      }
+      const V4<T> ho = get(hin + 2 * N + rrow), fhx = get(I.fh);
+      const T fhy = I.fh[nx + my];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        // E_y at mx + 1: the next place's (the next lane's first for the fourth, read by the
+        // row's last lane), x = 0's on a periodic x past the end, else zero
+        T eyj;
+        if (mx[j] + 1 >= nx) eyj = I.px ? ein[N + rrow] : T(0);
+        else if (j < 3) eyj = ey.v[j + 1];
+        else eyj = lane < 31 ? eynext : ein[N + rrow + mx[j] + 1];
+        dxEy[j] = eyj - ey.v[j];
+        dyEx[j] = exn.v[j] - ex.v[j];
+        hz[j] = ho.v[j] - I.dt * (dxEy[j] * fhx.v[j] - dyEx[j] * fhy);
+      }
+      // the CPML: H_z along x (+), then along y (-)
+      if (!I.px) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (!ok[j]) continue;
+          const SlabEntry &s = I.hx[mx[j] < nx / 2 ? 0 : 1];
+          if (in_slab(s, mx[j]))
+            hz[j] = slab_h(I, s, mx[j], s.psi + (long long)my * s.pw + (mx[j] - s.pf), pin, pout,
+                           own, dxEy[j], 0, T(1), hz[j]);
+        }
+      }
+      if (!I.py) {
+        const SlabEntry &s = I.hy[my < ny / 2 ? 0 : 1];
+        if (in_slab(s, my))
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (ok[j])
+              hz[j] = slab_h(I, s, my, s.psi + (long long)(my - s.from) * nx + mx[j], pin, pout,
+                             own, dyEx[j], 1, T(-1), hz[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (!ok[j]) hz[j] = T(0);
+    }
+    stv(sh + w * ROW + VEC * lane, hz);
+    const int b = I.bucket0 + lt;
+    const int hg0 = hbucket[b], hg1 = hbucket[b + 1];
+    if (hg1 > hg0) {
+      __syncthreads();
+      // the magnetic sources (src/fdtd.rs:1348-1359), each value's entries in CPU order
+      for (int g = hg0 + threadIdx.x; g < hg1; g += THREADS) {
+        const Group gr = hgroups[g];
+        T v = sh[gr.local];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          const Entry en = entries[q];
+          const double *wv = waves_h + 2 * (long long)en.emitter;
+          const double amount = en.are * wv[0] - en.aim * wv[1];
+          if (sizeof(T) == 8) v = v - (T)(I.dt64 * amount);
+          else v = v - I.dt * (T)amount;
+        }
+        sh[gr.local] = v;
+      }
+    }
+    __syncthreads();
+    // -- E_x, E_y at the owned places (reference.rs:58-99): back differences of the new H_z
+    if (own && live) {
+      const V4<T> h = ldv(sh + w * ROW + VEC * lane), hu = ldv(sh + (w - 1) * ROW + VEC * lane);
+      const T hl = sh[w * ROW + VEC * lane - 1];
+      const V4<T> fex = get(I.fe), cbx = get(I.cb + rrow), cby = get(I.cb + N + rrow);
+      const T fey = I.fe[nx + my];
+      V4<T> cax, cay;
+      if (I.ca) {
+        cax = get(I.ca + rrow);
+        cay = get(I.ca + N + rrow);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          cax.v[j] = cbx.v[j] == T(0) ? T(0) : T(1);
+          cay.v[j] = cby.v[j] == T(0) ? T(0) : T(1);
+        }
+      }
+      T nex[4], ney[4], dyHz[4], dxHz[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        dyHz[j] = h.v[j] - hu.v[j];
+        dxHz[j] = h.v[j] - (j > 0 ? h.v[j - 1] : hl);
+        // curl_x = dyHz fey - dzHy fez and curl_y = dzHx fez - dxHz fex, with dzHy = dzHx = +0
+        const T curl0 = dyHz[j] * fey;
+        const T curl1 = T(0) - dxHz[j] * fex.v[j];
+        nex[j] = cax.v[j] * ex.v[j] + cbx.v[j] * curl0;
+        ney[j] = cay.v[j] * ey.v[j] + cby.v[j] * curl1;
+      }
+      // the CPML: E_x along y (+), E_y along x (-)
+      if (!I.py) {
+        const SlabEntry &s = I.ey[my < ny / 2 ? 0 : 1];
+        if (in_slab(s, my))
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (ok[j])
+              nex[j] = slab_e(I, s, my, s.psi + (long long)(my - s.from) * nx + mx[j], I.psi_e,
+                              dyHz[j], 1, T(1), cbx.v[j], nex[j]);
+      }
+      if (!I.px) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (!ok[j]) continue;
+          const SlabEntry &s = I.ex[mx[j] < nx / 2 ? 0 : 1];
+          if (in_slab(s, mx[j]))
+            ney[j] = slab_e(I, s, mx[j], s.psi + (long long)my * s.pw + (mx[j] - s.pf), I.psi_e,
+                            dxHz[j], 0, T(-1), cby.v[j], ney[j]);
+        }
+      }
+      if (vec) {
+        stv(hout + 2 * N + rrow + mx[0], h.v);
+        stv(eout + rrow + mx[0], nex);
+        stv(eout + N + rrow + mx[0], ney);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (ok[j]) {
+            hout[2 * N + rrow + mx[j]] = h.v[j];
+            eout[rrow + mx[j]] = nex[j];
+            eout[N + rrow + mx[j]] = ney[j];
+          }
+      }
+    }
+    const int eg0 = ebucket[b], eg1 = ebucket[b + 1];
+    if (eg1 > eg0) {
+      __syncthreads();  // this CTA's E values are in memory
+      // the electric currents (src/fdtd.rs:1375-1387): local = the place in the tile, x fastest
+      for (int g = eg0 + threadIdx.x; g < eg1; g += THREADS) {
+        const Group gr = egroups[g];
+        const int lq = gr.local;
+        const int x = x0 + lq % OWN, yy = y0 + lq / OWN;
+        const long long at = (long long)gr.comp * N + (long long)yy * nx + x;
+        T v = eout[at];
+        const T cbv = I.cb[at];
+        for (int q = gr.first; q < gr.first + gr.count; q++) {
+          const Entry en = entries[q];
+          const double *wv = waves_e + 2 * (long long)en.emitter;
+          const double amount = en.are * wv[0] - en.aim * wv[1];
+          if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
+          else v = v - cbv * (T)amount;
+        }
+        eout[at] = v;
+      }
+    }
+    __syncthreads();  // sh is reused by the next tile
+  }
+}
+
 // The chunk's waveforms: per (instance, emitter, step m) at H's time (first+m) dt and E's
 // (first+m+1/2) dt (waves_kernel in engine.cu). Emitter numbers in `entries` are batch-wide:
 // wave0 + the instance's own; the tables are [m][emitter].
@@ -617,7 +863,10 @@ __global__ void te_grad_kernel(const long long *design, long long n, const T *K,
 struct Shape {
   int tw, th;
 };
-const Shape SHAPES[] = {{32, 8}, {32, 16}, {64, 4}, {64, 8}, {128, 2}, {128, 4}};
+// the last: te_quad_kernel's rows
+const Shape SHAPES[] = {{32, 8}, {32, 16}, {64, 4}, {64, 8}, {128, 2}, {128, 4},
+                        {teq::OWN, teq::RW}};
+constexpr int QUAD_SHAPE = 6;
 constexpr int NSHAPES = sizeof(SHAPES) / sizeof(SHAPES[0]);
 constexpr int DEFAULT_SHAPE = 3;  // 64 x 8
 
@@ -861,16 +1110,19 @@ int build(fdtd_batch *b, const std::vector<InstanceView> &views, const std::vect
           continue;
         }
         // (tile, position in its H region) along each axis: its own tile, and the tile whose
-        // column (row) below it is, also across a periodic wrap
-        auto options = [](int c, int n, int w, int periodic) {
-          std::vector<std::pair<int, int>> o{{c / w, c - (c / w) * w + 1}};
-          if (c + 1 < n && (c + 1) % w == 0) o.push_back({(c + 1) / w, 0});
-          if (periodic && c == n - 1) o.push_back({0, 0});
+        // column (row) below it is, also across a periodic wrap. The region starts `off` places
+        // before the tile: one row; one column, or te_quad_kernel's first lane's four places
+        auto options = [](int c, int n, int w, int periodic, int off) {
+          std::vector<std::pair<int, int>> o{{c / w, c - (c / w) * w + off}};
+          if (c + 1 < n && (c + 1) % w == 0) o.push_back({(c + 1) / w, off - 1});
+          if (periodic && c == n - 1) o.push_back({0, off - 1});
           return o;
         };
-        for (auto oy : options(y, I.ny, TH, I.py))
-          for (auto ox : options(x, I.nx, TW, I.px))
-            add(hper[oy.first * I.tiles_x + ox.first], oy.second * (TW + 1) + ox.second);
+        const bool rows = sh == QUAD_SHAPE;
+        const int xoff = rows ? teq::VEC : 1, hrow = rows ? teq::ROW : TW + 1;
+        for (auto oy : options(y, I.ny, TH, I.py, 1))
+          for (auto ox : options(x, I.nx, TW, I.px, xoff))
+            add(hper[oy.first * I.tiles_x + ox.first], oy.second * hrow + ox.second);
       }
     }
     for (int t = 0; t < ntile; t++) {
@@ -944,7 +1196,13 @@ void step_by_shape(fdtd_batch *b, int m) {
     case 2: launch_step<T, 64, 4>(b, m); break;
     case 3: launch_step<T, 64, 8>(b, m); break;
     case 4: launch_step<T, 128, 2>(b, m); break;
-    default: launch_step<T, 128, 4>(b, m); break;
+    case 5: launch_step<T, 128, 4>(b, m); break;
+    default:
+      te_quad_kernel<T><<<b->blocks, THREADS, 0, b->stream>>>(
+          (const TeInst<T> *)b->d_insts, b->d_tile_inst, b->ntiles, b->d_hbucket, b->d_ebucket,
+          b->d_hgroups, b->d_egroups, b->d_entries,
+          b->d_waves_h + 2LL * m * b->nwaves_total, b->d_waves_e + 2LL * m * b->nwaves_total, m);
+      break;
   }
 }
 
@@ -957,7 +1215,8 @@ int occupancy(fdtd_batch *b) {
     case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 64, 4>, THREADS, 0); break;
     case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 64, 8>, THREADS, 0); break;
     case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 128, 2>, THREADS, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 128, 4>, THREADS, 0); break;
+    case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_step_kernel<T, 128, 4>, THREADS, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, te_quad_kernel<T>, THREADS, 0); break;
   }
   return std::max(per, 1);
 }
