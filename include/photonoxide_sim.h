@@ -95,7 +95,8 @@ int64_t pxs_probe(pxs_sim *s, int32_t n, double *out);
 int64_t pxs_transforms(pxs_sim *s, double *out);
 /* Simulation::flux (src/fdtd/monitors.rs:539-552): returns the frequencies' count */
 int pxs_flux(pxs_sim *s, int32_t n, double *out);
-/* the setup tables, as orc_tables: 0 ca, 1 cb, 2 kappa/h nodes, 3 halves, 4 slabs */
+/* the setup tables, as orc_tables: 0 ca, 1 cb, 2 kappa/h nodes, 3 halves, 4 slabs, 5 media
+ * groups (per group chi, npoles, 3 per pole, count, then comp, index, scale per member) */
 int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out);
 /* The device engine under it (created at the first run), or NULL. */
 struct fdtd_ctx *pxs_engine(pxs_sim *s);

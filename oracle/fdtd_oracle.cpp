@@ -1251,6 +1251,19 @@ long orc_tables(const orc_sim *s, int which, double *out) {
         for (double v : sl.b) put(v);
         for (double v : sl.a) put(v);
       }
+    } else if (which == 5) {  // the media groups: chi, poles, members (comp, index, scale)
+      for (const auto &gr : x.groups) {
+        put((double)gr.chi);
+        put((double)gr.poles.size());
+        for (const auto &p : gr.poles)
+          for (int q = 0; q < 3; q++) put((double)p[q]);
+        put((double)gr.values.size());
+        for (size_t v = 0; v < gr.values.size(); v++) {
+          put(gr.values[v].first);
+          put((double)gr.values[v].second);
+          put((double)gr.scale[v]);
+        }
+      }
     }
     return at;
   });

@@ -75,7 +75,8 @@ long orc_probe(const orc_sim *s, int p, double *out);
 long orc_transforms(const orc_sim *s, double *out);
 int orc_flux(const orc_sim *s, int n, double *out);
 /* Setup tables for comparisons: which 0 ca, 1 cb (3 x cells), 2 kappa/h at nodes, 3 at halves
- * (nx+ny+nz), 4 slab table: per slab {field, comp, axis, from, count} then b[count], a[count].
+ * (nx+ny+nz), 4 slab table: per slab {field, comp, axis, from, count} then b[count], a[count],
+ * 5 media groups: per group {chi, npoles, 3 per pole, count} then {comp, index, scale} per member.
  * Returns the number of doubles (out may be NULL to ask). */
 long orc_tables(const orc_sim *s, int which, double *out);
 /* Stability of a medium (src/fdtd/media.rs:261-309): 1 stable, 0 not. */

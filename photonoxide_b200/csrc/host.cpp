@@ -16,6 +16,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "photonoxide_fdtd.h"
@@ -297,7 +298,7 @@ struct pxs_sim {
   std::vector<int> dft_monitor;  // add_dft's monitors, by number
   std::vector<std::vector<FluxFace>> fluxes;
   std::vector<MediaGroup> groups;
-  std::map<std::pair<int, int64_t>, int> members;
+  std::unordered_map<int64_t, int> members;  // a dispersive value (comp * N + r): its group
   bool configured = false;  // sources, probes and transforms pushed to the engine
   bool fields_dropped = false;  // released without reading the fields back (a served job's)
   fdtd_ctx *ctx = nullptr;
@@ -944,7 +945,7 @@ int pxs_conductor(pxs_sim *s, int32_t comp, int64_t i, int64_t j, int64_t k) {
   int64_t r = s->index(i, j, k);
   s->ca[comp][r] = s->cb[comp][r] = 0.0;
   if (!s->e.empty()) s->e[comp * s->N() + r] = 0.0;
-  auto it = s->members.find({comp, r});
+  auto it = s->members.find(comp * s->N() + r);
   if (it != s->members.end()) {  // Media::remove (src/fdtd/media.rs:641-653)
     MediaGroup &G = s->groups[it->second];
     for (size_t v = 0; v < G.r.size(); v++)
@@ -996,72 +997,86 @@ int pxs_medium(pxs_sim *s, double eps_inf, int32_t npoles, const double *poles,
   double chi = gsum / (4.0 * dt);
   Geometry geo(geometry);
   int64_t N = s->N();
+  // which E values the medium takes (not those a wall or conductor has zeroed), all at once
+  std::vector<uint8_t> in((size_t)(3 * N), 0);
+#pragma omp parallel for schedule(dynamic, 65536)
+  for (int64_t q = 0; q < 3 * N; q++) {
+    const int c = (int)(q / N);
+    const int64_t r = q - c * N;
+    if (s->cb[c][r] == 0.0) continue;
+    if (inside) {
+      in[q] = inside[q] != 0;
+    } else {
+      double p[3];
+      s->g.e_position(c, r, p);
+      in[q] = geo.at(p) != 0.0;
+    }
+  }
+  auto old_chi_of = [&](int64_t q) {
+    auto it = s->members.find(q);
+    return it != s->members.end() ? s->groups[it->second].chi : 0.0;
+  };
   {
     double top = 0.0, largest = 0.0;
     for (int a = 0; a < 3; a++)
       if (s->varies[a]) top += 1.0 / (s->g.d[a] * s->g.d[a]);
     top *= 4.0;
-    for (int c = 0; c < 3; c++)
-      for (int64_t r = 0; r < N; r++) {
-        if (s->cb[c][r] == 0.0) continue;
-        bool in;
-        if (inside) in = inside[c * N + r] != 0;
-        else {
-          double p[3];
-          s->g.e_position(c, r, p);
-          in = geo.at(p) != 0.0;
-        }
-        if (!in) continue;
-        auto it = s->members.find({c, r});
-        double old_chi = it != s->members.end() ? s->groups[it->second].chi : 0.0;
-        largest = std::max(largest, (1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi);
-      }
+    for (int64_t q = 0; q < 3 * N; q++) {
+      if (!in[q]) continue;
+      const int c = (int)(q / N);
+      const int64_t r = q - c * N;
+      largest = std::max(largest, (1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi_of(q));
+    }
     for (double sg : {0.0, largest})
       if (!medium_stable(eps_inf, co, sg, dt, top))
         return s->fail(FDTD_E_INVALID,
                        "the medium isn't stable at the time step %g um/c (a term's w0 dt above 2, "
                        "or a Courant number above sqrt(eps_inf)): take a smaller step", dt);
   }
+  // each value taken leaves the group it was in (Media::remove), in value order
   MediaGroup G;
   G.chi = chi;
   G.poles = co;
-  for (int c = 0; c < 3; c++)
-    for (int64_t r = 0; r < N; r++) {
-      if (s->cb[c][r] == 0.0) continue;
-      bool in;
-      if (inside) in = inside[c * N + r] != 0;
-      else {
-        double p[3];
-        s->g.e_position(c, r, p);
-        in = geo.at(p) != 0.0;
-      }
-      if (!in) continue;
-      double old_chi = 0.0;
-      auto it = s->members.find({c, r});
-      if (it != s->members.end()) old_chi = s->groups[it->second].chi;
-      double sg = std::max((1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi, 0.0);
-      if (it != s->members.end()) {
-        MediaGroup &O = s->groups[it->second];
-        for (size_t v = 0; v < O.r.size(); v++)
-          if (O.comp[v] == c && O.r[v] == r) {
-            O.comp.erase(O.comp.begin() + v);
-            O.r.erase(O.r.begin() + v);
-            O.scale.erase(O.scale.begin() + v);
-            break;
-          }
-        s->members.erase(it);
-      }
-      double nu = 1.0 + dt / eps_inf * (sg / 2.0 + chi);
-      s->ca[c][r] = (1.0 - dt * sg / (2.0 * eps_inf)) / nu;
-      s->cb[c][r] = dt / eps_inf / nu;
-      G.comp.push_back(c);
-      G.r.push_back(r);
-      G.scale.push_back(s->cb[c][r]);
+  std::vector<char> left(s->groups.size(), 0);
+  for (int64_t q = 0; q < 3 * N; q++) {
+    if (!in[q]) continue;
+    const int c = (int)(q / N);
+    const int64_t r = q - c * N;
+    double old_chi = 0.0;
+    auto it = s->members.find(q);
+    if (it != s->members.end()) {
+      old_chi = s->groups[it->second].chi;
+      left[it->second] = 1;
+      s->members.erase(it);
     }
+    double sg = std::max((1.0 - s->ca[c][r]) / s->cb[c][r] - old_chi, 0.0);
+    double nu = 1.0 + dt / eps_inf * (sg / 2.0 + chi);
+    s->ca[c][r] = (1.0 - dt * sg / (2.0 * eps_inf)) / nu;
+    s->cb[c][r] = dt / eps_inf / nu;
+    G.comp.push_back(c);
+    G.r.push_back(r);
+    G.scale.push_back(s->cb[c][r]);
+  }
+  // the groups values left keep the rest, in their order
+  for (size_t g = 0; g < left.size(); g++) {
+    if (!left[g]) continue;
+    MediaGroup &O = s->groups[g];
+    size_t k = 0;
+    for (size_t v = 0; v < O.r.size(); v++) {
+      if (in[O.comp[v] * N + O.r[v]]) continue;
+      O.comp[k] = O.comp[v];
+      O.r[k] = O.r[v];
+      O.scale[k] = O.scale[v];
+      k++;
+    }
+    O.comp.resize(k);
+    O.r.resize(k);
+    O.scale.resize(k);
+  }
   if (npoles > 0 && !G.r.empty()) {
     int gi = (int)s->groups.size();
-    (void)0;
-    for (size_t v = 0; v < G.r.size(); v++) s->members[{G.comp[v], G.r[v]}] = gi;
+    s->members.reserve(s->members.size() + G.r.size());
+    for (size_t v = 0; v < G.r.size(); v++) s->members[G.comp[v] * N + G.r[v]] = gi;
     s->groups.push_back(G);
   }
   return 0;
@@ -1436,6 +1451,18 @@ int64_t pxs_tables(const pxs_sim *s, int32_t which, double *out) {
       put((double)sl.count);
       for (double v : sl.b) put(v);
       for (double v : sl.a) put(v);
+    }
+  } else if (which == 5) {  // the media groups: chi, poles, members (comp, index, scale)
+    for (const MediaGroup &G : s->groups) {
+      put(G.chi);
+      put((double)(G.poles.size() / 3));
+      for (double v : G.poles) put(v);
+      put((double)G.r.size());
+      for (size_t v = 0; v < G.r.size(); v++) {
+        put(G.comp[v]);
+        put((double)G.r[v]);
+        put(G.scale[v]);
+      }
     }
   }
   return at;

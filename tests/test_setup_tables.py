@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 
 from photonoxide_b200.fdtd import Simulation, average
-from photonoxide_b200.types import INF, Boundaries, Boxes, Cpml, Grid3d, Pml, Periodic
+from photonoxide_b200.types import (INF, Axis, Boundaries, Boxes, Cpml, Dispersive, Grid3d, Pml,
+                                    Periodic, Pole)
 from pyoracle import OracleSimulation, average_boxes
 from scenarios import busy, closed, stirred
 
@@ -65,3 +66,35 @@ def test_refusals_as_the_reference():
         s.add_probe(0, 0, (10, 0, 0))
     with pytest.raises(InvalidValue):
         s.add_dft((0, 0, 0), (3, 3, 3), [1.0 / s.dt])  # beyond Nyquist
+
+
+def overlapping_media(make):
+    """Seeded random Drude and two-pole Lorentz boxes that overlap one another and a conductivity
+    region, a conductor, and a medium given by a mask: every value a later medium takes leaves the
+    group it was in (src/fdtd/media.rs:641-653, 749-825)."""
+    rng = np.random.default_rng(3)
+    g = Grid3d.centred((40, 34, 22), 0.02)
+    s = make(g, Boxes(1.0).add((-0.1, -0.1, -INF), (0.12, 0.08, INF), 2.5), Boundaries.with_cpml(4),
+             0.5)
+    s.with_conductivity(Boxes(0.0).add((0.0, -INF, -INF), (INF, 0.05, INF), 0.7))
+    drude, lorentz = Boxes(0.0), Boxes(0.0)
+    for q in range(14):
+        lo = rng.uniform(-0.4, 0.2, 3) * np.array([1.0, 1.0, 0.5])
+        hi = lo + rng.uniform(0.05, 0.3, 3)
+        (drude if q % 2 else lorentz).add(tuple(lo), tuple(hi), 1.0)
+    s.with_medium(Dispersive(1.0, [Pole.drude(7.27, 0.0531)]), drude)
+    s.with_medium(Dispersive(2.25, [Pole.lorentz(1.2, 0.7, 0.01), Pole.lorentz(0.6, 0.45, 0.02)]),
+                  lorentz)
+    mask = np.zeros((3, g.cells()), dtype=np.uint8)
+    mask[1, ::7] = 1
+    s.with_medium(Dispersive(1.5, [Pole.lorentz(0.8, 0.9, 0.03)]), mask)
+    s.conductor(Axis.Y, (20, 17, 11))
+    return s
+
+
+def test_media_tables_bitwise():
+    p = overlapping_media(lambda *a: Simulation(*a, precision=64))
+    o = overlapping_media(lambda *a: OracleSimulation(*a, precision=64))
+    for which in (0, 1, 5):
+        assert same(p.tables(which), o.tables(which)), which
+    assert len(p.tables(5)) > 1000
