@@ -1673,6 +1673,12 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     compute_h(se, se1, sh, k, true, hn);
     // H's tile to memory, H_x and H_z to the row below
     const long long at = (long long)k * plane + rowoff + (mxb < 0 ? 0 : mxb);
+    // the lossy form's ca of E's plane k, read now so that the barrier below covers the wait
+    Vec4<T> ca[3];
+    if (LOSSY && w >= 1 && any_own) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) ca[c] = ld4(A.ca + c * N + at);
+    }
     if (w >= 1 && lane >= 1 && rowh && mxb >= 0 && xb < nx) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
@@ -1699,12 +1705,11 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
     T en[3][4];
     if (w >= 1) {
-      Vec4<T> e[3], cb[3], ca[3], hxm, hzm;
+      Vec4<T> e[3], cb[3], hxm, hzm;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         e[c] = ld4(Erow(se, c, w) + VEC * lane);
         cb[c] = ld4(Brow(sh, c) + VEC * lane);
-        if (LOSSY && any_own) ca[c] = ld4(A.ca + c * N + at);
       }
       hxm = ld4(sX + (size_t)(w - 1) * ROW + VEC * lane);  // the row before
       hzm = ld4(sX + (size_t)(WARPS + w - 1) * ROW + VEC * lane);
