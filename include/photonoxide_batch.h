@@ -35,8 +35,9 @@ const char *fdtd_batch_last_error(const fdtd_batch *batch);
 int fdtd_batch_run(fdtd_batch *batch, int64_t steps, const int64_t *first_steps);
 /* The tile shape in use (0 x 0 before the first run chooses one). */
 int fdtd_batch_tile(const fdtd_batch *batch, int32_t *width, int32_t *height);
-/* Fixes the tile shape (one of 32x8, 32x16, 64x4, 64x8, 128x2, 128x4), or 0 x 0: choose by
- * timing on the next run. */
+/* Fixes the tile shape (one of 32x8, 32x16, 64x4, 64x8, 128x2, 128x4, or 124x7: a warp per row
+ * of 124 places, four a lane), or 0 x 0: choose by timing on the next run of at least 480
+ * steps (shorter first runs take 64x8). */
 int fdtd_batch_set_tile(fdtd_batch *batch, int32_t width, int32_t height);
 /* Kernel launches the batch has made (graph replays count their kernels). */
 int64_t fdtd_batch_launches(const fdtd_batch *batch);

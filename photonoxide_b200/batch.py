@@ -71,7 +71,8 @@ class Batch:
 
     def run(self, steps: int) -> "Batch":
         """``steps`` steps of every simulation. The first run of a batch without a fixed tile
-        shape times each shape on chunks of these steps and keeps the fastest."""
+        shape (32x8, 32x16, 64x4, 64x8, 128x2, 128x4 or the 124x7 rows) times each shape on
+        chunks of these steps and keeps the fastest, when it has at least 480 of them."""
         self._check(_lib().pxs_batch_run(self._h, int(steps)))
         return self
 
