@@ -36,6 +36,11 @@ typedef struct {
  * cells); only values whose cell crosses a box's face take the 8^3-sample average. */
 int pxs_average(const int64_t n[3], const double d[3], const double o[3], const pxs_geometry *g,
                 double *out);
+/* The same average on the current CUDA device, one thread per value (the same functions, so the
+ * same bits); `out` is host memory. The reference averages on the CPU, sequentially
+ * (src/fdtd.rs:583-594). Returns 0, -1 for bad sizes, -2 for a CUDA error. */
+int pxs_average_device(const int64_t n[3], const double d[3], const double o[3],
+                       const pxs_geometry *g, double *out);
 
 /* Simulation::new / with_permittivity (src/fdtd.rs:570-796): grid n, d, origin o; kind[a] 0 a
  * CPML of low/high cells (0 = wall), 1 periodic; cpml = {reflection, sigma (NaN: from

@@ -24,6 +24,7 @@
 #include "photonoxide_adjoint.h"
 #include "photonoxide_batch.h"
 #include "portable.h"
+#include "average.cuh"
 
 namespace {
 
@@ -56,80 +57,22 @@ struct Geometry {
     boxes.assign(g->boxes, g->boxes + 7 * (size_t)g->nboxes);
   }
   size_t count() const { return boxes.size() / 7; }
-  double at(const double p[3]) const {
-    double v = background;
-    for (size_t b = 0; b < count(); b++) {
-      const double *x = &boxes[7 * b];
-      if (x[0] < p[0] && p[0] < x[1] && x[2] < p[1] && p[1] < x[3] && x[4] < p[2] && p[2] < x[5])
-        v = x[6];
-    }
-    return v;
-  }
+  pxa::BoxView view() const { return pxa::BoxView{background, (int64_t)count(), boxes.data()}; }
+  double at(const double p[3]) const { return view().at(p); }
 };
 
-// The cell average of one value (src/fdfd/three.rs:563-588), in num-complex's arithmetic on a
-// zero imaginary part: 1/eps = eps/(eps eps), n/inverse = n inverse/(inverse inverse).
+// The cell average of one value (src/fdfd/three.rs:563-588): average.cuh, shared with the device.
 double average_cell(const Geometry &geo, const double centre[3], const double h[3], int along) {
-  const int samples = 8;
-  const double n = 8.0;
-  int a = along, b = first_of(along), c = second_of(along);
-  double sum = 0.0, p[3] = {centre[0], centre[1], centre[2]};
-  for (int sb = 0; sb < samples; sb++) {
-    p[b] = centre[b] + (((double)sb + 0.5) / n - 0.5) * h[b];
-    for (int sc = 0; sc < samples; sc++) {
-      p[c] = centre[c] + (((double)sc + 0.5) / n - 0.5) * h[c];
-      double inverse = 0.0;
-      for (int sa = 0; sa < samples; sa++) {
-        p[a] = centre[a] + (((double)sa + 0.5) / n - 0.5) * h[a];
-        double e = geo.at(p);
-        inverse += (1.0 * e) / (e * e);
-      }
-      sum += (n * inverse) / (inverse * inverse);
-    }
-  }
-  return sum / (n * n);
+  return pxa::average_cell(geo.view(), centre, h, along);
 }
 
-// The same average of a uniform value: what every cell away from the boxes' faces gives.
-double average_uniform(double e) {
-  const double n = 8.0;
-  double sum = 0.0;
-  for (int q = 0; q < 64; q++) {
-    double inverse = 0.0;
-    for (int s = 0; s < 8; s++) inverse += (1.0 * e) / (e * e);
-    sum += (n * inverse) / (inverse * inverse);
-  }
-  return sum / (n * n);
-}
+double average_uniform(double e) { return pxa::average_uniform(e); }
 
-// Whether every sample of the cell around `centre` sees the same boxes: along each axis the
-// samples run from centre + offset(0) h to centre + offset(7) h, and a box holds all of them or
-// none when, on some axis, both ends are outside on the same side, or on every axis both are in.
+// Whether every sample of the cell sees the same value, and which (average.cuh).
 bool uniform_cell(const Geometry &geo, const double centre[3], const double h[3], double *value) {
-  double lo[3], hi[3];
-  for (int a = 0; a < 3; a++) {
-    lo[a] = centre[a] + ((0.0 + 0.5) / 8.0 - 0.5) * h[a];
-    hi[a] = centre[a] + ((7.0 + 0.5) / 8.0 - 0.5) * h[a];
-  }
-  double v = geo.background;
-  for (size_t b = 0; b < geo.count(); b++) {
-    const double *x = &geo.boxes[7 * b];
-    bool none = false, all = true;
-    for (int a = 0; a < 3; a++) {
-      double blo = x[2 * a], bhi = x[2 * a + 1];
-      bool lo_in = blo < lo[a] && lo[a] < bhi, hi_in = blo < hi[a] && hi[a] < bhi;
-      if (!(lo_in && hi_in)) all = false;
-      if ((hi[a] <= blo) || (lo[a] >= bhi)) none = true;  // both ends on one side, outside
-      else if (!(lo_in && hi_in)) {
-        // the box's face crosses the samples along this axis: the samples differ unless another
-        // axis puts them all outside
-      }
-    }
-    if (none) continue;
-    if (!all) return false;
-    v = x[6];
-  }
-  *value = v;
+  const int64_t b = pxa::uniform_cell(geo.view(), centre, h);
+  if (b == -2) return false;
+  *value = b < 0 ? geo.background : geo.boxes[7 * b + 6];
   return true;
 }
 

@@ -111,15 +111,23 @@ def _geometry(g: Boxes):
     return arr, Geometry(float(g.background), len(g.boxes), arr.ctypes.data_as(DP))
 
 
-def average(grid: Grid3d, geometry: Boxes) -> np.ndarray:
+def average(grid: Grid3d, geometry: Boxes, device: bool = False) -> np.ndarray:
     """FDFD's cell average of a box geometry at each value of E, (3, cells): what
-    ``Simulation::new`` takes from ``eps(x, y, z)`` (``src/fdtd.rs:570-604``)."""
+    ``Simulation::new`` takes from ``eps(x, y, z)`` (``src/fdtd.rs:570-604``). ``device``: on
+    the current CUDA device, one thread per value (the same bits as on the host)."""
     n, d, o = grid.as_arrays()
     out = np.empty(3 * grid.cells())
     keep = [_i64(n), _d(d), _d(o)]
     arr, geo = _geometry(geometry)
-    library().pxs_average(keep[0][1], keep[1][1], keep[2][1], C.byref(geo),
-                          out.ctypes.data_as(DP))
+    x = library()
+    if device:
+        x.pxs_average_device.argtypes = [I64P, DP, DP, C.POINTER(Geometry), DP]
+        code = x.pxs_average_device(keep[0][1], keep[1][1], keep[2][1], C.byref(geo),
+                                    out.ctypes.data_as(DP))
+        if code != 0:
+            raise GpuError(f"the cell average on the device failed ({code})")
+    else:
+        x.pxs_average(keep[0][1], keep[1][1], keep[2][1], C.byref(geo), out.ctypes.data_as(DP))
     return out.reshape(3, -1)
 
 
