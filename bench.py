@@ -23,6 +23,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -61,7 +62,9 @@ class Clocks:
 
     def __init__(self, gpu_index: int):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # the samples' file: PHOTONOXIDE_CLOCKS_DIR, else the system's temporary directory
+        where = os.environ.get("PHOTONOXIDE_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(where, f"clocks_{os.getpid()}.csv")
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.out = open(self.path, "w")
