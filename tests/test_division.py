@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 @pytest.fixture(scope="module")
-def checker():
+def check_program():
     with tempfile.TemporaryDirectory() as d:
         exe = os.path.join(d, "check")
         subprocess.run(["g++", "-O2", "-std=c++17", "-mfma", "-ffp-contract=off",
@@ -23,7 +23,7 @@ def checker():
 
 
 @pytest.mark.parametrize("h", ["0.02", "0.05", "0.01", "0.04", "0.03", "0.013"])
-def test_product_form_gives_division_bits(checker, h):
-    bad, total = map(int, subprocess.run([checker, h, "251"], check=True, capture_output=True,
+def test_product_form_gives_division_bits(check_program, h):
+    bad, total = map(int, subprocess.run([check_program, h, "251"], check=True, capture_output=True,
                                          text=True).stdout.split())
     assert total > 100_000_000 and bad == 0, f"{bad} of {total} differ"
