@@ -256,7 +256,9 @@ __global__ void __launch_bounds__(THREADS) te_step_kernel(
 // places x0-4+4l .. x0-1+4l (lane 0 the column before the tile), read and written 16 bytes at a
 // time where a grid's rows are (nx a multiple of 4), one value at a time otherwise. H_z goes
 // through shared memory, where the magnetic sources are added and E reads its neighbours. Each
-// value's arithmetic is te_step_kernel's; the lane's index arithmetic serves four values.
+// value's arithmetic is te_step_kernel's; the lane's index arithmetic serves four values. Four
+// CTAs per SM (64 registers, a few spilled): with three, at 78 registers, it ran 50 Gcell/s
+// on 64 grids of widths a multiple of 4, with four 61 (the 32 x 16 tiles: 55).
 namespace teq {
 constexpr int VEC = 4, ROW = 128, OWN = 124, RW = 7, WARPS = RW + 1;
 static_assert(WARPS * 32 == THREADS, "a warp per row");
@@ -289,7 +291,7 @@ __device__ __forceinline__ void stv(T *p, const T v[4]) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(THREADS) te_quad_kernel(
+__global__ void __launch_bounds__(THREADS, 4) te_quad_kernel(
     const TeInst<T> *__restrict__ insts, const int *__restrict__ tile_inst, int ntiles,
     const int *__restrict__ hbucket, const int *__restrict__ ebucket,
     const Group *__restrict__ hgroups, const Group *__restrict__ egroups,
