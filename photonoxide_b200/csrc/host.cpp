@@ -1735,7 +1735,12 @@ struct pxs_server {
             batch = nullptr;
             te.clear();
           } else {
-            fdtd_batch_set_tile(batch, 32, 16);
+            // the row tiles where every grid's rows are 16-byte aligned (61 against 55
+            // Gcell-updates/s on such grids), else the 32 x 16 tiles
+            bool aligned = true;
+            for (ServerJob *j : te) aligned = aligned && j->sim->g.n[0] % 4 == 0;
+            if (aligned) fdtd_batch_set_tile(batch, 124, 7);
+            else fdtd_batch_set_tile(batch, 32, 16);
             batch_jobs = te;
           }
         }
