@@ -54,14 +54,56 @@ def ncu_traffic():
 
 
 class Clocks:
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """SM clocks and clock-event reasons sampled while the timed region runs: NVML polled every
+    2 ms from a thread (the timed regions here can be a few milliseconds, shorter than
+    nvidia-smi's sampling), else nvidia-smi every 200 ms. Read-only queries."""
 
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index: int):
         self.proc = None
+        self.thread = None
+        self.samples = []  # (sm MHz, max MHz, set of reasons)
+        try:
+            self._start_nvml(gpu_index)
+        except Exception:
+            self.thread = None
+            self._start_smi(gpu_index)
+
+    def _start_nvml(self, gpu_index):
+        import threading
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(gpu_index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            handle = nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            handle = nv.nvmlDeviceGetHandleByIndex(gpu_index)
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(handle, nv.NVML_CLOCK_SM))
+        self.stop_flag = threading.Event()
+
+        def poll():
+            while not self.stop_flag.is_set():
+                try:
+                    sm = float(nv.nvmlDeviceGetClockInfo(handle, nv.NVML_CLOCK_SM))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
+                except Exception:
+                    pass
+                self.stop_flag.wait(0.002)
+        self.thread = threading.Thread(target=poll, daemon=True)
+        self.thread.start()
+
+    def _start_smi(self, gpu_index):
         # the samples' file: PHOTONOXIDE_CLOCKS_DIR, else the system's temporary directory
         where = os.environ.get("PHOTONOXIDE_CLOCKS_DIR") or tempfile.gettempdir()
         self.path = os.path.join(where, f"clocks_{os.getpid()}.csv")
@@ -74,34 +116,41 @@ class Clocks:
         except Exception:
             self.proc = None
 
-    def stop(self):
-        if self.proc is None:
-            return None
+    def _read_smi(self):
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.out.close()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
                 if len(parts) < 9:
                     continue
                 try:
-                    sm.append(float(parts[1]))
-                    mx = max(mx, float(parts[2]))
+                    sm, mx = float(parts[1]), float(parts[2])
                 except ValueError:
                     continue
-                for name, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(name)
-        if not sm:
+                self.samples.append((sm, mx, {n for n, v in zip(self.NAMES, parts[5:9])
+                                              if v.lower().startswith("active")}))
+
+    def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            source = "nvml, every 2 ms"
+        elif self.proc is not None:
+            self._read_smi()
+            source = "nvidia-smi, every 200 ms"
+        else:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.samples:
+            return None
+        reasons = set().union(*(r for _, _, r in self.samples))
+        return {"sm_mhz": float(np.median([s for s, _, _ in self.samples])),
+                "sm_max_mhz": max(m for _, m, _ in self.samples), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": source}
 
 
 def aggregate(ms, steps, cells, dist=None, device="cpu"):
@@ -117,15 +166,25 @@ def aggregate(ms, steps, cells, dist=None, device="cpu"):
     return ms, world * steps * cells / (ms / 1e3) / 1e9
 
 
-def cpu_baseline(eps, target_seconds=15.0):
-    """The oracle (f64, all host threads) on the same MMI problem, timed over a bounded number
-    of steps (about 10-30 s of CPU work)."""
+WORKLOAD = ("3D MMI 600x200x100 (20 nm), CPML 10, Gaussian-profile current, 2 flux planes x 51 "
+            "wavelengths, f32 fields, f64 transforms")
+
+
+def config_of(cells: int, world: int) -> dict:
+    """The workload's description, the same on both arms."""
+    return {"workload": WORKLOAD, "cells": cells, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (fields+coefficients 432 MB)"}
+
+
+def _oracle_rate(eps, precision, target_seconds):
+    """The oracle's Gcell-updates/s on the MMI at `precision`, over about target_seconds of
+    steps (at most 200), and the steps and seconds it took."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from pyoracle import OracleSimulation
     from photonoxide_b200 import configs
 
-    def make(g, _geo, b, courant, precision=64):
-        return OracleSimulation(g, eps, b, courant, precision=64)
+    def make(g, _geo, b, courant, precision=precision):
+        return OracleSimulation(g, eps, b, courant, precision=precision)
 
     s, info = configs.mmi_3d(make)
     t0 = time.perf_counter()
@@ -135,11 +194,25 @@ def cpu_baseline(eps, target_seconds=15.0):
     t0 = time.perf_counter()
     s.run(n)
     dt = time.perf_counter() - t0
+    return n * info["cells"] / dt / 1e9, n, dt
+
+
+def cpu_baseline(eps, target_seconds=12.0):
+    """The oracle (photonoxide's CPU kernel restated, all host threads) on the same MMI problem,
+    timed over a bounded number of steps: f64 (the reference's default arithmetic, the value) and
+    f32 (its Yee<f32> kernel, the like-for-like arithmetic), with the host's STREAM triad."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from pyoracle import triad
+    v64, n64, s64 = _oracle_rate(eps, 64, target_seconds)
+    v32, n32, s32 = _oracle_rate(eps, 32, target_seconds)
+    bw = triad()
     cores = os.cpu_count() or 1
-    value = n * info["cells"] / dt / 1e9
-    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{n} steps of the full 600x200x100 MMI grid, f64, OpenMP on {cores} threads "
-                      f"({dt:.1f} s)"}
+    return {"value": v64, "unit": UNIT, "cores": cores, "kind": "port",
+            "f32": {"value": v32, "unit": UNIT, "steps": n32, "seconds": s32},
+            "triad_gbs": bw,
+            "sample": f"{n64} steps (f64, {s64:.1f} s) and {n32} steps (f32, {s32:.1f} s) of the "
+                      f"full 600x200x100 MMI grid, OpenMP on {cores} threads; STREAM triad "
+                      f"{bw:.0f} GB/s on the same threads"}
 
 
 def reference_arm(args):
@@ -159,8 +232,8 @@ def reference_arm(args):
 
     s, info = configs.mmi_3d(make)
     t0 = time.perf_counter()
-    s.run(max(1, min(args.warmup, 3)))
-    one = (time.perf_counter() - t0) / max(1, min(args.warmup, 3))
+    s.run(args.warmup)
+    one = (time.perf_counter() - t0) / args.warmup
     steps = max(1, min(args.steps, int(90.0 / max(one, 1e-3))))
     t0 = time.perf_counter()
     s.run(steps)
@@ -169,11 +242,10 @@ def reference_arm(args):
     cores = os.cpu_count() or 1
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": min(args.warmup, 3), "ms_per_step": dt / steps * 1e3,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "3D MMI 600x200x100 (20 nm), CPML 10, Gaussian-profile current, "
-                               "2 flux planes x 51 wavelengths", "cells": info["cells"]},
+        "config": config_of(info["cells"], int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{steps} steps of the full grid (the oracle: photonoxide's CPU "
                                    f"kernel restated in C++, f64, OpenMP on {cores} threads)"},
@@ -266,16 +338,21 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    wall0 = time.perf_counter()
+    # each call returns once its copies are done (the run once its steps are): the wall time
+    # between returns is the phase's
+    phases, marks = {}, [time.perf_counter()]
     e0.record(stream)
-    eng.upload_coeffs(None, cb)
-    eng.upload_fields(e_host, h_host)
-    eng.run_async(args.steps, 0)
-    eng.download_fields(e_host, h_host)
-    eng.read_dft(sums)
+    for name, call in (("upload_coeffs", lambda: eng.upload_coeffs(None, cb)),
+                       ("upload_fields", lambda: eng.upload_fields(e_host, h_host)),
+                       ("steps", lambda: (eng.run_async(args.steps, 0), eng.synchronize())),
+                       ("download_fields", lambda: eng.download_fields(e_host, h_host)),
+                       ("read_dft", lambda: eng.read_dft(sums))):
+        call()
+        marks.append(time.perf_counter())
+        phases[name] = marks[-1] - marks[-2]
     e1.record(stream)
     eng.synchronize()
-    wall = time.perf_counter() - wall0
+    wall = time.perf_counter() - marks[0]
     e2e_ms = max(e0.elapsed_time(e1), 0.0)
     e2e_ms, e2e_value = aggregate(e2e_ms, args.steps, cells, dist if world > 1 else None, "cuda")
     h2d = (3 * N + 6 * N) * 8 / args.steps
@@ -288,7 +365,7 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            base = cpu_baseline(np.asarray(configs_eps(sim)), 15.0)
+            base = cpu_baseline(np.asarray(configs_eps(sim)))
         except Exception as exc:  # the baseline is reported, not the target
             base = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                     "sample": f"failed: {exc}"}
@@ -301,16 +378,14 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "3D MMI 600x200x100 (20 nm), CPML 10, Gaussian-profile current, "
-                               "2 flux planes x 51 wavelengths, f32 fields, f64 transforms",
-                   "cells": cells, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (fields+coefficients 432 MB)"},
+        "config": config_of(cells, world),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_kind": peak_kind, "bytes_per_launch": bytes_step,
                      "kernel_ms_per_launch": per_launch_s * 1e3},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "wall_s": wall},
+                "d2h_bytes_per_step": d2h, "wall_s": wall,
+                "phases_s": phases},
         "gpu_launches": launches,
         "clocks": clk,
         "cpu_baseline": base,

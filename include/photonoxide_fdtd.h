@@ -4,8 +4,8 @@
  * This is the drop-in seam for photonoxide's GPU device: every entry point here replaces one
  * step of the reference's `gpu::Resident` (src/fdtd/gpu/resident.rs), which `Simulation` drives
  * through its `OnGpu` slot (src/fdtd.rs:528-535, run/step diverting at src/fdtd.rs:1142-1146,
- * 1319-1323). A Rust shim binds these as `extern "C"`; the Python package
- * and the C++ host library in this repository call them the same way.
+ * 1319-1323). A Rust shim binds these as `extern "C"`; the Python package and the C++ host
+ * library in this repository call them the same way.
  *
  * Conventions (the reference's): field 0 = E, 1 = H (H~ = eta0 H); component/axis 0, 1, 2 =
  * x, y, z; within a component the value (i, j, k) is at r = (k*ny + j)*nx + i
@@ -108,17 +108,23 @@ const char *fdtd_last_error(const fdtd_ctx *ctx);
 /* Resident::upload (resident.rs:378-399): E's coefficients. ca may be NULL for a medium with no
  * conductivity (ca 1 wherever cb isn't 0, and 0 where it is), which the step then never reads. */
 int fdtd_upload_coeffs(fdtd_ctx *ctx, const double *ca, const double *cb);
-/* The fields (3 x cells each) and each slab's psi (in slab order; NULL entries mean zero). */
+/* The fields (3 x cells each) and each slab's psi (in slab order; NULL entries mean zero).
+ * Host arrays that are page-locked and mapped (cudaHostAlloc'd or registered) are read by the
+ * device directly, converted to the context's precision as they cross; pageable ones go through
+ * a staging buffer the context allocates on its first such transfer (within its HBM budget) and
+ * keeps. The same holds for fdtd_upload_coeffs, fdtd_download_fields and fdtd_read_dft. Every
+ * one of these calls returns with its host arrays free for the caller to reuse. */
 int fdtd_upload_fields(fdtd_ctx *ctx, const double *e, const double *h, const double *const *psi);
 /* fdtd_upload_fields(ctx, e, h, NULL) without allocating any device memory, for callers that
  * can't allocate at that point: a serving loop that has handed out its whole HBM budget, an
  * application whose CUDA allocator is its own, code that must leave a stream-ordered memory pool
  * untouched. No counterpart in the reference (its uploads go through wgpu's staging buffers).
- * The f64 host values pass through a fixed 16 MiB device array of the library (2^21 values, held
- * by every GPU that loads it until exit), one field component at a time: a grid of more than
- * 2^21 cells is refused (FDTD_E_INVALID); use fdtd_upload_fields. psi restarts from zero. The
- * first call on a device looks the array up (call it before any stream capture); calls that
- * overlap on the GPU share the array and race. */
+ * An f32 context's f64 host values pass through a fixed 16 MiB device array of the library
+ * (2^21 values, held by every GPU that loads it until exit), one field component at a time, so
+ * an f32 grid of more than 2^21 cells is refused (FDTD_E_INVALID; use fdtd_upload_fields); an
+ * f64 context copies straight into its fields, any size. psi restarts from zero. The first f32
+ * call on a device looks the array up (call it before any stream capture); calls that overlap on
+ * the GPU share the array and race. */
 int fdtd_upload_fields_static(fdtd_ctx *ctx, const double *e, const double *h);
 
 /* Which axes' CPML differences are divided by the grid step through a reciprocal product with

@@ -5,6 +5,8 @@
 #include "fdtd_oracle.h"
 #include "refmath.h"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -1275,6 +1277,24 @@ int orc_medium_stable(double eps_inf, int npoles, const double *poles, double si
   for (int p = 0; p < npoles; p++)
     ps.push_back(Pole{(int)poles[4 * p], poles[4 * p + 1], poles[4 * p + 2], poles[4 * p + 3]});
   return stable(ps, eps_inf, sigma, dt, top) ? 1 : 0;
+}
+
+double orc_triad(long len, int repeats) {
+  // the STREAM triad as the reference measures its host's bandwidth (src/traffic.rs:56-80):
+  // a = b + s c over `len` doubles on all threads, the best of `repeats`, 24 bytes an element
+  std::vector<double> a(len, 0.0), b(len, 1.0), c(len, 2.0);
+  volatile double sv = 3.0;
+  const double sc = sv;
+  double best = 1e300;
+  for (int r = 0; r < std::max(1, repeats); r++) {
+    const double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(static, 1 << 14)
+    for (long q = 0; q < len; q++) a[q] = b[q] + sc * c[q];
+    best = std::min(best, omp_get_wtime() - t0);
+  }
+  volatile double sink = a[len / 2];
+  (void)sink;
+  return 24.0 * (double)len / best / 1e9;
 }
 
 }  // extern "C"

@@ -82,6 +82,9 @@ long orc_tables(const orc_sim *s, int which, double *out);
 /* Stability of a medium (src/fdtd/media.rs:261-309): 1 stable, 0 not. */
 int orc_medium_stable(double eps_inf, int npoles, const double *poles, double sigma, double dt,
                       double top);
+/* The STREAM triad a = b + s c over len doubles on all OpenMP threads, the best of `repeats`
+ * runs, in GB/s at 24 bytes an element (the reference's traffic::triad, src/traffic.rs:56-80). */
+double orc_triad(long len, int repeats);
 
 #ifdef __cplusplus
 }

@@ -72,6 +72,8 @@ def lib():
         x.orc_tables.argtypes = [P, C.c_int, DP]
         x.orc_tables.restype = L
         x.orc_medium_stable.argtypes = [D, C.c_int, DP, D, D, D]
+        x.orc_triad.argtypes = [L, C.c_int]
+        x.orc_triad.restype = D
         _lib = x
     return _lib
 
@@ -279,3 +281,8 @@ class OracleSimulation:
 def medium_stable(medium: Dispersive, sigma: float, dt: float, top: float) -> bool:
     p, pp = _d([v for q in medium.poles for v in q.as_array()] or [0.0])
     return bool(lib().orc_medium_stable(medium.eps_inf, len(medium.poles), pp, sigma, dt, top))
+
+
+def triad(length: int = 1 << 26, repeats: int = 5) -> float:
+    """The host's STREAM triad bandwidth, GB/s, as the reference measures it (src/traffic.rs)."""
+    return float(lib().orc_triad(int(length), int(repeats)))

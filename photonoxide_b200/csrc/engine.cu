@@ -1908,15 +1908,27 @@ __global__ void dft_kernel(const SeriesDev *series, int nseries, const long long
   }
 }
 
+// f64 host values to the engine's precision and back. `in` or `out` may be a host array mapped
+// into the device's address space (then the kernel reads or writes it over the host link
+// directly); grid-stride, so that a few CTAs per SM keep enough requests in flight.
 template <typename T>
 __global__ void convert_kernel(const double *in, T *out, long long n) {
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) out[q] = (T)in[q];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+    out[q] = (T)in[q];
 }
 template <typename T>
 __global__ void widen_kernel(const T *in, double *out, long long n) {
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < n) out[q] = (double)in[q];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+    out[q] = (double)in[q];
+}
+// host[q] += dev[q]: the transforms' sums added into the caller's (Monitors::add,
+// src/fdtd/monitors.rs:866-887), `host` mapped into the device's address space
+__global__ void add_into_kernel(const double *dev, double *host, long long n) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+    host[q] = host[q] + dev[q];
 }
 
 }  // namespace pxf
@@ -2029,6 +2041,10 @@ struct fdtd_ctx {
   MediaArgs<float> mf;
   MediaArgs<double> md;
   long long launches = 0;
+  // staging for host arrays a kernel can't reach (pageable memory): f64 values, made on the
+  // first such transfer and kept (counted in the HBM budget)
+  double *stage = nullptr;
+  long long stage_len = 0;
   // step-kernel timing: pairs of events around each launch while profiling
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -2088,30 +2104,69 @@ cudaError_t copy(fdtd_ctx *c, void *dst, const void *src, size_t bytes, cudaMemc
   return e;
 }
 
+// The device's address of a host array of `bytes` bytes when all of it is page-locked and mapped
+// into the device's address space (cudaHostAlloc'd, or registered with the runtime); else null:
+// pageable memory, which only the copy engines reach, through a staging buffer.
+void *mapped_range(const void *host, size_t bytes) {
+  if (!host || bytes == 0) return nullptr;
+  auto device_address = [](const void *p) -> char * {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? static_cast<char *>(a.devicePointer) : nullptr;
+  };
+  char *first = device_address(host);
+  char *last = device_address(static_cast<const char *>(host) + bytes - 1);
+  if (!first || !last || last != first + (bytes - 1)) return nullptr;
+  return first;
+}
+
+// Blocks for a grid-stride pass over n values: a few CTAs per SM, fewer for short arrays.
+unsigned stride_blocks(const fdtd_ctx *c, long long n) {
+  return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 4LL * c->sms));
+}
+
+// The context's staging buffer for pageable transfers, made on first use.
+int staging(fdtd_ctx *c) {
+  if (c->stage) return 0;
+  const long long len = std::min<long long>(3 * c->N, 1LL << 21);
+  if (int r = alloc(c, (void **)&c->stage, (size_t)len * 8)) return r;
+  c->stage_len = len;
+  return 0;
+}
+
+// n f64 host values into dst in the engine's precision. f64: one copy. f32 from mapped host
+// memory: one kernel reading the host array over the link and converting as it goes (nothing
+// staged); from pageable memory: through the context's staging buffer, a chunk at a time. The
+// caller synchronizes before handing the host array back.
 template <typename T>
 int upload_as(fdtd_ctx *c, void *dst, const double *src, long long n) {
-  // through a staging copy of f64 on the device, converted there
   if (n == 0) return 0;
   if (sizeof(T) == 8) {
     CUDA_TRY(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->stream));
     return 0;
   }
-  double *stage = nullptr;
-  long long chunk = std::min<long long>(n, 1LL << 24);
-  CUDA_TRY(c, cudaMallocAsync((void **)&stage, chunk * 8, c->stream));
-  for (long long at = 0; at < n; at += chunk) {
-    long long m = std::min(chunk, n - at);
-    cudaMemcpyAsync(stage, src + at, m * 8, cudaMemcpyHostToDevice, c->stream);
-    convert_kernel<T><<<(unsigned)((m + 255) / 256), 256, 0, c->stream>>>(stage, (T *)dst + at, m);
+  if (const void *dev = mapped_range(src, (size_t)n * 8)) {
+    convert_kernel<T><<<stride_blocks(c, n), 256, 0, c->stream>>>((const double *)dev, (T *)dst, n);
+    CUDA_TRY(c, cudaGetLastError());
+    return 0;
   }
-  cudaFreeAsync(stage, c->stream);
-  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  CUDA_TRY(c, cudaGetLastError());
+  if (int r = staging(c)) return r;
+  for (long long at = 0; at < n; at += c->stage_len) {
+    const long long m = std::min(c->stage_len, n - at);
+    CUDA_TRY(c, cudaMemcpyAsync(c->stage, src + at, m * 8, cudaMemcpyHostToDevice, c->stream));
+    convert_kernel<T><<<stride_blocks(c, m), 256, 0, c->stream>>>(c->stage, (T *)dst + at, m);
+    CUDA_TRY(c, cudaGetLastError());
+  }
   return 0;
 }
 int upload(fdtd_ctx *c, void *dst, const double *src, long long n) {
   return c->precision == 64 ? upload_as<double>(c, dst, src, n) : upload_as<float>(c, dst, src, n);
 }
+// n values of src into the host's f64 array dst, finished before returning; the mirror of
+// upload_as (f32 into mapped host memory: one kernel widening as it writes over the link).
 template <typename T>
 int download_as(fdtd_ctx *c, double *dst, const void *src, long long n) {
   if (n == 0) return 0;
@@ -2120,17 +2175,20 @@ int download_as(fdtd_ctx *c, double *dst, const void *src, long long n) {
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return 0;
   }
-  double *stage = nullptr;
-  long long chunk = std::min<long long>(n, 1LL << 24);
-  CUDA_TRY(c, cudaMallocAsync((void **)&stage, chunk * 8, c->stream));
-  for (long long at = 0; at < n; at += chunk) {
-    long long m = std::min(chunk, n - at);
-    widen_kernel<T><<<(unsigned)((m + 255) / 256), 256, 0, c->stream>>>((const T *)src + at, stage, m);
-    cudaMemcpyAsync(dst + at, stage, m * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (void *dev = mapped_range(dst, (size_t)n * 8)) {
+    widen_kernel<T><<<stride_blocks(c, n), 256, 0, c->stream>>>((const T *)src, (double *)dev, n);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return 0;
   }
-  cudaFreeAsync(stage, c->stream);
+  if (int r = staging(c)) return r;
+  for (long long at = 0; at < n; at += c->stage_len) {
+    const long long m = std::min(c->stage_len, n - at);
+    widen_kernel<T><<<stride_blocks(c, m), 256, 0, c->stream>>>((const T *)src + at, c->stage, m);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(dst + at, c->stage, m * 8, cudaMemcpyDeviceToHost, c->stream));
+  }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  CUDA_TRY(c, cudaGetLastError());
   return 0;
 }
 int download(fdtd_ctx *c, double *dst, const void *src, long long n) {
@@ -2284,13 +2342,13 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
 // once per (device, step) and remembered.
 int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
   static std::mutex mu;
+  // keyed on the step's exact bits (r is a function of h)
   static std::map<std::pair<int, unsigned>, int> seen;
   int dev = 0;
   CUDA_TRY(c, cudaGetDevice(&dev));
-  unsigned hb, rb;
+  unsigned hb;
   memcpy(&hb, &h, 4);
-  memcpy(&rb, &r, 4);
-  const auto key = std::make_pair(dev, hb ^ (rb * 2654435761u));
+  const auto key = std::make_pair(dev, hb);
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = seen.find(key);
@@ -2711,6 +2769,7 @@ int fdtd_upload_coeffs(fdtd_ctx *c, const double *ca, const double *cb) {
     if (int r = upload(c, c->ca, ca, 3 * c->N)) return r;
   }
   if (int r = upload(c, c->cb, cb, 3 * c->N)) return r;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));  // the host arrays are the caller's again
   c->coeffs_set = true;
   return 0;
 }
@@ -3177,10 +3236,19 @@ int fdtd_read_dft(fdtd_ctx *c, double *sums, int64_t count) {
   if (count != c->nsums)
     return fail(c, FDTD_E_INVALID, "the transforms hold %lld sums, not %lld", c->nsums, (long long)count);
   if (c->nsums == 0) return 0;
+  const long long n = 2 * c->nsums;
+  if (void *dev = mapped_range(sums, (size_t)n * 8)) {
+    // added over the link into the caller's mapped array
+    add_into_kernel<<<stride_blocks(c, n), 256, 0, c->stream>>>(c->sums, (double *)dev, n);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemsetAsync(c->sums, 0, c->nsums * 16, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return 0;
+  }
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  std::vector<double> tmp(2 * c->nsums);
+  std::vector<double> tmp(n);
   CUDA_TRY(c, copy(c, tmp.data(), c->sums, c->nsums * 16, cudaMemcpyDeviceToHost));
-  for (long long q = 0; q < 2 * c->nsums; q++) sums[q] += tmp[q];
+  for (long long q = 0; q < n; q++) sums[q] += tmp[q];
   CUDA_TRY(c, cudaMemsetAsync(c->sums, 0, c->nsums * 16, c->stream));
   return 0;
 }
@@ -3219,13 +3287,15 @@ int64_t fdtd_launches(const fdtd_ctx *c) { return c ? c->launches : 0; }
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
-// Uploading without allocating. fdtd_upload_fields stages each f32 upload through a device
-// buffer it allocates and frees per call. Some callers can't allocate device memory at that
-// point: a serving loop that has handed out its whole HBM budget up front, an application whose
-// CUDA allocator is its own and forbids others, code that must not perturb a stream-ordered
-// memory pool. fdtd_upload_fields_static stages through a fixed array instead: a file-scope
-// device array of STATIC_STAGE_VALUES doubles (16 MiB), which every GPU that loads this library
-// holds until the process exits. The array's address is looked up once per device (below), on
+// Uploading without allocating. fdtd_upload_fields stages an f32 upload from pageable host memory
+// through a device buffer of the context's, which it allocates on the first such upload. Some
+// callers can't allocate device memory at that point: a serving loop that has handed out its
+// whole HBM budget up front, an application whose CUDA allocator is its own and forbids others,
+// code that must not perturb a stream-ordered memory pool. fdtd_upload_fields_static stages
+// through a fixed array instead: a file-scope device array of STATIC_STAGE_VALUES doubles
+// (16 MiB), which every GPU that loads this library holds until the process exits. Only f32
+// contexts stage (f64 values are copied straight into the fields), so only they are limited to
+// components of at most STATIC_STAGE_VALUES values. The array's address is looked up once per device (below), on
 // the first call made with that device current; that first call should come before any stream
 // capture. All calls share the array and it keeps the last call's contents (nothing in it has to
 // start at zero: each pass overwrites what it reads); calls that overlap on the GPU, from two
@@ -3272,14 +3342,15 @@ int upload_static_as(fdtd_ctx *c, double *stage, void *dst, const double *src, l
 
 extern "C" int fdtd_upload_fields_static(fdtd_ctx *c, const double *e, const double *h) {
   if (!c) return FDTD_E_INVALID;
-  c->generation++;
-  if (c->N > STATIC_STAGE_VALUES)
+  if (c->precision == 32 && c->N > STATIC_STAGE_VALUES)
     return fail(c, FDTD_E_INVALID,
                 "a field component of %lld values exceeds the %lld-value static staging array: "
                 "use fdtd_upload_fields",
                 c->N, STATIC_STAGE_VALUES);
   double *stage = nullptr;
-  if (int r = static_stage_address(c, &stage)) return r;
+  if (c->precision == 32)
+    if (int r = static_stage_address(c, &stage)) return r;
+  c->generation++;
   c->parity = 0;
   const size_t E = c->elem;
   const double *src[2] = {e, h};

@@ -49,17 +49,23 @@ extern "C" int pxs_average_device(const int64_t n[3], const double d[3], const d
   cudaStream_t st = nullptr;
   double *d_boxes = nullptr, *d_uniform = nullptr, *d_out = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-  auto step = [&](cudaError_t r) {
-    if (e == cudaSuccess) e = r;
+  // each step runs only while every one before it succeeded (the first error is kept); the
+  // buffers made are freed whatever happened
+  auto step = [&](auto &&call) {
+    if (e == cudaSuccess) e = call();
   };
-  step(cudaMallocAsync(&d_boxes, (size_t)std::max<int64_t>(nb, 1) * 7 * 8, st));
-  step(cudaMallocAsync(&d_uniform, (size_t)(nb + 1) * 8, st));
-  step(cudaMallocAsync(&d_out, (size_t)total * 8, st));
-  if (nb > 0) step(cudaMemcpyAsync(d_boxes, boxes.data(), (size_t)nb * 7 * 8,
-                                   cudaMemcpyHostToDevice, st));
-  step(cudaMemcpyAsync(d_uniform, uniform.data(), (size_t)(nb + 1) * 8, cudaMemcpyHostToDevice,
-                       st));
-  if (e == cudaSuccess) {
+  step([&] { return cudaMallocAsync(&d_boxes, (size_t)std::max<int64_t>(nb, 1) * 7 * 8, st); });
+  step([&] { return cudaMallocAsync(&d_uniform, (size_t)(nb + 1) * 8, st); });
+  step([&] { return cudaMallocAsync(&d_out, (size_t)total * 8, st); });
+  if (nb > 0)
+    step([&] {
+      return cudaMemcpyAsync(d_boxes, boxes.data(), (size_t)nb * 7 * 8, cudaMemcpyHostToDevice, st);
+    });
+  step([&] {
+    return cudaMemcpyAsync(d_uniform, uniform.data(), (size_t)(nb + 1) * 8, cudaMemcpyHostToDevice,
+                           st);
+  });
+  step([&] {
     AverageArgs A;
     for (int a = 0; a < 3; a++) A.n[a] = n[a], A.d[a] = d[a], A.o[a] = o[a];
     A.geo = pxa::BoxView{background, nb, d_boxes};
@@ -67,13 +73,17 @@ extern "C" int pxs_average_device(const int64_t n[3], const double d[3], const d
     A.out = d_out;
     A.total = total;
     average_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(A);
-    step(cudaGetLastError());
+    return cudaGetLastError();
+  });
+  step([&] { return cudaMemcpyAsync(out, d_out, (size_t)total * 8, cudaMemcpyDeviceToHost, st); });
+  if (st) {
+    if (d_boxes) cudaFreeAsync(d_boxes, st);
+    if (d_uniform) cudaFreeAsync(d_uniform, st);
+    if (d_out) cudaFreeAsync(d_out, st);
+    const cudaError_t done = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = done;
+    cudaStreamDestroy(st);
   }
-  step(cudaMemcpyAsync(out, d_out, (size_t)total * 8, cudaMemcpyDeviceToHost, st));
-  if (d_boxes) cudaFreeAsync(d_boxes, st);
-  if (d_uniform) cudaFreeAsync(d_uniform, st);
-  if (d_out) cudaFreeAsync(d_out, st);
-  step(cudaStreamSynchronize(st));
-  if (st) cudaStreamDestroy(st);
+  if (e != cudaSuccess) cudaGetLastError();  // leave no sticky launch error behind
   return e == cudaSuccess ? 0 : -2;
 }

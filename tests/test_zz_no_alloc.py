@@ -35,6 +35,21 @@ def ptr(a):
     return a.ctypes.data_as(DP)
 
 
+def pool_in_use():
+    """Bytes the device's default memory pool (the one cudaMallocAsync draws on) has handed out,
+    and the device's free memory: an upload that allocates moves one or the other."""
+    from cuda.bindings import runtime as rt
+    import torch
+    dev = torch.cuda.current_device()
+    err, pool = rt.cudaDeviceGetDefaultMemPool(dev)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, free, _total = rt.cudaMemGetInfo()
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(used), int(free)
+
+
 @pytest.mark.parametrize("precision", [32, 64])
 def test_static_upload_matches_the_allocating_one_twice(precision):
     lib = bind()
@@ -52,7 +67,11 @@ def test_static_upload_matches_the_allocating_one_twice(precision):
         out = []
         for static in (False, True):
             if static:
+                used0, free0 = pool_in_use()
                 rc = lib.fdtd_upload_fields_static(ctx, ptr(e), ptr(h))
+                # nothing allocated: the pool hands out no more, the device has no less free
+                used1, free1 = pool_in_use()
+                assert used1 == used0 and free1 >= free0, (call, used0, used1, free0, free1)
             else:
                 rc = lib.fdtd_upload_fields(ctx, ptr(e), ptr(h), None)
             assert rc == 0, lib.fdtd_last_error(ctx)
@@ -74,3 +93,27 @@ def test_static_upload_refuses_a_grid_beyond_its_array():
     rc = lib.fdtd_upload_fields_static(ctx, ptr(e), ptr(e))
     assert rc == -1
     assert b"static staging array" in lib.fdtd_last_error(ctx)
+
+
+def test_static_upload_takes_any_f64_grid():
+    """Only an f32 context stages through the fixed array: an f64 context copies straight into
+    its fields, so a grid beyond the array's 2^21 values is taken, with the allocating upload's
+    result."""
+    lib = bind()
+    g = Grid3d(256, 128, 65, 0.05, 0.05, 0.05)  # 2 129 920 cells > 2^21
+    sim = Simulation(g, np.full((3, g.cells()), 2.0), Boundaries.walls(), 0.5, precision=64)
+    sim.run(1)
+    ctx = sim.engine()
+    rng = np.random.default_rng(3)
+    n = 3 * g.cells()
+    e, h = rng.standard_normal(n), rng.standard_normal(n)
+    out = []
+    for static in (False, True):
+        rc = (lib.fdtd_upload_fields_static(ctx, ptr(e), ptr(h)) if static
+              else lib.fdtd_upload_fields(ctx, ptr(e), ptr(h), None))
+        assert rc == 0, lib.fdtd_last_error(ctx)
+        assert lib.fdtd_run(ctx, 3, 0) == 0, lib.fdtd_last_error(ctx)
+        ed = np.empty(n)
+        assert lib.fdtd_download_fields(ctx, ptr(ed), None, None) == 0
+        out.append(ed)
+    assert np.array_equal(out[0], out[1])
