@@ -387,8 +387,9 @@ struct Sim : Base {
       double h = g.d[axis];
       auto profile = [&](double depth, long cells, double &s, double &k) {
         double d = (double)cells * h;
-        double x = std::pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
-        double smax = std::isnan(sig) ? (order + 1.0) * (-std::log(R)) / (2.0 * d) : sig;
+        // portable::powf and portable::ln (src/fdtd.rs:811-815), restated in refmath.h
+        double x = refmath::ref_pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
+        double smax = std::isnan(sig) ? (order + 1.0) * (-refmath::ref_ln(R)) / (2.0 * d) : sig;
         s = smax * x;
         k = 1.0 + (kmax - 1.0) * x;
       };
@@ -701,7 +702,7 @@ std::vector<c64> roots(std::vector<double> p) {
   if (n == 0) return {};
   double lead = p[n];
   for (double &c : p) c /= lead;
-  double radius = std::max(std::pow(std::fabs(p[0]), 1.0 / (double)n), 1e-3);
+  double radius = std::max(refmath::ref_pow(std::fabs(p[0]), 1.0 / (double)n), 1e-3);
   std::vector<c64> z(n);
   for (size_t k = 0; k < n; k++) z[k] = std::polar(radius, TAU * ((double)k + 0.25) / (double)n);
   for (int it = 0; it < 500; it++) {

