@@ -1,0 +1,117 @@
+"""The measured workloads at their full grid sizes: the engine in f32 (the product) against the
+oracle in f64 (the reference's own arithmetic, src/fdtd/kernel/reference.rs), with the error
+stated per result against the tolerances the engine is held to: a monitor's time series within a
+relative L2 of 1e-4, a flux spectrum within |dT(lambda)| / max T of 1e-4, fields within the
+reference's GPU tolerance of 2e-5 of their largest value (src/fdtd/gpu/tests.rs:51-66,
+docs/validation-gpu.md:15-16, where its f32 GPU kernel is held to its f64 CPU one).
+
+- The 2D TE strip (400 x 200, 4000 steps, a transform of the whole plane at 21 wavelengths) runs
+  in full on both, live.
+- The 3D MMI (600 x 200 x 100) and the dispersive grid (256 x 256 x 128, Drude and two-pole
+  Lorentz boxes) run a few hundred steps on both, live, and are compared field by field; their
+  full runs (20 000 and 10 000 steps) are compared with the oracle's results kept in
+  tests/golden/ (tests/golden/make_golden.py made them; the oracle takes tens of minutes there).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from photonoxide_b200 import configs
+from photonoxide_b200.fdtd import Simulation
+from pyoracle import OracleSimulation
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def engine32(*a, precision=32, **kw):
+    return Simulation(*a, precision=32, **kw)
+
+
+def oracle64(*a, precision=32, **kw):
+    return OracleSimulation(*a, precision=64, **kw)
+
+
+def golden(name):
+    path = os.path.join(GOLDEN, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not made (tests/golden/make_golden.py)")
+    return np.load(path)
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def worst_field(p, o):
+    """The largest difference over the six field components, relative to each one's largest."""
+    worst = 0.0
+    for get in ("e", "h"):
+        for c in range(3):
+            x, y = getattr(p, get)(c), getattr(o, get)(c)
+            scale = float(np.max(np.abs(y)))
+            if scale > 0:
+                worst = max(worst, float(np.max(np.abs(x - y))) / scale)
+    return worst
+
+
+def test_strip_2d_full_run():
+    p, info = configs.strip_2d(engine32)
+    o, _ = configs.strip_2d(oracle64)
+    p.run(info["steps"])
+    o.run(info["steps"])
+    probe = rel_l2(p.probe(info["probe"]), o.probe(info["probe"]))
+    dft = rel_l2(np.abs(p.transforms()), np.abs(o.transforms()))
+    print(f"strip 2D, 4000 steps: probe rel. L2 {probe:.3g}, |DFT| rel. L2 {dft:.3g}")
+    assert probe <= 1e-4
+    assert dft <= 1e-4
+    assert worst_field(p, o) <= 2e-5
+
+
+def test_mmi_fields():
+    p, info = configs.mmi_3d(engine32)
+    o, _ = configs.mmi_3d(oracle64)
+    p.run(300)
+    o.run(300)
+    worst = worst_field(p, o)
+    print(f"MMI, 300 steps: fields within {worst:.3g} of their largest")
+    assert worst <= 2e-5
+
+
+def test_mmi_full_run():
+    g = golden("mmi_20000.npz")
+    p, info = configs.mmi_3d(engine32)
+    p.run(int(g["steps"]))
+    flux = np.array([p.flux(n) for n in info["fluxes"]])
+    ref = g["flux"]
+    dT = float(np.max(np.abs(flux - ref)) / np.max(np.abs(ref)))
+    probe = rel_l2(p.probe(info["probe"]), g["probe"])
+    print(f"MMI, 20000 steps: max |dT| / max T {dT:.3g}, probe rel. L2 {probe:.3g}")
+    assert dT <= 1e-4
+    assert probe <= 1e-4
+
+
+def test_dispersive_fields():
+    p, info = configs.dispersive_3d(engine32, 7)
+    o, _ = configs.dispersive_3d(oracle64, 7)
+    p.run(200)
+    o.run(200)
+    worst = worst_field(p, o)
+    print(f"dispersive, 200 steps: fields within {worst:.3g} of their largest")
+    assert worst <= 2e-5
+
+
+def test_dispersive_full_run():
+    g = golden("dispersive_10000.npz")
+    p, info = configs.dispersive_3d(engine32, 7)
+    p.run(int(g["steps"]))
+    probe = rel_l2(p.probe(info["probe"]), g["probe"])
+    grid = p.grid
+    ez = p.e(2).reshape(grid.nz, grid.ny, grid.nx)[grid.nz // 2]
+    plane = rel_l2(ez, g["ez_mid"])
+    print(f"dispersive, 10000 steps: probe rel. L2 {probe:.3g}, E_z mid-plane rel. L2 {plane:.3g}")
+    assert probe <= 1e-4
+    assert plane <= 1e-4
