@@ -26,6 +26,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -826,31 +827,35 @@ __global__ void te_segment_phase_kernel(const TeInst<T> *insts, long long first,
 // Step m's direct part of J's derivative: the transforms took F dt e^{i w t} of each value, so
 // dJ/dF = sum over frequencies of dJ/dRe(sum) Re(phase) + dJ/dIm(sum) Im(phase), added to E~
 // or H~ of the value (TE components only: the others are zero whatever the permittivity).
+// Without atomics, so that the gradient's bits never depend on scheduling: one thread per field
+// value the transforms record, adding each of its transform values' dJ/dF in value order.
+// `owner` lists, per such field value, its place (with the H flag in bit 62, as `where`) and
+// its transform values order[start[g] .. start[g+1]).
 template <typename T>
-__global__ void te_inject_kernel(const TeInst<T> *insts, const RecItem *items, long long nitems,
-                                 const double *phase, const double *grad_sums, AdjState<T> A,
-                                 int m) {
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nitems) return;
-  const RecItem it = items[q];
-  if (it.kind != 0) return;
+__global__ void te_inject_kernel(const TeInst<T> *insts, const long long *owner, const int *start,
+                                 const long long *order, int nowners, const double *phase,
+                                 const double *grad_sums, AdjState<T> A, int m) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nowners) return;
   const TeInst<T> &I = insts[0];
-  const long long v = it.index;
-  const long long w = I.where[v];
+  const long long w = owner[g];
   const bool hfield = (w >> 62) != 0;
   const long long place = w & ((1LL << 62) - 1);
-  const int comp = (int)(place / I.N);
-  if (hfield ? comp != 2 : comp == 2) return;
-  const SeriesDev s = I.series[I.value_series[v]];
-  const long long o = v - s.value0;
-  const double *ph = phase + 2 * ((long long)m * I.nslots + s.slot0);
-  double x = 0.0;
-  for (int k = 0; k < s.nf; k++) {
-    const double *g = grad_sums + 2 * (s.sum0 + (long long)k * s.volume + o);
-    x += g[0] * ph[2 * k] + g[1] * ph[2 * k + 1];
+  T *f = hfield ? A.h[A.cur] + (place - 2 * I.N) : A.e[A.cur] + place;
+  T acc = *f;
+  for (int q = start[g]; q < start[g + 1]; q++) {
+    const long long v = order[q];
+    const SeriesDev s = I.series[I.value_series[v]];
+    const long long o = v - s.value0;
+    const double *ph = phase + 2 * ((long long)m * I.nslots + s.slot0);
+    double x = 0.0;
+    for (int k = 0; k < s.nf; k++) {
+      const double *gs = grad_sums + 2 * (s.sum0 + (long long)k * s.volume + o);
+      x += gs[0] * ph[2 * k] + gs[1] * ph[2 * k + 1];
+    }
+    acc = acc + (T)x;
   }
-  if (hfield) atomicAdd(A.h[A.cur] + (place - 2 * I.N), (T)x);
-  else atomicAdd(A.e[A.cur] + place, (T)x);
+  *f = acc;
 }
 
 // dJ/dcb at each design value += E~ (of the values after the step) x the step's curl there.
@@ -1564,6 +1569,10 @@ struct fdtd_adjoint {
   double *d_grad = nullptr;     // ndesign
   double *d_gsums = nullptr;    // dJ/dsums
   double *d_phase = nullptr;    // segment x nslots phases
+  // the injection's owners (te_inject_kernel): field values, their transform values
+  long long *d_owner = nullptr, *d_order = nullptr;
+  int *d_start = nullptr;
+  int nowners = 0;
   // checkpoints: E_x, E_y, H_z, H's psi and E's psi at the start of each segment, and at the end
   void *d_ckpt = nullptr;
   size_t ckpt_bytes = 0;
@@ -1703,9 +1712,9 @@ int backward_impl(fdtd_adjoint *a, const double *grad_sums, double *grad_cb) {
                                                                             a->d_phase);
     }
     for (int m = len - 1; m >= 0; m--) {
-      if (v.nsums > 0 && b->nrec > 0)
-        te_inject_kernel<T><<<(unsigned)((b->nrec + 255) / 256), 256, 0, b->stream>>>(
-            insts, b->d_rec, b->nrec, a->d_phase, a->d_gsums, A, m);
+      if (v.nsums > 0 && a->nowners > 0)
+        te_inject_kernel<T><<<(unsigned)((a->nowners + 255) / 256), 256, 0, b->stream>>>(
+            insts, a->d_owner, a->d_start, a->d_order, a->nowners, a->d_phase, a->d_gsums, A, m);
       te_grad_kernel<T><<<(unsigned)((a->ndesign + 255) / 256), 256, 0, b->stream>>>(
           a->d_design, a->ndesign, (const T *)a->d_K + (long long)m * a->ndesign, A, a->d_grad);
       te_adjoint_kernel<T, 64, 8><<<blocks, THREADS, 0, b->stream>>>(insts, A, tiles);
@@ -1779,6 +1788,35 @@ int fdtd_adjoint_create(fdtd_ctx *ctx, int64_t steps, int32_t segment, int64_t c
   if (int q = amalloc(a, &a->d_ckpt, (size_t)(a->nseg + 1) * a->ckpt_bytes)) return q;
   if (int q = amalloc(a, &a->d_adj, (size_t)2 * (3 * v.N + pe + ph) * E)) return q;
   ATRY(a, cudaMemcpy(a->d_design, design.data(), count * 8, cudaMemcpyHostToDevice));
+  // the field values the transforms record, each with its transform values in value order
+  if (v.nvalues > 0 && v.nsums > 0) {
+    std::vector<long long> where(v.nvalues);
+    ATRY(a, cudaMemcpy(where.data(), v.where, v.nvalues * 8, cudaMemcpyDeviceToHost));
+    std::map<long long, std::vector<long long>> by_place;
+    for (long long q = 0; q < v.nvalues; q++) {
+      const long long place = where[q] & ((1LL << 62) - 1);
+      const bool hfield = (where[q] >> 62) != 0;
+      const int comp = (int)(place / v.N);
+      if (hfield ? comp != 2 : comp == 2) continue;  // E_z, H_x, H_y: zero whatever eps
+      by_place[where[q]].push_back(q);
+    }
+    std::vector<long long> owner, order;
+    std::vector<int> start(1, 0);
+    for (const auto &kv : by_place) {
+      owner.push_back(kv.first);
+      order.insert(order.end(), kv.second.begin(), kv.second.end());
+      start.push_back((int)order.size());
+    }
+    a->nowners = (int)owner.size();
+    if (a->nowners > 0) {
+      if (int q = amalloc(a, (void **)&a->d_owner, owner.size() * 8)) return q;
+      if (int q = amalloc(a, (void **)&a->d_order, order.size() * 8)) return q;
+      if (int q = amalloc(a, (void **)&a->d_start, start.size() * 4)) return q;
+      ATRY(a, cudaMemcpy(a->d_owner, owner.data(), owner.size() * 8, cudaMemcpyHostToDevice));
+      ATRY(a, cudaMemcpy(a->d_order, order.data(), order.size() * 8, cudaMemcpyHostToDevice));
+      ATRY(a, cudaMemcpy(a->d_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
+    }
+  }
   fdtd_ctx *one[1] = {ctx};
   if (int q = fdtd_batch_create(1, one, &a->batch))
     return afail(a, q, "%s", fdtd_batch_last_error(a->batch));
