@@ -531,7 +531,9 @@ def _te_instances(count, seed=0, precision=32):
 def workload_batch(args):
     """Configuration 4, forward: 64 uneven 2D TE instances (sides log-uniform 256-1024 cells) with
     100x100 design regions, 6000 steps, batched (one persistent launch per step for all, CUDA-
-    graph chunks, tile shape by timing) against the same instances run one at a time."""
+    graph chunks, tile shape by timing) against the same instances run one at a time: through the
+    3D engine (``one_at_a_time``) and as batches of one on the same TE kernel and tile shape
+    (``one_at_a_time_te_kernel``, which isolates the batching's own gain)."""
     from photonoxide_b200.batch import Batch
     steps = args.batch_steps
     sims = _te_instances(64)
@@ -543,11 +545,18 @@ def workload_batch(args):
     for s in alone:
         s.run(3)
     _, ta = _timed(lambda: [s.run(steps) for s in alone])
+    # one at a time on the same TE kernel: each instance a batch of one, the batch's tile shape
+    ones = [Batch([s], tile=B.tile) for s in _te_instances(64)]
+    for one in ones:
+        one.run(3)
+    _, t1 = _timed(lambda: [one.run(steps) for one in ones])
     line = {"metric": "batched 2D TE Gcell-updates/s vs one at a time (64 instances)",
             "value": steps * cells / tb / 1e9, "unit": UNIT, "n_gpus": 1, "steps": steps,
             "dtype": "f32", "higher_is_better": True, "data": "synthetic",
             "one_at_a_time": steps * cells / ta / 1e9,
             "speedup": ta / tb, "tile": list(B.tile),
+            "one_at_a_time_te_kernel": steps * cells / t1 / 1e9,
+            "speedup_vs_te_kernel_one_at_a_time": t1 / tb,
             "config": {"workload": "64 2D TE instances, sides log-uniform 256-1024 at 20 nm, "
                                    "100x100 random design, CPML 12, flux monitor at 1550 nm",
                        "cells": cells}}
@@ -596,8 +605,9 @@ def workload_adjoint(args):
 
 
 def workload_serving(args):
-    """Configuration 5, scaled to minutes: a seeded Poisson stream of jobs (20/s; 70% 2D, 30% 3D;
-    cells log-uniform 1e5-5e6; steps 2000-20000; 1-4 Si boxes in SiO2; 1-51 DFT wavelengths) served
+    """Configuration 5: a seeded Poisson stream of jobs (20/s; 70% 2D, 30% 3D; cells log-uniform
+    1e5-5e7, or PHOTONOXIDE_SERVING_CELLS="lo,hi"; PHOTONOXIDE_SERVING_JOBS of them, 60 by default;
+    steps 2000-20000; 1-4 Si boxes in SiO2; 1-51 DFT wavelengths) served
     by the resident loop (150 GB budget, continuous admission) against the same jobs run one at a
     time in arrival order: p50/p99 latency and aggregate Gcell-updates/s. The offered load exceeds
     the GPU's capacity (a backlog builds), as at full scale. A job's results are its transforms
@@ -607,7 +617,8 @@ def workload_serving(args):
     import torch
     from photonoxide_b200.serving import Server, job_stream, make_job
     count = int(os.environ.get("PHOTONOXIDE_SERVING_JOBS", "60"))
-    specs = job_stream(count, rate=20.0, seed=5, cells=(1e5, 5e6), steps=(2000, 20000))
+    lo, hi = (float(v) for v in os.environ.get("PHOTONOXIDE_SERVING_CELLS", "1e5,5e7").split(","))
+    specs = job_stream(count, rate=20.0, seed=5, cells=(lo, hi), steps=(2000, 20000))
     work = sum(int(np.prod(sp.n)) * sp.steps for sp in specs)
     # one at a time, in arrival order: each job run and its results read back
     sims = [make_job(sp) for sp in specs]
@@ -648,9 +659,9 @@ def workload_serving(args):
                                             "p99": float(np.percentile(lat1, 99))}},
             "speedup": span1 / span,
             "loop_seconds": {k: loop[k] for k in ("launch_s", "host_s", "wait_s")},
-            "config": {"workload": "Poisson stream, 20 jobs/s, 70% 2D / 30% 3D, cells "
-                                   "log-uniform 1e5-5e6 (scaled from 1e5-5e7), steps "
-                                   "2000-20000, 150 GB budget; host set-up before the stream", "cell_updates": work}}
+            "config": {"workload": f"Poisson stream, 20 jobs/s, 70% 2D / 30% 3D, cells "
+                                   f"log-uniform {lo:g}-{hi:g}, steps 2000-20000, 150 GB budget; "
+                                   "host set-up before the stream", "cell_updates": work}}
     print(json.dumps(line), flush=True)
     return 0
 
