@@ -66,6 +66,9 @@ struct MediaArgs {
   T two_dt;
   const long long *place;  // per member: its value (component * N + r); members in value order
   long long members;
+  // quad kernel: per (tile, plane), tile * nz + k, whether any of its values is a member (then
+  // its lanes read their values' member numbers, four at once)
+  const unsigned char *tileplane;
 };
 
 // The quad kernel's runs of z-planes, at most this many (their starts travel with the launch).
@@ -1779,13 +1782,19 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
               }
         }
       }
-      if (MEDIA && any_own) {
+      // the dispersive media's ADE currents (src/fdtd/media.rs:661-705), last, in the same pass:
+      // only tiles and planes that hold members look their values' member numbers up
+      if (MEDIA && any_own && A.media.tileplane[(long long)tile * nz + k]) {
+        int4 mq[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          mq[c] = __ldg(reinterpret_cast<const int4 *>(A.media.member + c * N + at));
 #pragma unroll
         for (int c = 0; c < 3; c++)
 #pragma unroll
           for (int j = 0; j < 4; j++) {
             if (!ownv[j]) continue;
-            int mi = A.media.member[c * N + at + j];
+            const int mi = j == 0 ? mq[c].x : (j == 1 ? mq[c].y : (j == 2 ? mq[c].z : mq[c].w));
             if (mi < 0) continue;
             const MediaArgs<T> &M = A.media;
             int g = M.group[mi];
@@ -2254,36 +2263,6 @@ void launch_staged(fdtd_ctx *c, const StepArgs<T> &A) {
   kernel<<<ctas, NT, smem, c->stream>>>(A, total, ctas);
 }
 
-// The dispersive media's ADE update (src/fdtd/media.rs:661-705) as a pass of its own over the
-// members, after the step kernel has written E (curl, slabs and currents): the same arithmetic
-// as the kernels' fused MEDIA branch, reading E^n from the step's input copy and the updated E
-// from its output, one member a thread in value order.
-template <typename T>
-__global__ void media_kernel(StepArgs<T> A) {
-  const MediaArgs<T> &M = A.media;
-  long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= M.members) return;
-  const long long at = M.place[q];
-  const int g = M.group[q];
-  const int np = M.gpoles[g];
-  const T before = M.before[q];
-  T rest = M.gchi[g] * before;
-  const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
-  T *cur = M.current + q * M.maxpoles;
-  T *prev = M.previous + q * M.maxpoles;
-  for (int p = 0; p < np; p++)
-    rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
-  const T next = A.e_out[at] + M.scale[q] * rest;
-  const T slope = (next - before) / M.two_dt;
-  for (int p = 0; p < np; p++) {
-    const T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
-    prev[p] = cur[p];
-    cur[p] = jn;
-  }
-  M.before[q] = A.e_in[at];
-  A.e_out[at] = next;
-}
-
 template <typename T>
 void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
   if (c->quad) {
@@ -2294,11 +2273,14 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       kernel<<<grid, quad::THREADS, smem, c->stream>>>(A);
     };
-    // media: the step without them, then their pass over the members
-    if (c->lossless) go(quad_kernel<T, false, false>);
-    else go(quad_kernel<T, true, false>);
-    if (c->media)
-      media_kernel<T><<<(unsigned)((A.media.members + 255) / 256), 256, 0, c->stream>>>(A);
+    // the media's ADE fused in (MEDIA): one launch a step
+    if (c->media) {
+      if (c->lossless) go(quad_kernel<T, false, true>);
+      else go(quad_kernel<T, true, true>);
+    } else {
+      if (c->lossless) go(quad_kernel<T, false, false>);
+      else go(quad_kernel<T, true, false>);
+    }
     return;
   }
   if (c->row) {
@@ -2502,7 +2484,7 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
       } else {
         launch_step<T>(c, A);
       }
-      c->launches += (c->quad && c->media) ? 2 : 1;
+      c->launches += 1;
       c->parity = 1 - c->parity;
       long long gathered = c->nvalues + c->nprobes;
       if (gathered > 0) {
@@ -3173,6 +3155,21 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
   CUDA_TRY(c, cudaMemsetAsync(d_before, 0, members * E, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(d_cur, 0, members * maxp * E, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(d_prev, 0, members * maxp * E, c->stream));
+  // the quad kernel's (tile, plane) flags
+  void *d_tileplane = nullptr;
+  if (c->quad) {
+    const long long nxy = (long long)c->n[0] * c->n[1];
+    std::vector<unsigned char> tp((size_t)c->tiles_x * c->tiles_y * c->n[2], 0);
+    for (long long m = 0; m < members; m++) {
+      const long long r = place[m] % c->N;
+      const int i = (int)(r % c->n[0]), j = (int)((r / c->n[0]) % c->n[1]);
+      const int k = (int)(r / nxy);
+      const long long tile = (long long)(j / quad::RW) * c->tiles_x + i / quad::OWNX;
+      tp[(size_t)(tile * c->n[2] + k)] = 1;
+    }
+    if (int r = alloc(c, &d_tileplane, tp.size())) return r;
+    CUDA_TRY(c, copy(c, d_tileplane, tp.data(), tp.size(), cudaMemcpyHostToDevice));
+  }
   auto fillm = [&](auto &M) {
     using T = typename std::remove_pointer<decltype(M.scale)>::type;
     using TT = typename std::remove_const<T>::type;
@@ -3190,6 +3187,7 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
     M.two_dt = (TT)(2.0 * c->dt);
     M.place = (const long long *)d_place;
     M.members = members;
+    M.tileplane = (const unsigned char *)d_tileplane;
   };
   if (c->precision == 64) fillm(c->md);
   else fillm(c->mf);
