@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 namespace {
@@ -1120,24 +1121,33 @@ int orc_add_medium(orc_sim *s, double eps_inf, int npoles, const double *poles,
         }
     }
     std::vector<T> scale;
+    // Media::remove of every value this medium takes over: each old group keeps its other values
+    // in their order. Done a group at a time (one pass over each group that loses values) rather
+    // than one pass per value, which is the same result.
+    std::map<int, std::unordered_set<long>> leaving;
+    for (size_t v = 0; v < values.size(); v++) {
+      auto it = x.members.find(values[v]);
+      if (it != x.members.end()) {
+        leaving[it->second].insert(values[v].first * N + values[v].second);
+        x.members.erase(it);
+      }
+    }
+    for (auto &kv : leaving) {
+      auto &gr = x.groups[kv.first];
+      std::vector<std::pair<int, long>> keep;
+      std::vector<T> sc;
+      for (size_t q = 0; q < gr.values.size(); q++)
+        if (!kv.second.count(gr.values[q].first * N + gr.values[q].second)) {
+          keep.push_back(gr.values[q]);
+          sc.push_back(gr.scale[q]);
+        }
+      gr.values = keep;
+      gr.scale = sc;
+      gr.resize();
+    }
     for (size_t v = 0; v < values.size(); v++) {
       int c = values[v].first;
       long r = values[v].second;
-      auto it = x.members.find({c, r});
-      if (it != x.members.end()) {  // Media::remove
-        auto &gr = x.groups[it->second];
-        std::vector<std::pair<int, long>> keep;
-        std::vector<T> sc;
-        for (size_t q = 0; q < gr.values.size(); q++)
-          if (gr.values[q] != values[v]) {
-            keep.push_back(gr.values[q]);
-            sc.push_back(gr.scale[q]);
-          }
-        gr.values = keep;
-        gr.scale = sc;
-        gr.resize();
-        x.members.erase(it);
-      }
       double sg = sigmas[v];
       double nu = 1.0 + dt / eps_inf * (sg / 2.0 + chi);
       x.ca64[c][r] = (1.0 - dt * sg / (2.0 * eps_inf)) / nu;
