@@ -133,4 +133,30 @@ __host__ __device__ __forceinline__ double div_by_step(double x, double h, doubl
   return x / h;
 }
 
+// Four quotients x[j] / h at once, each div_by_step's: where all four take its common path (x
+// not tiny, a normal quotient) that path's three operations each and one test for the four;
+// otherwise div_by_step value by value. The same bits either way.
+__host__ __device__ __forceinline__ void div4_by_step(const float x[4], float q[4], float h, float r,
+                                                      double rd, int fast) {
+  if (fast) {
+    bool common = true;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const float q0 = x[j] * r;
+      const float e = fmaf(-q0, h, x[j]);
+      q[j] = fmaf(e, r, q0);
+      const float aq = fabsf(q[j]);
+      common = common && fabsf(x[j]) >= 0x1p-90f && aq >= 0x1p-126f && aq <= 3.40282347e38f;
+    }
+    if (common) return;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) q[j] = div_by_step(x[j], h, r, rd, fast);
+}
+__host__ __device__ __forceinline__ void div4_by_step(const double x[4], double q[4], double h,
+                                                      double, double, int) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) q[j] = x[j] / h;
+}
+
 }  // namespace pxf

@@ -66,9 +66,6 @@ struct MediaArgs {
   T two_dt;
   const long long *place;  // per member: its value (component * N + r); members in value order
   long long members;
-  // quad kernel: per (tile, plane), tile * nz + k, whether any of its values is a member (then
-  // its lanes read their values' member numbers, four at once)
-  const unsigned char *tileplane;
 };
 
 // The quad kernel's runs of z-planes, at most this many (their starts travel with the launch).
@@ -397,6 +394,11 @@ __device__ inline void cp_async16(void *smem, const void *gmem, bool valid) {
                : "memory");
 }
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Brings `bytes` (a multiple of 16, from a 16-byte aligned address) of global memory into L2
+// ahead of use, without waiting and without registers.
+__device__ inline void prefetch_l2(const void *gmem, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(gmem), "r"(bytes) : "memory");
+}
 template <int N>
 __device__ inline void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -1215,9 +1217,11 @@ __device__ __forceinline__ void slab4(const StepArgs<T> &A, T *psi_out, const T 
                                       bool write) {
   Vec4<T> old = ld4(psi_in);
   Vec4<T> nw;
+  T q[4];
+  div4_by_step(diff, q, A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    T d = div_by_step(diff[j], A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
+    T d = q[j];
     nw.v[j] = b * old.v[j] + a * d;
     T u = sign * nw.v[j];
     if (FIELD == 1) v[j] = v[j] - A.dt * u;
@@ -1233,9 +1237,11 @@ __device__ __forceinline__ void slab4_loaded(const StepArgs<T> &A, T *psi_out, c
                                              const T diff[4], T v[4], const T cbv[4], bool write) {
   const T b = A.coefs[s.coef + q], a = A.coefs[s.coef + s.count + q];
   Vec4<T> nw;
+  T dq[4];
+  div4_by_step(diff, dq, A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
 #pragma unroll
   for (int j = 0; j < 4; j++) {
-    T d = div_by_step(diff[j], A.step[axis], A.inv_step[axis], A.inv_step64[axis], A.fast_div[axis]);
+    T d = dq[j];
     nw.v[j] = b * old.v[j] + a * d;
     T u = sign * nw.v[j];
     if (FIELD == 1) v[j] = v[j] - A.dt * u;
@@ -1395,7 +1401,45 @@ __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x
   }
 }
 
-template <typename T, bool LOSSY, bool MEDIA>
+// Member q's ADE update (src/fdtd/media.rs:661-705), after the step has written E^{n+1} (curl,
+// slabs and currents) into e_out: J_p^{n+1} = alpha J_p^n + xi J_p^{n-1} + gamma (E^{n+1} -
+// E^{n-1}) / (2 dt) with E^{n+1} corrected by the currents' chi; E^n from e_in kept as E^{n-1}.
+template <typename T>
+__device__ __forceinline__ void ade_update(const StepArgs<T> &A, long long q) {
+  const MediaArgs<T> &M = A.media;
+  const long long at = M.place[q];
+  const int g = M.group[q];
+  const int np = M.gpoles[g];
+  const T before = M.before[q];
+  T rest = M.gchi[g] * before;
+  const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
+  T *cur = M.current + q * M.maxpoles;
+  T *prev = M.previous + q * M.maxpoles;
+  for (int p = 0; p < np; p++)
+    rest = rest - T(0.5) * ((pl[3 * p] + T(1)) * cur[p] + pl[3 * p + 1] * prev[p]);
+  const T next = A.e_out[at] + M.scale[q] * rest;
+  const T slope = (next - before) / M.two_dt;
+  for (int p = 0; p < np; p++) {
+    const T jn = pl[3 * p] * cur[p] + pl[3 * p + 1] * prev[p] + pl[3 * p + 2] * slope;
+    prev[p] = cur[p];
+    cur[p] = jn;
+  }
+  M.before[q] = A.e_in[at];
+  A.e_out[at] = next;
+}
+
+// The dispersive media's ADE update as a pass of its own after the step kernel, one thread a
+// member in value order. (Run inside the step kernel, at the end of each CTA's run of planes,
+// the same update took a step on the dispersive 256 x 256 x 128 grid from 0.353 to 0.434 ms:
+// the members' gathers are latency-bound and held up the stencil's CTAs; as a pass of its own
+// they run at the whole device's occupancy.)
+template <typename T>
+__global__ void ade_kernel(StepArgs<T> A) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < A.media.members) ade_update(A, q);
+}
+
+template <typename T, bool LOSSY>
 __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   using namespace quad;
   using S = Smem<T>;
@@ -1496,75 +1540,66 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const bool ecur = A.ebucket[(long long)tile * nz] != A.ebucket[(long long)tile * nz + nz];
 
   // -- copies: warp w copies E's row w (and the last warp also row RW+1), H's row w and cb's row
-  // w-1 of a plane; lane l the chunks of its four places (lane 0 also the chunk after the row)
+  // w-1 of a plane; lane l the chunks of its four places (lane 0 also the chunk after the row).
+  // Where a chunk lies beyond a wall (a row, a group of four or a plane the grid doesn't have)
+  // it is zero-filled, so the staged neighbours there are the zeros the differences need.
+  // Each chunk's offset within a plane is fixed for the run: -1 where it lies beyond a wall.
   const int myp_last = wrap_index(y0 + RW, ny, A.periodic[1]);
-  auto issue = [&](int eslot, int ke, int hslot, int kh) {
-    // E(ke) rows into E slot `eslot` (ke < 0: zeros); H(kh), cb(kh) rows into HB slot `hslot`
-    T *E = sEs + (size_t)eslot * S::E_SLOT;
-    const T *dummy = A.e_in;
+  const bool last_warp = w == WARPS - 1;
+  const long long off_e0 = (my >= 0 && mxb >= 0) ? (long long)my * nx + mxb : -1;
+  const long long off_ea0 = (my >= 0 && mxa >= 0) ? (long long)my * nx + mxa : -1;
+  const long long off_e1 = (myp_last >= 0 && mxb >= 0) ? (long long)myp_last * nx + mxb : -1;
+  const long long off_ea1 = (myp_last >= 0 && mxa >= 0) ? (long long)myp_last * nx + mxa : -1;
+  const long long off_h = off_e0;
+  const long long off_b = (w >= 1 && gy < ny) ? off_e0 : -1;
+  // this thread's places in a staged E row, H row and cb row
+  const int erow = w * EW + VEC * lane, hrow = w * ROW + VEC * lane;
+  const int brow = (w >= 1 ? w - 1 : 0) * ROW + VEC * lane;
+  auto chunk = [&](T *dst, const T *field, long long off, long long pbase) {
+    const bool ok = off >= 0 && pbase >= 0;
+    const T *src = ok ? field + pbase + off : A.e_in;
 #pragma unroll
-    for (int rsel = 0; rsel < 2; rsel++) {
-      if (rsel == 1 && w != WARPS - 1) break;
-      const int r = rsel == 0 ? w : RW + 1;
-      const int yrow = rsel == 0 ? my : myp_last;
-      const bool rok = yrow >= 0 && ke >= 0;
-      const long long base = (long long)ke * plane + (long long)(yrow < 0 ? 0 : yrow) * nx;
+    for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
+  };
+  // E(ke) rows into E slot E (ke < 0: zeros); H(kh), cb(kh) rows into HB slot H (H null: none)
+  auto issue = [&](T *E, int ke, T *H, int kh) {
+    const long long pe = ke >= 0 ? (long long)ke * plane : -1;
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        T *dst = E + ((size_t)c * ER + r) * EW + VEC * lane;
-        const bool ok = rok && mxb >= 0;
-        const T *src = ok ? A.e_in + c * N + base + mxb : dummy;
-#pragma unroll
-        for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
-        if (lane == 0) {
-          const bool oka = rok && mxa >= 0;
-          const T *srca = oka ? A.e_in + c * N + base + mxa : dummy;
-          T *dsta = E + ((size_t)c * ER + r) * EW + ROW;
-#pragma unroll
-          for (int q = 0; q < VEC / CH; q++) cp_async16(dsta + q * CH, srca + q * CH, oka);
-        }
+    for (int c = 0; c < 3; c++) {
+      const T *f = A.e_in + c * N;
+      chunk(E + c * ER * EW + erow, f, off_e0, pe);
+      if (lane == 0) chunk(E + (c * ER + w) * EW + ROW, f, off_ea0, pe);
+      if (last_warp) {
+        chunk(E + (c * ER + RW + 1) * EW + VEC * lane, f, off_e1, pe);
+        if (lane == 0) chunk(E + (c * ER + RW + 1) * EW + ROW, f, off_ea1, pe);
       }
     }
-    if (hslot >= 0) {
-      T *H = sHB + (size_t)hslot * S::HB_SLOT;
-      const bool ok = my >= 0 && mxb >= 0 && kh >= 0;
-      const long long at = (long long)(kh < 0 ? 0 : kh) * plane + rowoff + (mxb < 0 ? 0 : mxb);
+    if (H) {
+      const long long ph = kh >= 0 ? (long long)kh * plane : -1;
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        T *dst = H + ((size_t)c * WARPS + w) * ROW + VEC * lane;
-        const T *src = ok ? A.h_in + c * N + at : dummy;
-#pragma unroll
-        for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
-      }
+      for (int c = 0; c < 3; c++) chunk(H + c * WARPS * ROW + hrow, A.h_in + c * N, off_h, ph);
       if (w >= 1) {
         T *B = H + 3 * WARPS * ROW;
-        const bool okb = ok && gy < ny;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          T *dst = B + ((size_t)c * RW + (w - 1)) * ROW + VEC * lane;
-          const T *src = okb ? A.cb + c * N + at : dummy;
-#pragma unroll
-          for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, okb);
-        }
+        for (int c = 0; c < 3; c++) chunk(B + c * RW * ROW + brow, A.cb + c * N, off_b, ph);
       }
     }
     cp_async_commit();
   };
-  auto Erow = [&](int slot, int c, int r) -> const T * {
-    return sEs + (size_t)slot * S::E_SLOT + ((size_t)c * ER + r) * EW;
-  };
-  auto Hrow = [&](int slot, int c) -> const T * {
-    return sHB + (size_t)slot * S::HB_SLOT + ((size_t)c * WARPS + w) * ROW;
-  };
-  auto Brow = [&](int slot, int c) -> const T * {
-    return sHB + (size_t)slot * S::HB_SLOT + 3 * WARPS * ROW + ((size_t)c * RW + (w - 1)) * ROW;
+  // the slots as pointers, turned round as the planes go by: E(k), E(k+1) and the one being
+  // filled (E(k+2)); H and cb of plane k and the one being filled
+  T *e_cur = sEs, *e_next = sEs + S::E_SLOT, *e_fill = sEs + 2 * S::E_SLOT;
+  T *hb_cur = sHB, *hb_fill = sHB + S::HB_SLOT;
+  auto Erow = [&](const T *slot, int c, int r) -> const T * { return slot + (c * ER + r) * EW; };
+  auto Hrow = [&](const T *slot, int c) -> const T * { return slot + c * WARPS * ROW + w * ROW; };
+  auto Brow = [&](const T *slot, int c) -> const T * {
+    return slot + 3 * WARPS * ROW + c * RW * ROW + (w - 1) * ROW;
   };
 
   // H's new plane k at the lane's four places, from E(k) (E slot se), E(k+1) (slot se1), H(k)
   // (HB slot sh): the forward differences, then the slabs along x, y, z
-  auto compute_h = [&](int se, int se1, int sh, int k, bool write, T hn[3][4]) {
-    const int kn = wrap_index(k + 1, nz, A.periodic[2]);
-    const T fhz = A.fh[nx + ny + k];
+  auto compute_h = [&](const T *se, const T *se1, const T *sh, int k, T fhz, bool write,
+                       T hn[3][4]) {
     Vec4<T> e[3], eyp[2], ez1[2], ho[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -1582,14 +1617,13 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       ey_n = Erow(se, 1, w)[ROW];
       ez_n = Erow(se, 2, w)[ROW];
     }
-    const bool yb = myp >= 0;   // the row after exists (or wraps)
-    const bool zb = kn >= 0;    // the plane after exists (or wraps)
+    // a row or plane after beyond a wall was staged as zeros: no test needed here
     T dyEz[4], dzEy[4], dzEx[4], dxEz[4], dxEy[4], dyEx[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       T eyn = j < 3 ? e[1].v[j + 1] : ey_n, ezn = j < 3 ? e[2].v[j + 1] : ez_n;
-      T exy = yb ? eyp[0].v[j] : T(0), ezy = yb ? eyp[1].v[j] : T(0);
-      T exz = zb ? ez1[0].v[j] : T(0), eyz = zb ? ez1[1].v[j] : T(0);
+      T exy = eyp[0].v[j], ezy = eyp[1].v[j];
+      T exz = ez1[0].v[j], eyz = ez1[1].v[j];
       dyEz[j] = ezy - e[2].v[j];
       dzEy[j] = eyz - e[1].v[j];
       dzEx[j] = exz - e[0].v[j];
@@ -1615,10 +1649,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       const T nocb[3][4] = {};
       cpml4<T, 1>(A, k, my, mxb, sxl, xmixed, inx, zs, sy, ow, hn, diff, nocb, sXC + VEC * lane);
     }
-    // beyond a wall H is zero (E's back differences read zero there)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      if (!hv[j]) hn[0][j] = hn[1][j] = hn[2][j] = T(0);
+    // beyond a wall H comes out zero (E's back differences read zero there): its E and H were
+    // staged as zeros and its kappa/h is zero, so every term above is +0
     // the magnetic currents at this tile and plane, each value's entries in CPU order
     const int bucket = tile * nz + k;
     const int g0 = hcur ? A.hbucket[bucket] : 0, g1 = hcur ? A.hbucket[bucket + 1] : 0;
@@ -1649,12 +1681,12 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   // prologue: H's new plane kbeg-1 (wrapped on a periodic z)
   const int km = wrap_index(kbeg - 1, nz, A.periodic[2]);
   // positions: E slots by position p = plane - kbeg + 1 (km at 0), HB slots alike
-  issue(0, km, 0, km);                                   // E(km), H(km), cb(km)
-  issue(1, kbeg, -1, -1);                                // E(kbeg)
+  issue(e_cur, km, hb_cur, km);                          // E(km), H(km), cb(km)
+  issue(e_next, kbeg, nullptr, -1);                      // E(kbeg)
   if (km >= 0) {
     cp_async_wait<0>();
     __syncthreads();
-    compute_h(0, 1, 0, km, false, hn);
+    compute_h(e_cur, e_next, hb_cur, km, A.fh[nx + ny + km], false, hn);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       hprev[0][j] = hn[0][j];
@@ -1665,15 +1697,69 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     for (int j = 0; j < 4; j++) hprev[0][j] = hprev[1][j] = T(0);
   }
   __syncthreads();
-  // plane kbeg's H and cb, and E(kbeg+1)
-  issue(2, wrap_index(kbeg + 1, nz, A.periodic[2]), 1, kbeg);
+  // plane kbeg's H and cb, and E(kbeg+1); then the slots move on one plane: E(kbeg) current
+  issue(e_fill, wrap_index(kbeg + 1, nz, A.periodic[2]), hb_fill, kbeg);
+  {
+    T *t = e_cur;
+    e_cur = e_next;
+    e_next = e_fill;
+    e_fill = t;
+    t = hb_cur;
+    hb_cur = hb_fill;
+    hb_fill = t;
+  }
+  // kappa/h along z at plane k, read a plane ahead
+  T fhz = A.fh[nx + ny + kbeg], fez = A.fe[nx + ny + kbeg];
+  // the CPML's psi rows of this warp's row at plane kp into L2 (one thread a row): read from
+  // memory a plane later, they then come from L2 rather than DRAM
+  const int pf0 = max(x0 - VEC, 0), pf1 = min(x0 + OWNX, nx);
+  auto prefetch_psi = [&](int kp) {
+    const bool zsp = !A.periodic[2] && (kp < A.low[2] || kp >= nz - A.high[2]);
+    const int zside = kp < A.low[2] ? 0 : 1;
+    const unsigned row = (unsigned)((pf1 - pf0) * (int)sizeof(T));
+#pragma unroll
+    for (int f = 0; f < 2; f++) {
+      const T *base = f == 1 ? A.psi_h_in : A.psi_e;
+      if (sy >= 0) {
+#pragma unroll
+        for (int c = 0; c < 3; c += 2) {  // x and z along y
+          const SlabEntry &sl = A.slab[f][c][1][sy];
+          if (sl.count)
+            prefetch_l2(base + sl.psi + ((long long)kp * sl.count + (my - sl.from)) * nx + pf0, row);
+        }
+      }
+      if (zsp) {
+#pragma unroll
+        for (int c = 0; c < 2; c++) {  // x and y along z
+          const SlabEntry &sl = A.slab[f][c][2][zside];
+          if (sl.count)
+            prefetch_l2(base + sl.psi + (long long)(kp - sl.from) * plane + (long long)my * nx + pf0,
+                        row);
+        }
+      }
+      if (xco) {
+        int p0, P;
+        const int side = xslab_places(A, x0, p0, P);
+#pragma unroll
+        for (int c = 1; c < 3; c++) {  // y and z along x
+          const SlabEntry &sl = A.slab[f][c][0][side];
+          if (sl.count)
+            prefetch_l2(base + sl.psi + ((long long)kp * ny + my) * sl.pw,
+                        (unsigned)(sl.pw * (int)sizeof(T)));
+        }
+      }
+    }
+  };
   for (int k = kbeg; k < kend; k++) {
-    const int p = k - kbeg + 1;
-    const int se = p % 3, se1 = (p + 1) % 3, sh = p % 2;
+    const T fhz_next = k + 1 < kend ? A.fh[nx + ny + k + 1] : T(0);
+    const T fez_next = k + 1 < kend ? A.fe[nx + ny + k + 1] : T(0);
     cp_async_wait<0>();
     __syncthreads();  // plane k's rows landed; every warp is done with plane k-1
-    if (k + 1 < kend) issue((p + 2) % 3, wrap_index(k + 2, nz, A.periodic[2]), (p + 1) % 2, k + 1);
-    compute_h(se, se1, sh, k, true, hn);
+    if (k + 1 < kend) {
+      issue(e_fill, wrap_index(k + 2, nz, A.periodic[2]), hb_fill, k + 1);
+      if (lane == 0 && rowh && pf1 > pf0) prefetch_psi(k + 1);
+    }
+    compute_h(e_cur, e_next, hb_cur, k, fhz, true, hn);
     // H's tile to memory, H_x and H_z to the row below
     const long long at = (long long)k * plane + rowoff + (mxb < 0 ? 0 : mxb);
     // the lossy form's ca of E's plane k, read now so that the barrier below covers the wait
@@ -1703,16 +1789,14 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
     __syncthreads();
     // E's plane k at the owned places: back differences, then the slabs
-    const T fez = A.fe[nx + ny + k];
-    const bool zb = wrap_index(k - 1, nz, A.periodic[2]) >= 0;
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
     T en[3][4];
     if (w >= 1) {
       Vec4<T> e[3], cb[3], hxm, hzm;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        e[c] = ld4(Erow(se, c, w) + VEC * lane);
-        cb[c] = ld4(Brow(sh, c) + VEC * lane);
+        e[c] = ld4(Erow(e_cur, c, w) + VEC * lane);
+        cb[c] = ld4(Brow(hb_cur, c) + VEC * lane);
       }
       hxm = ld4(sX + (size_t)(w - 1) * ROW + VEC * lane);  // the row before
       hzm = ld4(sX + (size_t)(WARPS + w - 1) * ROW + VEC * lane);
@@ -1723,7 +1807,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         T hzx = j > 0 ? hn[2][j - 1] : hz_p, hyx = j > 0 ? hn[1][j - 1] : hy_p;
-        T hyz = zb ? hprev[1][j] : T(0), hxz = zb ? hprev[0][j] : T(0);
+        // H's plane before: the prologue's (zeros below a wall) or the last iteration's
+        T hyz = hprev[1][j], hxz = hprev[0][j];
         dyHz[j] = hn[2][j] - hzm.v[j];
         dzHy[j] = hn[1][j] - hyz;
         dzHx[j] = hn[0][j] - hxz;
@@ -1782,41 +1867,6 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
               }
         }
       }
-      // the dispersive media's ADE currents (src/fdtd/media.rs:661-705), last, in the same pass:
-      // only tiles and planes that hold members look their values' member numbers up
-      if (MEDIA && any_own && A.media.tileplane[(long long)tile * nz + k]) {
-        int4 mq[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-          mq[c] = __ldg(reinterpret_cast<const int4 *>(A.media.member + c * N + at));
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            if (!ownv[j]) continue;
-            const int mi = j == 0 ? mq[c].x : (j == 1 ? mq[c].y : (j == 2 ? mq[c].z : mq[c].w));
-            if (mi < 0) continue;
-            const MediaArgs<T> &M = A.media;
-            int g = M.group[mi];
-            int np = M.gpoles[g];
-            T before = M.before[mi];
-            T rest = M.gchi[g] * before;
-            const T *pl = M.gpole + (long long)g * M.maxpoles * 3;
-            T *cur = M.current + (long long)mi * M.maxpoles;
-            T *prev = M.previous + (long long)mi * M.maxpoles;
-            for (int q = 0; q < np; q++)
-              rest = rest - T(0.5) * ((pl[3 * q] + T(1)) * cur[q] + pl[3 * q + 1] * prev[q]);
-            T next = en[c][j] + M.scale[mi] * rest;
-            T slope = (next - before) / M.two_dt;
-            for (int q = 0; q < np; q++) {
-              T jn = pl[3 * q] * cur[q] + pl[3 * q + 1] * prev[q] + pl[3 * q + 2] * slope;
-              prev[q] = cur[q];
-              cur[q] = jn;
-            }
-            M.before[mi] = e[c].v[j];
-            en[c][j] = next;
-          }
-      }
       if (lane >= 1 && rowh && mxb >= 0 && xb < nx) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -1832,6 +1882,15 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       hprev[0][j] = hn[0][j];
       hprev[1][j] = hn[1][j];
     }
+    fhz = fhz_next;
+    fez = fez_next;
+    T *t = e_cur;  // the slots move on one plane
+    e_cur = e_next;
+    e_next = e_fill;
+    e_fill = t;
+    t = hb_cur;
+    hb_cur = hb_fill;
+    hb_fill = t;
   }
   cp_async_wait<0>();
 }
@@ -2273,14 +2332,11 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       kernel<<<grid, quad::THREADS, smem, c->stream>>>(A);
     };
-    // the media's ADE fused in (MEDIA): one launch a step
-    if (c->media) {
-      if (c->lossless) go(quad_kernel<T, false, true>);
-      else go(quad_kernel<T, true, true>);
-    } else {
-      if (c->lossless) go(quad_kernel<T, false, false>);
-      else go(quad_kernel<T, true, false>);
-    }
+    // media: the step (its E update without them), then their pass over the members
+    if (c->lossless) go(quad_kernel<T, false>);
+    else go(quad_kernel<T, true>);
+    if (c->media)
+      ade_kernel<T><<<(unsigned)((A.media.members + 255) / 256), 256, 0, c->stream>>>(A);
     return;
   }
   if (c->row) {
@@ -2484,7 +2540,7 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
       } else {
         launch_step<T>(c, A);
       }
-      c->launches += 1;
+      c->launches += (c->quad && c->media) ? 2 : 1;
       c->parity = 1 - c->parity;
       long long gathered = c->nvalues + c->nprobes;
       if (gathered > 0) {
@@ -3124,9 +3180,10 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
     }
   }
   std::sort(all.begin(), all.end(), [](const In &a, const In &b) { return a.at < b.at; });
+  for (long long m = 1; m < members; m++)
+    if (all[m].at == all[m - 1].at) return fail(c, FDTD_E_INVALID, "a value is in two media");
   std::vector<long long> place(members);
   for (long long m = 0; m < members; m++) {
-    if (member[all[m].at] >= 0) return fail(c, FDTD_E_INVALID, "a value is in two media");
     member[all[m].at] = (int)m;
     group[m] = all[m].g;
     scale[m] = all[m].scale;
@@ -3155,21 +3212,6 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
   CUDA_TRY(c, cudaMemsetAsync(d_before, 0, members * E, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(d_cur, 0, members * maxp * E, c->stream));
   CUDA_TRY(c, cudaMemsetAsync(d_prev, 0, members * maxp * E, c->stream));
-  // the quad kernel's (tile, plane) flags
-  void *d_tileplane = nullptr;
-  if (c->quad) {
-    const long long nxy = (long long)c->n[0] * c->n[1];
-    std::vector<unsigned char> tp((size_t)c->tiles_x * c->tiles_y * c->n[2], 0);
-    for (long long m = 0; m < members; m++) {
-      const long long r = place[m] % c->N;
-      const int i = (int)(r % c->n[0]), j = (int)((r / c->n[0]) % c->n[1]);
-      const int k = (int)(r / nxy);
-      const long long tile = (long long)(j / quad::RW) * c->tiles_x + i / quad::OWNX;
-      tp[(size_t)(tile * c->n[2] + k)] = 1;
-    }
-    if (int r = alloc(c, &d_tileplane, tp.size())) return r;
-    CUDA_TRY(c, copy(c, d_tileplane, tp.data(), tp.size(), cudaMemcpyHostToDevice));
-  }
   auto fillm = [&](auto &M) {
     using T = typename std::remove_pointer<decltype(M.scale)>::type;
     using TT = typename std::remove_const<T>::type;
@@ -3187,7 +3229,6 @@ int fdtd_set_media(fdtd_ctx *c, int32_t ngroups, const fdtd_media_group *groups)
     M.two_dt = (TT)(2.0 * c->dt);
     M.place = (const long long *)d_place;
     M.members = members;
-    M.tileplane = (const unsigned char *)d_tileplane;
   };
   if (c->precision == 64) fillm(c->md);
   else fillm(c->mf);

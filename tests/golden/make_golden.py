@@ -8,7 +8,8 @@ counts on the host's cores and keeps the results the parity tests compare the CU
   after 20 000 steps: both arms' flux spectra at 51 wavelengths and the probe's time series.
 - ``dispersive_10000.npz``: the dispersive grid (256 x 256 x 128, Drude and two-pole Lorentz
   boxes, seed 7) after 10 000 steps: the probe's time series and the final E_z plane through the
-  source.
+  source; ``dispersive_10000_f32.npz`` the same from the oracle's f32 arithmetic
+  (``dispersive32``).
 
 Each takes tens of minutes on 8 host threads; the fixtures are small (the spectra and series).
 """
@@ -43,19 +44,22 @@ def mmi():
     print(f"mmi: {info['steps']} steps in {seconds:.0f} s", flush=True)
 
 
-def dispersive():
-    s, info = configs.dispersive_3d(oracle, 7)
+def dispersive(precision=64):
+    s, info = configs.dispersive_3d(
+        lambda *a, **kw: OracleSimulation(*a, **{**kw, "precision": precision}), 7)
     t0 = time.perf_counter()
     s.run(info["steps"])
     seconds = time.perf_counter() - t0
     g = s.grid
     ez = s.e(2).reshape(g.nz, g.ny, g.nx)[g.nz // 2]
-    np.savez_compressed(os.path.join(HERE, "dispersive_10000.npz"), probe=s.probe(info["probe"]),
+    name = "dispersive_10000.npz" if precision == 64 else "dispersive_10000_f32.npz"
+    np.savez_compressed(os.path.join(HERE, name), probe=s.probe(info["probe"]),
                         ez_mid=ez, steps=info["steps"], seconds=seconds)
-    print(f"dispersive: {info['steps']} steps in {seconds:.0f} s", flush=True)
+    print(f"dispersive (f{precision}): {info['steps']} steps in {seconds:.0f} s", flush=True)
 
 
 if __name__ == "__main__":
     which = sys.argv[1:] or ["mmi", "dispersive"]
     for name in which:
-        {"mmi": mmi, "dispersive": dispersive}[name]()
+        {"mmi": mmi, "dispersive": dispersive,
+         "dispersive32": lambda: dispersive(32)}[name]()
