@@ -1290,6 +1290,73 @@ int orc_medium_stable(double eps_inf, int npoles, const double *poles, double si
   return stable(ps, eps_inf, sigma, dt, top) ? 1 : 0;
 }
 
+int orc_dft_value(const orc_sim *s, int monitor, int field, int comp, const long at[3], int f,
+                  double *out) {
+  return with(s, [&](auto &x) -> int {
+    if (monitor < 0 || monitor >= (int)x.dfts.size()) return 0;
+    c64 v;
+    if (!x.dfts[monitor].value(field, comp, at, f, &v)) return 0;
+    out[0] = v.real();
+    out[1] = v.imag();
+    return 1;
+  });
+}
+
+long orc_flux_derivatives(const orc_sim *s, int monitor, int f, double scale, long *keys,
+                          double *values, long capacity) {
+  // the derivative of flux monitor `monitor`'s flux at frequency f with respect to each
+  // transform it reads, times scale (src/fdtd/adjoint.rs:1036-1083, flux_derivatives, each face
+  // with its sign): the flux is the sum of w sign Re(1/2 (low + high) conj(H)) area, so with
+  // kappa = scale w sign area / 2 the derivative is kappa conj(H) / 2 at each of the two E
+  // planes and kappa conj(low + high) / 2 at H. Entries (field, component, index) in keys[3q],
+  // the complex derivative in values[2q]. Returns the count (keys may be null to ask).
+  return with(s, [&](auto &x) -> long {
+    if (monitor < 0 || monitor >= (int)x.fluxes.size()) return -1;
+    const Flux &fl = x.fluxes[monitor];
+    const Grid &g = x.g;
+    long n = 0;
+    auto put = [&](int field, int comp, const long at[3], c64 v) {
+      if (keys && n < capacity) {
+        keys[3 * n] = field;
+        keys[3 * n + 1] = comp;
+        keys[3 * n + 2] = (at[2] * g.n[1] + at[1]) * g.n[0] + at[0];
+        values[2 * n] = v.real();
+        values[2 * n + 1] = v.imag();
+      }
+      n++;
+    };
+    for (size_t face = 0; face < fl.planes.size(); face++) {
+      const FluxPlane &pl = fl.planes[face];
+      const Dft &dft = fl.dfts[face];
+      const int b = first_of(pl.axis), c = second_of(pl.axis);
+      const double area = g.d[b] * g.d[c];
+      struct T3 { int comp, h; double sign; };
+      const T3 terms[2] = {{b, c, 0.5}, {c, b, -0.5}};
+      for (const T3 &t : terms)
+        for (long v = pl.range_lo(g, c); v < pl.range_hi(g, c); v++)
+          for (long u = pl.range_lo(g, b); u < pl.range_hi(g, b); u++) {
+            const double w = pl.weight(b, u, t.comp == b) * pl.weight(c, v, t.comp == c);
+            if (w == 0.0) continue;
+            const double kappa = scale * fl.signs[face] * w * t.sign * 0.5 * area;
+            long at[3];
+            at[pl.axis] = pl.plane;
+            at[b] = u;
+            at[c] = v;
+            c64 hv, low, high;
+            dft.value(1, t.h, at, f, &hv);
+            dft.value(0, t.comp, at, f, &low);
+            long at2[3] = {at[0], at[1], at[2]};
+            at2[pl.axis] = pl.plane + 1;
+            dft.value(0, t.comp, at2, f, &high);
+            put(0, t.comp, at, 0.5 * kappa * std::conj(hv));
+            put(0, t.comp, at2, 0.5 * kappa * std::conj(hv));
+            put(1, t.h, at, 0.5 * kappa * std::conj(low + high));
+          }
+    }
+    return n;
+  });
+}
+
 double orc_triad(long len, int repeats) {
   // the STREAM triad as the reference measures its host's bandwidth (src/traffic.rs:56-80):
   // a = b + s c over `len` doubles on all threads, the best of `repeats`, 24 bytes an element

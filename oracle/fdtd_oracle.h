@@ -85,6 +85,15 @@ int orc_medium_stable(double eps_inf, int npoles, const double *poles, double si
 /* The STREAM triad a = b + s c over len doubles on all OpenMP threads, the best of `repeats`
  * runs, in GB/s at 24 bytes an element (the reference's traffic::triad, src/traffic.rs:56-80). */
 double orc_triad(long len, int repeats);
+/* Transform monitor `monitor`'s sum for (field, comp) at grid index at[3], frequency f: out[2]
+ * (re, im); 1 if the monitor holds that value, else 0. */
+int orc_dft_value(const orc_sim *s, int monitor, int field, int comp, const long at[3], int f,
+                  double *out);
+/* d(flux of monitor at frequency f)/d(each transform it reads) x scale, as the reference's
+ * adjoint takes it (src/fdtd/adjoint.rs:1036-1083): keys[3q] = (field, comp, index), values[2q] the
+ * complex derivative. Returns the count (keys null to ask), -1 for no such monitor. */
+long orc_flux_derivatives(const orc_sim *s, int monitor, int f, double scale, long *keys,
+                          double *values, long capacity);
 
 #ifdef __cplusplus
 }

@@ -153,14 +153,15 @@ def psi_values(grid: Grid3d, boundaries: Boundaries) -> int:
 
 
 def te_design(nx: int, ny: int, precision: int = 32, steps: int = 6000, segment: int = 500,
-              design_cells: int = 100, h: float = 0.02, bandwidth: float = 0.3):
+              design_cells: int = 100, h: float = 0.02, bandwidth: float = 0.3, cls=None):
     """Configuration 4, one instance: a 2D TE grid of nx x ny cells of 20 nm, 12-cell CPMLs, an
     input Si strip (0.5 um) from the left CPML into a design region of design_cells^2 cells at
     the centre and an output strip from it to the right CPML, all in SiO2. A Gaussian-profile
     current on E_y across the input strip carries a pulse centred on 1550 nm (``bandwidth`` c/um
     wide, so that it has passed within the run); flux monitor 0 sits across the output strip
     (the arm) at 1550 nm. Returns the adjoint's TeProblem (design permittivities
-    eps in [1.444^2, 3.48^2] are the variables)."""
+    eps in [1.444^2, 3.48^2] are the variables); ``cls`` the simulation class its builder makes
+    (the engine's by default)."""
     from .adjoint import Design2d, TeProblem
     from .fdtd import Simulation, average
 
@@ -178,7 +179,7 @@ def te_design(nx: int, ny: int, precision: int = 32, steps: int = 6000, segment:
     span = int(round(1.0 / h))  # the monitor's window: 1 um either side of the strip
 
     def build(eps, prec):
-        s = Simulation(g, eps, Boundaries.cpml_2d(12), 0.5, precision=prec)
+        s = (cls or Simulation)(g, eps, Boundaries.cpml_2d(12), 0.5, precision=prec)
         values = []
         for j in range(jc - 25, jc + 26):
             y = (j + 0.5 - ny / 2) * h
