@@ -85,6 +85,12 @@ double pxs_dt(const pxs_sim *s);
 int64_t pxs_steps(const pxs_sim *s);
 /* Simulation::time (src/fdtd.rs:887-889): steps x dt */
 double pxs_time(const pxs_sim *s);
+/* Waveform::spectrum (src/fdtd.rs:361-396): the sum over n < steps of w.at(t_n) e^(i omega t_n)
+ * dt, t_n = n dt, plus dt/2 for E (field 0), at each of nf frequencies (c/um), with the
+ * reference's exp and sin/cos; out: nf complex, interleaved. waveform = {kind, p[0..4]} as
+ * fdtd_waveform. What an FDTD job divides a dipole run's fluxes by (src/job/fdtd.rs:2248-2318). */
+int pxs_waveform_spectrum(const double waveform[6], int32_t field, double dt, int64_t steps,
+                          int32_t nf, const double *freqs, double *out);
 /* Simulation::run_until (src/fdtd.rs:1161-1167) */
 int pxs_run_until(pxs_sim *s, double time);
 /* Simulation::run_until_decayed (src/fdtd/monitors.rs:742-838): *decayed 1 when the probes'

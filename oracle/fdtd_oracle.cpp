@@ -1375,4 +1375,25 @@ double orc_triad(long len, int repeats) {
   return 24.0 * (double)len / best / 1e9;
 }
 
+// Waveform::spectrum (src/fdtd.rs:361-396): the sum from zero, in step order, of
+// (w.at(t) + 0i) exp(i omega t) dt with t = n dt (+ dt/2 for E, field 0).
+int orc_waveform_spectrum(const double *wave, int field, double dt, long steps, int nf,
+                          const double *freqs, double *out) {
+  if (!wave || !freqs || !out || nf < 0 || steps < 0 || !(dt > 0.0)) return -1;
+  const Wave w = Wave::from(wave);
+  const double offset = field == 0 ? 0.5 * dt : 0.0;
+  for (int f = 0; f < nf; f++) {
+    const double omega = TAU * freqs[f];
+    c64 sum(0.0, 0.0);
+    for (long n = 0; n < steps; n++) {
+      const double t = (double)n * dt + offset;
+      const c64 v = cmul(c64(w.at(t), 0.0), cis(omega * t));
+      sum = c64(sum.real() + v.real() * dt, sum.imag() + v.imag() * dt);
+    }
+    out[2 * f] = sum.real();
+    out[2 * f + 1] = sum.imag();
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -85,6 +85,9 @@ int orc_medium_stable(double eps_inf, int npoles, const double *poles, double si
 /* The STREAM triad a = b + s c over len doubles on all OpenMP threads, the best of `repeats`
  * runs, in GB/s at 24 bytes an element (the reference's traffic::triad, src/traffic.rs:56-80). */
 double orc_triad(long len, int repeats);
+/* Waveform::spectrum (src/fdtd.rs:361-396) at nf frequencies: out nf complex, interleaved. */
+int orc_waveform_spectrum(const double *wave, int field, double dt, long steps, int nf,
+                          const double *freqs, double *out);
 /* Transform monitor `monitor`'s sum for (field, comp) at grid index at[3], frequency f: out[2]
  * (re, im); 1 if the monitor holds that value, else 0. */
 int orc_dft_value(const orc_sim *s, int monitor, int field, int comp, const long at[3], int f,

@@ -74,6 +74,7 @@ def lib():
         x.orc_medium_stable.argtypes = [D, C.c_int, DP, D, D, D]
         x.orc_triad.argtypes = [L, C.c_int]
         x.orc_triad.restype = D
+        x.orc_waveform_spectrum.argtypes = [DP, C.c_int, D, L, C.c_int, DP, DP]
         _lib = x
     return _lib
 
@@ -286,3 +287,14 @@ def medium_stable(medium: Dispersive, sigma: float, dt: float, top: float) -> bo
 def triad(length: int = 1 << 26, repeats: int = 5) -> float:
     """The host's STREAM triad bandwidth, GB/s, as the reference measures it (src/traffic.rs)."""
     return float(lib().orc_triad(int(length), int(repeats)))
+
+
+def waveform_spectrum(waveform, field, dt: float, steps: int, frequencies) -> np.ndarray:
+    """``Waveform::spectrum`` (src/fdtd.rs:361-396) at each frequency: complex."""
+    w, wp = _d(waveform.as_array())
+    f, fp = _d(np.asarray(frequencies, dtype=np.float64).reshape(-1))
+    out = np.zeros(2 * f.size)
+    if lib().orc_waveform_spectrum(wp, int(field), float(dt), int(steps), f.size, fp,
+                                   out.ctypes.data_as(DP)) != 0:
+        raise InvalidValue("a waveform's spectrum needs dt > 0 and steps >= 0")
+    return out[0::2] + 1j * out[1::2]

@@ -731,7 +731,56 @@ struct pxs_sim {
   }
 };
 
+// Waveform::at (src/fdtd.rs:399-424), a point source's value at t, with the reference's exp and
+// sin/cos: w = {kind, p[0..4]} as fdtd_waveform holds it.
+double waveform_at(const double w[6], double t) {
+  const double TAU = 6.283185307179586476925286766559;
+  const double *p = w + 1;
+  if (w[0] == 0.0) {
+    const double u = (t - p[2]) / p[1];
+    double s, c;
+    pxp::sincos((TAU * p[0]) * (t - p[2]), &s, &c);
+    return pxp::exp(-u * u) * s;
+  }
+  if (w[0] == 1.0) {
+    const double u = (t - p[1]) / p[0];
+    return -u * pxp::exp(-u * u) * std::sqrt(2.0 * 2.718281828459045235);
+  }
+  double ss = 1.0;
+  if (p[3] > 0.0) {
+    const double r = std::min(std::max(t / p[3], 0.0), 1.0);
+    ss = r * r * (3.0 - 2.0 * r);
+  }
+  double s, c;
+  pxp::sincos(-(TAU * p[0]) * t, &s, &c);
+  return ss * (p[1] * c - p[2] * s);
+}
+
 extern "C" {
+
+int pxs_waveform_spectrum(const double waveform[6], int32_t field, double dt, int64_t steps,
+                          int32_t nf, const double *freqs, double *out) {
+  if (!waveform || !freqs || !out || nf < 0 || steps < 0 || !(dt > 0.0)) return FDTD_E_INVALID;
+  const double TAU = 6.283185307179586476925286766559;
+  const double offset = field == 0 ? 0.5 * dt : 0.0;
+  for (int32_t f = 0; f < nf; f++) {
+    const double omega = TAU * freqs[f];
+    // the sum from zero, in step order: (v + 0i)(cos + i sin) dt, as num-complex multiplies
+    double re = 0.0, im = 0.0;
+    for (int64_t n = 0; n < steps; n++) {
+      const double t = (double)n * dt + offset;
+      const double v = waveform_at(waveform, t);
+      const double x = omega * t;
+      double s = 0.0, c = 1.0;
+      if (x != 0.0) pxp::sincos(x, &s, &c);
+      re += (v * c - 0.0 * s) * dt;
+      im += (v * s + 0.0 * c) * dt;
+    }
+    out[2 * f] = re;
+    out[2 * f + 1] = im;
+  }
+  return 0;
+}
 
 int pxs_average(const int64_t n[3], const double d[3], const double o[3], const pxs_geometry *gm,
                 double *out) {

@@ -86,6 +86,7 @@ def library():
         x.pxs_time.restype = D
         x.pxs_run_until.argtypes = [P, D]
         x.pxs_run_until_decayed.argtypes = [P, I32, I32P, D, D, D, I32P, DP]
+        x.pxs_waveform_spectrum.argtypes = [DP, I32, D, I64, I32, DP, DP]
         x.pxs_engine.restype = P
         _lib = x
     return _lib
@@ -129,6 +130,20 @@ def average(grid: Grid3d, geometry: Boxes, device: bool = False) -> np.ndarray:
     else:
         x.pxs_average(keep[0][1], keep[1][1], keep[2][1], C.byref(geo), out.ctypes.data_as(DP))
     return out.reshape(3, -1)
+
+
+def waveform_spectrum(waveform, field, dt: float, steps: int, frequencies) -> np.ndarray:
+    """``Waveform::spectrum`` (``src/fdtd.rs:361-396``): sum over n < steps of w(t_n)
+    e^(i omega t_n) dt, t_n = n dt (+ dt/2 for E), at each frequency (c/um), with the
+    reference's exp and sin/cos; complex, one per frequency."""
+    w, wp = _d(waveform.as_array())
+    f, fp = _d(np.asarray(frequencies, dtype=np.float64).reshape(-1))
+    out = np.zeros(2 * f.size)
+    code = library().pxs_waveform_spectrum(wp, int(field), float(dt), int(steps), f.size, fp,
+                                           out.ctypes.data_as(DP))
+    if code != 0:
+        raise InvalidValue(f"a waveform's spectrum needs dt > 0 and steps >= 0 ({code})")
+    return out[0::2] + 1j * out[1::2]
 
 
 class Simulation:
