@@ -41,6 +41,15 @@ int pxs_average(const int64_t n[3], const double d[3], const double o[3], const 
  * (src/fdtd.rs:583-594). Returns 0, -1 for bad sizes, -2 for a CUDA error. */
 int pxs_average_device(const int64_t n[3], const double d[3], const double o[3],
                        const pxs_geometry *g, double *out);
+/* The CPML's tables (Simulation::build_cpml, src/fdtd.rs:799-869) on the current CUDA device, one
+ * thread per node of each axis, the host library's functions so its bits: which 2 the kappa
+ * factors at the nodes over the step (sum of n), 3 at the half-steps, 4 the slabs (per slab its
+ * field, component, axis, first node, count, then b and a), as pxs_tables lays them out. Grid,
+ * edges and cpml as pxs_create, dt the time step. Returns the count (out NULL: the count alone,
+ * no device work), -1 for bad sizes, -2 for a CUDA error. */
+int64_t pxs_cpml_device(const int64_t n[3], const double d[3], const int32_t kind[3],
+                        const int64_t low[3], const int64_t high[3], const double cpml[5],
+                        double dt, int32_t which, double *out);
 
 /* Simulation::new / with_permittivity (src/fdtd.rs:570-796): grid n, d, origin o; kind[a] 0 a
  * CPML of low/high cells (0 = wall), 1 periodic; cpml = {reflection, sigma (NaN: from

@@ -25,6 +25,7 @@
 #include "photonoxide_batch.h"
 #include "portable.h"
 #include "average.cuh"
+#include "cpml.cuh"
 
 namespace {
 
@@ -264,25 +265,15 @@ struct pxs_sim {
 
   // Simulation::build_cpml (src/fdtd.rs:799-869)
   void build_cpml() {
-    double R = cpml[0], sig = cpml[1], order = cpml[2], kmax = cpml[3], alpha = cpml[4];
+    const double alpha = cpml[4];
     for (int axis = 0; axis < 3; axis++) {
       kn[axis].assign(g.n[axis], 1.0);
       kh[axis].assign(g.n[axis], 1.0);
       if (periodic(axis)) continue;
-      int64_t lo = low[axis], hi = high[axis], n = g.n[axis];
-      double hstep = g.d[axis];
-      auto profile = [&](double depth, int64_t cells, double &s, double &k) {
-        double d = (double)cells * hstep;
-        // the reference's powf and ln (portable.h), so that the grading is its bits
-        double x = pxp::pow(std::min(std::max(depth / (double)cells, 0.0), 1.0), order);
-        double smax = std::isnan(sig) ? (order + 1.0) * (-pxp::ln(R)) / (2.0 * d) : sig;
-        s = smax * x;
-        k = 1.0 + (kmax - 1.0) * x;
-      };
+      const int64_t lo = low[axis], hi = high[axis], n = g.n[axis];
+      // sigma and kappa by the reference's powf and ln (cpml.cuh, shared with the device)
       auto at = [&](double pos, double &s, double &k) {
-        if (lo > 0 && pos < (double)lo) profile((double)lo - pos, lo, s, k);
-        else if (hi > 0 && pos > (double)(n - hi)) profile(pos - (double)(n - hi), hi, s, k);
-        else { s = 0.0; k = 1.0; }
+        pxc::grade(pos, lo, hi, n, g.d[axis], cpml, &s, &k);
       };
       for (int64_t m = 0; m < n; m++) {
         double s, k;
@@ -301,12 +292,11 @@ struct pxs_sim {
           sl.from = froms[side];
           sl.count = counts[side];
           for (int64_t m = sl.from; m < sl.from + sl.count; m++) {
-            double s, k;
+            double s, k, b, a;
             at((double)m + (field == 0 ? 0.0 : 0.5), s, k);
-            double b = pxp::exp(-(s / k + alpha) * dt);
-            double den = s * k + k * k * alpha;
+            pxc::recursion(s, k, alpha, dt, &b, &a);
             sl.b.push_back(b);
-            sl.a.push_back((s > 0.0 && den > 0.0) ? s * (b - 1.0) / den : 0.0);
+            sl.a.push_back(a);
           }
           for (int comp : {first_of(axis), second_of(axis)}) {
             sl.comp = comp;

@@ -132,6 +132,28 @@ def average(grid: Grid3d, geometry: Boxes, device: bool = False) -> np.ndarray:
     return out.reshape(3, -1)
 
 
+def cpml_tables(grid: Grid3d, boundaries, dt: float, which: int) -> np.ndarray:
+    """The CPML's tables (``Simulation::build_cpml``, ``src/fdtd.rs:799-869``) made on the
+    current CUDA device, one thread per node, with the host library's functions (the same bits):
+    ``which`` 2 the kappa factors over the step at the nodes, 3 at the half-steps, 4 the slabs,
+    laid out as :meth:`Simulation.tables` lays them out."""
+    n, d, _ = grid.as_arrays()
+    kind, low, high = boundaries.as_arrays()
+    keep = [_i64(n), _d(d), _i32(kind), _i64(low), _i64(high), _d(boundaries.cpml.as_array())]
+    x = library()
+    x.pxs_cpml_device.argtypes = [I64P, DP, I32P, I64P, I64P, DP, D, I32, DP]
+    x.pxs_cpml_device.restype = I64
+    args = [k[1] for k in keep] + [float(dt), int(which)]
+    count = x.pxs_cpml_device(*args, None)
+    if count < 0:
+        raise InvalidValue(f"the CPML's tables need a grid and CPMLs that fit it ({count})")
+    out = np.empty(count)
+    code = x.pxs_cpml_device(*args, out.ctypes.data_as(DP))
+    if code != count:
+        raise GpuError(f"the CPML's tables on the device failed ({code})")
+    return out
+
+
 def waveform_spectrum(waveform, field, dt: float, steps: int, frequencies) -> np.ndarray:
     """``Waveform::spectrum`` (``src/fdtd.rs:361-396``): sum over n < steps of w(t_n)
     e^(i omega t_n) dt, t_n = n dt (+ dt/2 for E), at each frequency (c/um), with the
