@@ -294,6 +294,75 @@ struct Injection {  // a source or current value: field, component, index, ampli
   bool point;  // a point source takes w.at(t); a current Re(a w(t))
 };
 
+// Twice a value's position along `axis` in steps from node 0 (src/fdtd/sources.rs:155-162): a node
+// m is 2m, halfway after it 2m + 1; E's component is halfway along itself, H's along the others.
+inline long twice(int field, int comp, int axis, long m) {
+  const bool half = field == 0 ? comp == axis : comp != axis;
+  return 2 * m + (half ? 1 : 0);
+}
+
+// One coupling across a total-field/scattered-field surface (src/fdtd/sources.rs:138-153).
+struct Link {
+  int target, comp;
+  long r;
+  double weight;
+  int from_field, from_comp;
+  long from[3];
+};
+
+// A plane wave's run (src/fdtd/sources.rs:740-1041): its auxiliary 1D grid along the direction
+// (p, q, s), sample l at l = sum of g_a twice_a, and the couplings of its box.
+struct PlaneRun {
+  long g[3];
+  double steps[3];
+  long base = 0, pad = 0, len = 0;
+  std::vector<double> e[3], h[3], ca, cb, da, db;
+  struct Sheet { int c; long i; double j; };
+  std::vector<Sheet> sheet;
+  Wave wave;
+  struct Coupling { int c; long r; double w; int from; long i; };
+  std::vector<Coupling> on_e, on_h;
+
+  bool sample(int field, int comp, const long at[3], long *i) const {
+    long l = 0;
+    for (int a = 0; a < 3; a++) l += g[a] * twice(field, comp, a, at[a]);
+    const long q = l - base;
+    if (q < 0 || q >= len) return false;
+    *i = q;
+    return true;
+  }
+  double value(int field, int comp, const long at[3]) const {
+    long i;
+    if (!sample(field, comp, at, &i)) return 0.0;
+    return field == 0 ? e[comp][i] : h[comp][i];
+  }
+  double difference(const std::vector<double> &f, int axis, long i) const {
+    const long o = g[axis];
+    if (o == 0) return 0.0;
+    return (f[i + o] - f[i - o]) / steps[axis];
+  }
+  void step_h() {
+    for (int c = 0; c < 3; c++) {
+      const int a = first_of(c), b = second_of(c);
+      for (long i = pad; i < len - pad; i++) {
+        const double curl = difference(e[b], a, i) - difference(e[a], b, i);
+        h[c][i] = da[i] * h[c][i] - db[i] * curl;
+      }
+    }
+  }
+  void step_e(double half) {
+    for (int c = 0; c < 3; c++) {
+      const int a = first_of(c), b = second_of(c);
+      for (long i = pad; i < len - pad; i++) {
+        const double curl = difference(h[b], a, i) - difference(h[a], b, i);
+        e[c][i] = ca[i] * e[c][i] + cb[i] * curl;
+      }
+    }
+    const double w = wave.at(half);
+    for (const Sheet &q : sheet) e[q.c][q.i] -= cb[q.i] * q.j * w;
+  }
+};
+
 struct Base {
   virtual ~Base() {}
 };
@@ -323,6 +392,7 @@ struct Sim : Base {
   std::vector<Flux> fluxes;
   std::vector<Group<T>> groups;
   std::map<std::pair<int, long>, int> members;
+  std::vector<PlaneRun> plane_waves;
 
   long stride(int a) const { return a == 0 ? 1 : (a == 1 ? g.n[0] : g.n[0] * g.n[1]); }
   bool periodic(int a) const { return kind[a] == 1; }
@@ -579,6 +649,121 @@ struct Sim : Base {
     }
   }
 
+  // PlaneWaveRun::correct (src/fdtd/sources.rs:971-991): the box's corrections from the incident
+  // field now, in f64 as the reference; the f32 run rounds each correction to T.
+  void correct(const PlaneRun &p, int field) {
+    if (field == 0) {
+      for (const PlaneRun::Coupling &q : p.on_e) {
+        const double amount = (cb64[q.c][q.r] * q.w) * p.h[q.from][q.i];
+        e[q.c][q.r] = e[q.c][q.r] - (T)amount;
+      }
+    } else {
+      for (const PlaneRun::Coupling &q : p.on_h) {
+        const double amount = (dt64 * q.w) * p.e[q.from][q.i];
+        h[q.c][q.r] = h[q.c][q.r] - (T)amount;
+      }
+    }
+  }
+
+  // Simulation::links (src/fdtd/sources.rs:316-420): the couplings across a total-field /
+  // scattered-field surface among the values in region [lo, hi) per axis, total() saying which
+  // side each value is on; values held at zero (cb = 0) neither take nor give one.
+  template <typename F>
+  std::vector<Link> links(const long lo[3], const long hi[3], const F &total) const {
+    auto neighbour = [&](const long at[3], int axis, bool forward, long out[3]) -> bool {
+      for (int q = 0; q < 3; q++) out[q] = at[q];
+      const long n = g.n[axis];
+      if (forward) {
+        if (at[axis] + 1 < n) out[axis] += 1;
+        else if (periodic(axis)) out[axis] = 0;
+        else return false;
+      } else if (at[axis] > 0) {
+        out[axis] -= 1;
+      } else if (periodic(axis)) {
+        out[axis] = n - 1;
+      } else {
+        return false;
+      }
+      return true;
+    };
+    auto index = [&](const long at[3]) { return (at[2] * g.n[1] + at[1]) * g.n[0] + at[0]; };
+    auto held = [&](int comp, const long at[3]) { return cb64[comp][index(at)] == 0.0; };
+    std::vector<Link> out;
+    for (long k = lo[2]; k < hi[2]; k++)
+      for (long j = lo[1]; j < hi[1]; j++)
+        for (long i = lo[0]; i < hi[0]; i++) {
+          const long at[3] = {i, j, k};
+          const long r = index(at);
+          for (int c = 0; c < 3; c++) {
+            const int a = first_of(c), b = second_of(c);
+            struct Term { int comp; bool ok; long from[3]; double coefficient; };
+            if (!held(c, at)) {
+              const bool inside = total(0, c, at);
+              const double fa = kn64[a][at[a]] / g.d[a], fb = kn64[b][at[b]] / g.d[b];
+              Term terms[4];
+              terms[0] = {b, true, {i, j, k}, fa};
+              terms[1].comp = b;
+              terms[1].ok = neighbour(at, a, false, terms[1].from);
+              terms[1].coefficient = -fa;
+              terms[2] = {a, true, {i, j, k}, -fb};
+              terms[3].comp = a;
+              terms[3].ok = neighbour(at, b, false, terms[3].from);
+              terms[3].coefficient = fb;
+              for (const Term &q : terms) {
+                if (!q.ok) continue;
+                if (total(1, q.comp, q.from) != inside) {
+                  const double sign = inside ? -1.0 : 1.0;
+                  out.push_back(Link{0, c, r, sign * q.coefficient, 1, q.comp,
+                                     {q.from[0], q.from[1], q.from[2]}});
+                }
+              }
+            }
+            const bool inside = total(1, c, at);
+            const double fa = kh64[a][at[a]] / g.d[a], fb = kh64[b][at[b]] / g.d[b];
+            Term terms[4];
+            terms[0].comp = b;
+            terms[0].ok = neighbour(at, a, true, terms[0].from);
+            terms[0].coefficient = fa;
+            terms[1] = {b, true, {i, j, k}, -fa};
+            terms[2].comp = a;
+            terms[2].ok = neighbour(at, b, true, terms[2].from);
+            terms[2].coefficient = -fb;
+            terms[3] = {a, true, {i, j, k}, fb};
+            for (const Term &q : terms) {
+              if (!q.ok) continue;
+              if (held(q.comp, q.from)) continue;
+              if (total(0, q.comp, q.from) != inside) {
+                const double sign = inside ? 1.0 : -1.0;
+                out.push_back(Link{1, c, r, sign * q.coefficient, 0, q.comp,
+                                   {q.from[0], q.from[1], q.from[2]}});
+              }
+            }
+          }
+        }
+    return out;
+  }
+
+  // Simulation::uniform (src/fdtd/sources.rs:509-522): every value of E on the surface lossless
+  // in a medium of eps.
+  bool uniform(const std::vector<Link> &ls, double eps) const {
+    const double expected = dt64 / eps;
+    for (const Link &l : ls) {
+      int c;
+      long r;
+      if (l.target == 0) {
+        c = l.comp;
+        r = l.r;
+      } else {
+        c = l.from_comp;
+        r = (l.from[2] * g.n[1] + l.from[1]) * g.n[0] + l.from[0];
+      }
+      if (!(std::fabs(cb64[c][r] - expected) <= 1e-12 * expected && ca64[c][r] == 1.0 &&
+            members.find({c, r}) == members.end()))
+        return false;
+    }
+    return true;
+  }
+
   // Media::save / Media::update (src/fdtd/media.rs:661-705)
   void media_save() {
     for (Group<T> &gr : groups)
@@ -641,10 +826,18 @@ struct Sim : Base {
     curl_update(1);
     update_slabs(1);
     inject(1, t);
+    for (PlaneRun &p : plane_waves) {
+      correct(p, 1);
+      p.step_h();
+    }
     media_save();
     curl_update(0);
     update_slabs(0);
     inject(0, half);
+    for (PlaneRun &p : plane_waves) {
+      correct(p, 0);
+      p.step_e(half);
+    }
     media_update();
     steps += 1;
     for (Probe &p : probes)
@@ -1373,6 +1566,152 @@ double orc_triad(long len, int repeats) {
   volatile double sink = a[len / 2];
   (void)sink;
   return 24.0 * (double)len / best / 1e9;
+}
+
+// Simulation::add_plane_wave / PlaneWaveRun::new (src/fdtd/sources.rs:716-951): the box from
+// nodes low to high, the direction (p, q, s) in cells, E's polarization, the background's eps.
+// Returns the wave's number, or -1 with the reason in err.
+int orc_add_plane_wave(orc_sim *s, const long low[3], const long high[3], const long dir[3],
+                       const double pol[3], double eps, const double *wave, char *err,
+                       int errlen) {
+  return with(s, [&](auto &x) -> int {
+    auto gcd = [](long a, long b) {
+      while (b != 0) {
+        const long t = a % b;
+        a = b;
+        b = t;
+      }
+      return a < 0 ? -a : a;
+    };
+    PlaneRun run;
+    const long divisor = gcd(gcd(dir[0], dir[1]), dir[2]);
+    if (divisor == 0) return fill(err, errlen, "a plane wave's direction can't be zero"), -1;
+    for (int a = 0; a < 3; a++) run.g[a] = dir[a] / divisor;
+    if (!(std::isfinite(eps) && eps > 0.0))
+      return fill(err, errlen, "the background's permittivity must be positive"), -1;
+    bool faces[3];
+    for (int a = 0; a < 3; a++) {
+      const long n = x.g.n[a];
+      faces[a] = true;
+      if (x.periodic(a)) {
+        if (low[a] != 0 || high[a] != n || run.g[a] != 0)
+          return fill(err, errlen, "along a periodic axis the box must be whole and the direction "
+                                   "zero"), -1;
+        faces[a] = false;
+      } else {
+        const long lo = x.low[a], hi = x.high[a];
+        if (low[a] < lo + 1 || high[a] + hi + 1 > n || low[a] >= high[a])
+          return fill(err, errlen, "the box's faces must be in order and a cell clear of the CPMLs "
+                                   "and the ends"), -1;
+      }
+    }
+    for (int a = 0; a < 3; a++) run.steps[a] = x.g.d[a];
+    double gv[3], khat[3], pt[3];
+    for (int a = 0; a < 3; a++) gv[a] = (double)run.g[a] / run.steps[a];
+    double sq = 0.0;
+    for (int a = 0; a < 3; a++) sq += gv[a] * gv[a];
+    const double norm = std::sqrt(sq);
+    for (int a = 0; a < 3; a++) khat[a] = gv[a] / norm;
+    double along = 0.0;
+    for (int a = 0; a < 3; a++) along += pol[a] * khat[a];
+    for (int a = 0; a < 3; a++) pt[a] = pol[a] - along * khat[a];
+    double size2 = 0.0;
+    for (int a = 0; a < 3; a++) size2 += pt[a] * pt[a];
+    const double size = std::sqrt(size2);
+    if (!(std::isfinite(size) && size > 1e-12))
+      return fill(err, errlen, "the polarization has nothing across the direction"), -1;
+    for (int a = 0; a < 3; a++) pt[a] /= size;
+    auto total = [&](int field, int comp, const long at[3]) {
+      for (int a = 0; a < 3; a++) {
+        if (!faces[a]) continue;
+        const long t = twice(field, comp, a, at[a]);
+        if (!(t >= 2 * low[a] && t <= 2 * high[a])) return false;
+      }
+      return true;
+    };
+    long rlo[3], rhi[3];
+    for (int a = 0; a < 3; a++) {
+      rlo[a] = faces[a] ? low[a] - 1 : 0;
+      rhi[a] = faces[a] ? high[a] + 2 : x.g.n[a];
+    }
+    const std::vector<Link> ls = x.links(rlo, rhi, total);
+    if (!x.uniform(ls, eps))
+      return fill(err, errlen, "the medium on the box's surface must be uniform, with the "
+                               "permittivity eps and no conductivity"), -1;
+    long least = 0, most = 0;
+    for (int a = 0; a < 3; a++) {
+      const long t0 = faces[a] ? 2 * low[a] - 2 : 0, t1 = faces[a] ? 2 * high[a] + 2 : 0;
+      least += std::min(run.g[a] * t0, run.g[a] * t1);
+      most += std::max(run.g[a] * t0, run.g[a] * t1);
+    }
+    long stride = 0;
+    for (int a = 0; a < 3; a++) stride = std::max(stride, run.g[a] < 0 ? -run.g[a] : run.g[a]);
+    const long pad = stride, absorber = 200 * stride;
+    const long sheet_at = least - 4 * stride - 4;
+    long base = sheet_at - (absorber + 4 * stride + pad);
+    base -= ((base % 2) + 2) % 2;
+    const long top = most + (4 * stride + absorber + pad);
+    const long len = top - base + 1;
+    const double sample = 1.0 / (2.0 * norm);
+    const double depth = (double)absorber * sample;
+    const double sqrt_eps = std::sqrt(eps);
+    const double sigma_max = 50.0 * sqrt_eps / depth;
+    const double dt = x.dt64;
+    run.ca.assign(len, 1.0);
+    run.cb.assign(len, dt / eps);
+    run.da.assign(len, 1.0);
+    run.db.assign(len, dt);
+    for (long i = 0; i < len; i++) {
+      double into;
+      if (i < pad + absorber) into = (double)(pad + absorber - i);
+      else if (i + pad + absorber >= len) into = (double)(i + pad + absorber + 1 - len);
+      else continue;
+      const double v = std::min(into / (double)absorber, 1.0);
+      const double sigma = sigma_max * (v * (v * v));  // portable::powi(v, 3)
+      const double half_e = sigma * dt / (2.0 * eps);
+      run.ca[i] = (1.0 - half_e) / (1.0 + half_e);
+      run.cb[i] = dt / eps / (1.0 + half_e);
+      const double half_h = sigma / eps * dt / 2.0;
+      run.da[i] = (1.0 - half_h) / (1.0 + half_h);
+      run.db[i] = dt / (1.0 + half_h);
+    }
+    for (int c = 0; c < 3; c++) {
+      if (pt[c] == 0.0) continue;
+      const double j = -2.0 * sqrt_eps * norm * pt[c];
+      if ((((sheet_at - run.g[c]) % 2) + 2) % 2 == 0) {
+        run.sheet.push_back({c, sheet_at - base, j});
+      } else {
+        run.sheet.push_back({c, sheet_at - 1 - base, 0.5 * j});
+        run.sheet.push_back({c, sheet_at + 1 - base, 0.5 * j});
+      }
+    }
+    run.base = base;
+    run.pad = pad;
+    run.len = len;
+    for (int c = 0; c < 3; c++) {
+      run.e[c].assign(len, 0.0);
+      run.h[c].assign(len, 0.0);
+    }
+    run.wave = Wave::from(wave);
+    for (const Link &l : ls) {
+      long i;
+      if (!run.sample(l.from_field, l.from_comp, l.from, &i))
+        return fill(err, errlen, "the auxiliary grid doesn't span the box"), -1;
+      PlaneRun::Coupling q{l.comp, l.r, l.weight, l.from_comp, i};
+      (l.target == 0 ? run.on_e : run.on_h).push_back(q);
+    }
+    x.plane_waves.push_back(run);
+    return (int)x.plane_waves.size() - 1;
+  });
+}
+
+// Simulation::incident (src/fdtd/sources.rs:729-767): plane wave n's incident field now at a value.
+double orc_incident(const orc_sim *s, int n, int field, int comp, long i, long j, long k) {
+  return with(s, [&](auto &x) -> double {
+    if (n < 0 || n >= (int)x.plane_waves.size()) return 0.0;
+    const long at[3] = {i, j, k};
+    return x.plane_waves[n].value(field, comp, at);
+  });
 }
 
 // Waveform::spectrum (src/fdtd.rs:361-396): the sum from zero, in step order, of

@@ -85,6 +85,12 @@ int orc_medium_stable(double eps_inf, int npoles, const double *poles, double si
 /* The STREAM triad a = b + s c over len doubles on all OpenMP threads, the best of `repeats`
  * runs, in GB/s at 24 bytes an element (the reference's traffic::triad, src/traffic.rs:56-80). */
 double orc_triad(long len, int repeats);
+/* Simulation::add_plane_wave (src/fdtd/sources.rs:716-951): a total-field/scattered-field box
+ * from nodes low to high, direction dir (cells), polarization pol, background eps; the wave's
+ * number, or -1 (reason in err). orc_incident: its incident field now at a value. */
+int orc_add_plane_wave(orc_sim *s, const long low[3], const long high[3], const long dir[3],
+                       const double pol[3], double eps, const double *wave, char *err, int errlen);
+double orc_incident(const orc_sim *s, int n, int field, int comp, long i, long j, long k);
 /* Waveform::spectrum (src/fdtd.rs:361-396) at nf frequencies: out nf complex, interleaved. */
 int orc_waveform_spectrum(const double *wave, int field, double dt, long steps, int nf,
                           const double *freqs, double *out);

@@ -15,7 +15,7 @@ import subprocess
 import numpy as np
 
 from photonoxide_b200.types import (Boxes, Current, Dipole, Dispersive, Field, FluxPlane,
-                                    Grid3d, InvalidValue, Source)
+                                    Grid3d, InvalidValue, PlaneWave, Source)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle_fdtd.so")
@@ -75,6 +75,9 @@ def lib():
         x.orc_triad.argtypes = [L, C.c_int]
         x.orc_triad.restype = D
         x.orc_waveform_spectrum.argtypes = [DP, C.c_int, D, L, C.c_int, DP, DP]
+        x.orc_add_plane_wave.argtypes = [P, LP, LP, LP, DP, D, DP, C.c_char_p, C.c_int]
+        x.orc_incident.argtypes = [P, C.c_int, C.c_int, C.c_int, L, L, L]
+        x.orc_incident.restype = D
         _lib = x
     return _lib
 
@@ -193,6 +196,22 @@ class OracleSimulation:
         a = complex(d.amplitude)
         if lib().orc_add_dipole(self._h, int(d.field), int(d.component), pp, a.real, a.imag, wp):
             raise InvalidValue(f"the dipole {d} is outside its component's values")
+
+    def add_plane_wave(self, wave: PlaneWave) -> int:
+        lo, lp = _l(wave.low)
+        hi, hp = _l(wave.high)
+        dr, dp = _l(wave.direction)
+        po, pp = _d(wave.polarization)
+        w, wp = _d(wave.waveform.as_array())
+        err = C.create_string_buffer(512)
+        r = lib().orc_add_plane_wave(self._h, lp, hp, dp, pp, float(wave.eps), wp, err, 512)
+        if r < 0:
+            raise InvalidValue(err.value.decode())
+        return r
+
+    def incident(self, n: int, field, component, at) -> float:
+        return float(lib().orc_incident(self._h, int(n), int(field), int(component),
+                                        *[int(v) for v in at]))
 
     def add_probe(self, field, component, at) -> int:
         r = lib().orc_add_probe(self._h, int(field), int(component), *[int(v) for v in at])

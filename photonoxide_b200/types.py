@@ -259,6 +259,21 @@ class Dipole:
 
 
 @dataclass(frozen=True)
+class PlaneWave:
+    """A plane wave on a total-field/scattered-field box (``src/fdtd/sources.rs:74-93``): the
+    total field from nodes ``low`` to ``high`` (inclusive; whole along a periodic axis), going
+    along ``direction`` = (p, q, s) cells (integers), E along ``polarization``'s part across it,
+    in a background of ``eps`` uniform on the box's surface."""
+
+    low: Tuple[int, int, int]
+    high: Tuple[int, int, int]
+    direction: Tuple[int, int, int]
+    polarization: Tuple[float, float, float]
+    eps: float
+    waveform: "Waveform"
+
+
+@dataclass(frozen=True)
 class FluxPlane:
     """Halfway between node planes ``plane`` and ``plane + 1`` along ``axis``, within a window
     along ``axis.others()`` (``src/fdtd/monitors.rs:212-263``)."""
