@@ -56,7 +56,10 @@ typedef struct {
 
 /* A source or current value, in the order a CPU step adds them (src/fdtd.rs:1348-1387): the
  * waveform of `emitter` taken at the field's time (M at t, J at t + dt/2), Re(a w) added as
- * H -= dt Re(a w) or E -= cb Re(a w). A point source has a = 1 and takes w.at(t). */
+ * H -= dt Re(a w) or E -= cb Re(a w). A point source has a = 1 and takes w.at(t). point 2: a
+ * coupling of a plane wave's box (PlaneWaveRun::correct, src/fdtd/sources.rs:971-991), its
+ * coefficient a_re (dt weight for H, cb weight for E) times the incident value in slot `emitter`
+ * of fdtd_set_plane_waves, subtracted as it is (H -= a_re h_inc). */
 typedef struct {
   int32_t field, component;
   int64_t r;
@@ -138,6 +141,34 @@ int fdtd_download_fields(fdtd_ctx *ctx, double *e, double *h, double *const *psi
 /* The run's sources and currents (Resident::plan's injection groups, resident.rs:546-590). */
 int fdtd_set_sources(fdtd_ctx *ctx, int32_t nwaves, const fdtd_waveform *waves, int64_t ninj,
                      const fdtd_injection *inj);
+/* A plane wave's auxiliary 1D run (PlaneWaveRun, src/fdtd/sources.rs:755-1041), stepped on the
+ * device with the grid: len samples, the first and last pad never updated; the direction g
+ * (cells) and the grid's steps for its differences; per sample E <- ca E + cb curl and H <- da H -
+ * db curl; the sheet's J (component, sample, J per unit waveform) with E's waveform at t + dt/2.
+ * Each step records the slots the box's couplings read: field 0, E's `comp` at sample i before
+ * the H step (for H's couplings), field 1, H after it (for E's). e0 and h0 (3 x len, component
+ * by component) its state now, or NULL for zeros. */
+typedef struct {
+  int64_t len, pad;
+  int64_t g[3];
+  double steps[3];
+  const double *ca, *cb, *da, *db;
+  int32_t nsheet;
+  const int32_t *sheet_comp;
+  const int64_t *sheet_i;
+  const double *sheet_j;
+  fdtd_waveform wave;
+  int32_t nslots;
+  const int32_t *slot_field, *slot_comp;
+  const int64_t *slot_i;
+  const double *e0, *h0;
+} fdtd_plane_wave;
+/* The plane waves' runs (their slots numbered on from one wave to the next, as point-2
+ * injections name them). Call before fdtd_set_sources, which lays out the step's values for
+ * them; no counterpart in the reference's GPU path, which refuses plane waves (gpu.rs:431). */
+int fdtd_set_plane_waves(fdtd_ctx *ctx, int32_t count, const fdtd_plane_wave *waves);
+/* Plane wave n's auxiliary state now: E and H, 3 x len each (either may be NULL). */
+int fdtd_plane_wave_state(fdtd_ctx *ctx, int32_t n, double *e, double *h);
 /* The probes: field, component and index of each value recorded after every step. */
 int fdtd_set_probes(fdtd_ctx *ctx, int32_t n, const int32_t *field, const int32_t *component,
                     const int64_t *r);

@@ -87,6 +87,18 @@ int pxs_add_dft(pxs_sim *s, const int64_t low[3], const int64_t high[3], int32_t
 int pxs_add_flux(pxs_sim *s, int32_t axis, int64_t plane, const int64_t window[4], int32_t nf,
                  const double *freqs);
 int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const double *freqs);
+/* Simulation::add_plane_wave (src/fdtd/sources.rs:716-951): a total-field/scattered-field box
+ * from nodes low to high (inclusive; whole along a periodic axis), the wave going along
+ * direction (cells, integers), E along polarization's part across it, the background's eps
+ * uniform on the box's surface; its auxiliary 1D run is stepped on the device with the grid.
+ * Returns the wave's number, or a negative status. */
+int pxs_add_plane_wave(pxs_sim *s, const int64_t low[3], const int64_t high[3],
+                       const int64_t direction[3], const double polarization[3], double eps,
+                       const double wave[6]);
+/* Simulation::incident (src/fdtd/sources.rs:729-767): plane wave n's incident field now at a
+ * value (E at the current time, H half a step behind), into *out; 0 beyond its run. */
+int pxs_incident(pxs_sim *s, int32_t n, int32_t field, int32_t comp, int64_t i, int64_t j,
+                 int64_t k, double *out);
 
 /* Simulation::run (src/fdtd.rs:1142-1158) on the device. */
 int pxs_run(pxs_sim *s, int64_t steps);

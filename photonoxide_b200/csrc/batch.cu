@@ -966,6 +966,9 @@ int admissible(fdtd_batch *b, const InstanceView &v, int i) {
   if (v.media)
     return bfail(b, FDTD_E_INVALID,
                  "simulation %d has dispersive media, which the batch does not step", i);
+  if (v.plane_waves)
+    return bfail(b, FDTD_E_INVALID,
+                 "simulation %d has a plane wave's box, which the batch does not step", i);
   return 0;
 }
 
@@ -1753,6 +1756,8 @@ int fdtd_adjoint_create(fdtd_ctx *ctx, int64_t steps, int32_t segment, int64_t c
   a->psi_e_len = v.psi_e_len;
   a->psi_h_len = v.psi_h_len;
   if (v.media) return afail(a, FDTD_E_INVALID, "the adjoint does not step dispersive media");
+  if (v.plane_waves)
+    return afail(a, FDTD_E_INVALID, "the adjoint does not step a plane wave's box");
   std::vector<long long> design(count);
   for (int64_t d = 0; d < count; d++) {
     if (component[d] < 0 || component[d] > 1 || r[d] < 0 || r[d] >= v.N)

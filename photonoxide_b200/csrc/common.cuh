@@ -28,9 +28,31 @@ struct Group {
 };
 struct Entry {
   double are, aim;
-  int emitter;
-  int pad;
+  int emitter;  // its values' slot among the step's waves (sources' first, then the couplings')
+  int pad;      // 1: a coupling of a plane wave's box
 };
+
+// One injection's share of a value of H (src/fdtd.rs:1346-1362): a point source or a current takes
+// v - dt Re(a w(t)); a coupling of a plane wave's total-field/scattered-field box (pad 1) takes
+// v - (dt weight) h_inc, its coefficient folded on the host and the incident value its "wave"
+// (src/fdtd/sources.rs:971-991). w: the step's values, 2 per emitter.
+template <typename T>
+__device__ __forceinline__ T apply_h(T v, const Entry &en, const double *w, T dt) {
+  const double amount = en.are * w[2 * en.emitter] - en.aim * w[2 * en.emitter + 1];
+  if (en.pad) return v - (T)amount;
+  if (sizeof(T) == 8) return v - (T)((double)dt * amount);
+  return v - dt * (T)amount;
+}
+
+// The same for a value of E (src/fdtd.rs:1366-1393): v - cb Re(a w(t)), or a coupling's
+// v - (cb weight) h_inc.
+template <typename T>
+__device__ __forceinline__ T apply_e(T v, const Entry &en, const double *w, T cbv) {
+  const double amount = en.are * w[2 * en.emitter] - en.aim * w[2 * en.emitter + 1];
+  if (en.pad) return v - (T)amount;
+  if (sizeof(T) == 8) return v - (T)((double)cbv * amount);
+  return v - cbv * (T)amount;
+}
 
 __host__ __device__ inline int wrap_index(int g, int n, int periodic) {
   if (g >= 0 && g < n) return g;

@@ -236,10 +236,7 @@ __global__ void __launch_bounds__(NT) step_kernel(StepArgs<T> A) {
       Group gr = A.hgroups[g];
       T *v = &sH[hb][gr.comp][0][0] + gr.local;
       for (int q = gr.first; q < gr.first + gr.count; q++) {
-        Entry en = A.entries[q];
-        double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
-        if (sizeof(T) == 8) *v = *v - (T)((double)A.dt * amount);
-        else *v = *v - A.dt * (T)amount;
+        *v = apply_h<T>(*v, A.entries[q], A.waves_h, A.dt);
       }
     }
   };
@@ -321,11 +318,7 @@ __global__ void __launch_bounds__(NT) step_kernel(StepArgs<T> A) {
         T cbv = A.cb[gr.comp * N + r];
         T *v = &sEn[gr.comp][ly][lx];
         for (int q = gr.first; q < gr.first + gr.count; q++) {
-          Entry en2 = A.entries[q];
-          double amount =
-              en2.are * A.waves_e[2 * en2.emitter] - en2.aim * A.waves_e[2 * en2.emitter + 1];
-          if (sizeof(T) == 8) *v = *v - (T)((double)cbv * amount);
-          else *v = *v - cbv * (T)amount;
+          *v = apply_e<T>(*v, A.entries[q], A.waves_e, cbv);
         }
       }
     }
@@ -566,10 +559,7 @@ __global__ void __launch_bounds__(NT) staged_kernel(StepArgs<T> A, long long tot
           Group gr = A.hgroups[g];
           T *v = &sHn[(size_t)gr.comp * S::HH * (TX + 1) + gr.local];
           for (int q = gr.first; q < gr.first + gr.count; q++) {
-            Entry en = A.entries[q];
-            double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
-            if (sizeof(T) == 8) *v = *v - (T)((double)A.dt * amount);
-            else *v = *v - A.dt * (T)amount;
+            *v = apply_h<T>(*v, A.entries[q], A.waves_h, A.dt);
           }
         }
       }
@@ -658,10 +648,7 @@ __global__ void __launch_bounds__(NT) staged_kernel(StepArgs<T> A, long long tot
           T cbv = A.cb[gr.comp * N + r0];
           T *v = &sEn[(size_t)gr.comp * TY * TX + gr.local];
           for (int q = gr.first; q < gr.first + gr.count; q++) {
-            Entry en2 = A.entries[q];
-            double amount = en2.are * A.waves_e[2 * en2.emitter] - en2.aim * A.waves_e[2 * en2.emitter + 1];
-            if (sizeof(T) == 8) *v = *v - (T)((double)cbv * amount);
-            else *v = *v - cbv * (T)amount;
+            *v = apply_e<T>(*v, A.entries[q], A.waves_e, cbv);
           }
         }
         __syncthreads();
@@ -959,10 +946,7 @@ __global__ void __launch_bounds__(rowstep::THREADS, 2) row_kernel(StepArgs<T> A)
         for (int c = 0; c < 3; c++)
           if (gr.comp == c) v = second ? hn[c][1] : hn[c][0];
         for (int q = gr.first; q < gr.first + gr.count; q++) {
-          Entry en = A.entries[q];
-          double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
-          if (sizeof(T) == 8) v = v - (T)((double)A.dt * amount);
-          else v = v - A.dt * (T)amount;
+          v = apply_h<T>(v, A.entries[q], A.waves_h, A.dt);
         }
 #pragma unroll
         for (int c = 0; c < 3; c++)
@@ -1088,10 +1072,7 @@ __global__ void __launch_bounds__(rowstep::THREADS, 2) row_kernel(StepArgs<T> A)
               v = second ? en[c][1] : en[c][0];
             }
           for (int q = gr.first; q < gr.first + gr.count; q++) {
-            Entry e2 = A.entries[q];
-            double amount = e2.are * A.waves_e[2 * e2.emitter] - e2.aim * A.waves_e[2 * e2.emitter + 1];
-            if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
-            else v = v - cbv * (T)amount;
+            v = apply_e<T>(v, A.entries[q], A.waves_e, cbv);
           }
 #pragma unroll
           for (int c = 0; c < 3; c++)
@@ -1666,10 +1647,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
             if (gr.comp == c && jj == j) {
               T v = hn[c][j];
               for (int q = gr.first; q < gr.first + gr.count; q++) {
-                Entry en = A.entries[q];
-                double amount = en.are * A.waves_h[2 * en.emitter] - en.aim * A.waves_h[2 * en.emitter + 1];
-                if (sizeof(T) == 8) v = v - (T)((double)A.dt * amount);
-                else v = v - A.dt * (T)amount;
+                v = apply_h<T>(v, A.entries[q], A.waves_h, A.dt);
               }
               hn[c][j] = v;
             }
@@ -1858,10 +1836,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
                 T v = en[c][j];
                 const T cbv = cb[c].v[j];
                 for (int q = gr.first; q < gr.first + gr.count; q++) {
-                  Entry e2 = A.entries[q];
-                  double amount = e2.are * A.waves_e[2 * e2.emitter] - e2.aim * A.waves_e[2 * e2.emitter + 1];
-                  if (sizeof(T) == 8) v = v - (T)((double)cbv * amount);
-                  else v = v - cbv * (T)amount;
+                  v = apply_e<T>(v, A.entries[q], A.waves_e, cbv);
                 }
                 en[c][j] = v;
               }
@@ -1899,9 +1874,10 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 // at H's time t = (first+m) dt and at E's t + dt/2, 2 doubles each per emitter.
 // point[e]: 1 if emitter e is a point source (w.at), else 0 (complex_at)
 // base: the batch's first step index in device memory (a captured batch), or null (first).
-__global__ void waves_kernel(const Wave *waves, const int *point, int nw, long long first,
-                             const long long *base, int batch, double dt, double *out_h,
-                             double *out_e) {
+// stride: each step's values, the emitters' then the plane waves' slots (2 doubles each)
+__global__ void waves_kernel(const Wave *waves, const int *point, int nw, int stride,
+                             long long first, const long long *base, int batch, double dt,
+                             double *out_h, double *out_e) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nw * batch) return;
   if (base) first = *base;
@@ -1910,11 +1886,91 @@ __global__ void waves_kernel(const Wave *waves, const int *point, int nw, long l
   double half = t + 0.5 * dt;
   double re, im;
   wave_eval(waves[e], t, &re, &im, point[e]);
-  out_h[2 * ((long long)m * nw + e)] = re;
-  out_h[2 * ((long long)m * nw + e) + 1] = im;
+  out_h[2 * ((long long)m * stride + e)] = re;
+  out_h[2 * ((long long)m * stride + e) + 1] = im;
   wave_eval(waves[e], half, &re, &im, point[e]);
-  out_e[2 * ((long long)m * nw + e)] = re;
-  out_e[2 * ((long long)m * nw + e) + 1] = im;
+  out_e[2 * ((long long)m * stride + e)] = re;
+  out_e[2 * ((long long)m * stride + e) + 1] = im;
+}
+
+// A plane wave's auxiliary 1D run on the device (PlaneWaveRun, src/fdtd/sources.rs:755-1041).
+struct AuxDev {
+  long long len, pad;
+  long long g[3];
+  double steps[3];
+  double *e, *h;  // 3 x len each, component by component
+  const double *ca, *cb, *da, *db;
+  int nsheet;
+  const int *sheet_comp;
+  const long long *sheet_i;
+  const double *sheet_j;
+  Wave wave;
+  int nslots, slot0;  // its slots, numbered on from slot0 after the other runs'
+  const int *slot_field, *slot_comp;
+  const long long *slot_i;
+};
+
+// (f[i + o] - f[i - o]) / step along an axis the direction moves o samples for (0 if none)
+__device__ __forceinline__ double aux_difference(const double *f, long long o, double step,
+                                                 long long i) {
+  if (o == 0) return 0.0;
+  return (f[i + o] - f[i - o]) / step;
+}
+
+// A batch of steps of every plane wave's run, a CTA each, in the reference's order
+// (PlaneWaveRun::step_h then step_e, src/fdtd/sources.rs:1008-1040): before step m's H update the
+// slots of E its box's H couplings read, after it the slots of H its E couplings read, into the
+// step's values at nw + slot (stride values a step). The run's state stays on the device.
+__global__ void __launch_bounds__(1024) aux_kernel(const AuxDev *runs, int nw, int stride,
+                                                   long long first, const long long *base,
+                                                   int batch, double dt, double *out_h,
+                                                   double *out_e) {
+  const AuxDev R = runs[blockIdx.x];
+  if (base) first = *base;
+  const long long len = R.len, inner = len - 2 * R.pad;
+  for (int m = 0; m < batch; m++) {
+    const double t = (double)(first + m) * dt, half = t + 0.5 * dt;
+    double *oh = out_h + 2LL * ((long long)m * stride + nw + R.slot0);
+    double *oe = out_e + 2LL * ((long long)m * stride + nw + R.slot0);
+    for (int q = threadIdx.x; q < R.nslots; q += blockDim.x)
+      if (R.slot_field[q] == 0) {
+        oh[2 * q] = R.e[R.slot_comp[q] * len + R.slot_i[q]];
+        oh[2 * q + 1] = 0.0;
+      }
+    for (long long q = threadIdx.x; q < 3 * inner; q += blockDim.x) {
+      const int c = (int)(q / inner);
+      const long long i = R.pad + q % inner;
+      const int a = (c + 1) % 3, b = (c + 2) % 3;
+      const double curl = aux_difference(R.e + b * len, R.g[a], R.steps[a], i) -
+                          aux_difference(R.e + a * len, R.g[b], R.steps[b], i);
+      R.h[c * len + i] = R.da[i] * R.h[c * len + i] - R.db[i] * curl;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < R.nslots; q += blockDim.x)
+      if (R.slot_field[q] == 1) {
+        oe[2 * q] = R.h[R.slot_comp[q] * len + R.slot_i[q]];
+        oe[2 * q + 1] = 0.0;
+      }
+    for (long long q = threadIdx.x; q < 3 * inner; q += blockDim.x) {
+      const int c = (int)(q / inner);
+      const long long i = R.pad + q % inner;
+      const int a = (c + 1) % 3, b = (c + 2) % 3;
+      const double curl = aux_difference(R.h + b * len, R.g[a], R.steps[a], i) -
+                          aux_difference(R.h + a * len, R.g[b], R.steps[b], i);
+      R.e[c * len + i] = R.ca[i] * R.e[c * len + i] + R.cb[i] * curl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && R.nsheet > 0) {  // the sheet's J at t + dt/2, one value at a time
+      double w, unused;
+      wave_eval(R.wave, half, &w, &unused, 1);
+      for (int q = 0; q < R.nsheet; q++) {
+        const long long i = R.sheet_i[q];
+        double &v = R.e[R.sheet_comp[q] * len + i];
+        v = v - R.cb[i] * R.sheet_j[q] * w;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // After a step: the probes' values into the record, the transformed values into the ring.
@@ -2070,8 +2126,16 @@ struct fdtd_ctx {
   int runs[quad_max_runs + 1] = {};  // the quad kernel's runs of planes (quad_runs)
   Group *hgroups = nullptr, *egroups = nullptr;
   Entry *entries = nullptr;
-  double *waves_h = nullptr, *waves_e = nullptr;  // batch x nwaves x 2
+  double *waves_h = nullptr, *waves_e = nullptr;  // batch x (nwaves + naux) x 2
   int wave_batch = 0;
+  // plane waves' auxiliary runs (fdtd_set_plane_waves): their descriptors (pointing into device
+  // memory), and the slots their couplings read, recorded each step after the emitters' values
+  int naux_runs = 0, naux = 0;
+  int naux_laid = 0;  // the slot count fdtd_set_sources laid the step's values out for
+  std::vector<AuxDev> aux;
+  std::vector<void *> aux_memory;
+  AuxDev *d_aux = nullptr;
+  int stride() const { return nwaves + naux; }
   // probes and transforms
   int nprobes = 0;
   long long *d_probes = nullptr;
@@ -2500,6 +2564,8 @@ template <typename T>
 int run_impl(fdtd_ctx *c, long long steps, long long first) {
   if (!c->coeffs_set || !c->fields_set)
     return fail(c, FDTD_E_STATE, "upload the coefficients and the fields before a run");
+  if (c->naux_laid != c->naux)
+    return fail(c, FDTD_E_STATE, "set the sources again after the plane waves");
   const int K = c->ring_k > 0 ? c->ring_k : 64;
   // the probes' record: grow to the run's steps
   if (c->nprobes > 0 && c->recorded + steps > c->record_cap) {
@@ -2518,14 +2584,20 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
     if (c->nwaves > 0) {
       int total = c->nwaves * batch;
       waves_kernel<<<(total + 127) / 128, 128, 0, c->stream>>>(
-          c->d_waves, c->d_point, c->nwaves, first + at, base, batch, c->dt, c->waves_h,
-          c->waves_e);
+          c->d_waves, c->d_point, c->nwaves, c->stride(), first + at, base, batch, c->dt,
+          c->waves_h, c->waves_e);
+      c->launches++;
+    }
+    if (c->naux_runs > 0) {
+      aux_kernel<<<c->naux_runs, 1024, 0, c->stream>>>(c->d_aux, c->nwaves, c->stride(),
+                                                       first + at, base, batch, c->dt,
+                                                       c->waves_h, c->waves_e);
       c->launches++;
     }
     for (int m = 0; m < batch; m++) {
       StepArgs<T> A = step_args<T>(c);
-      A.waves_h = c->waves_h + 2LL * m * c->nwaves;
-      A.waves_e = c->waves_e + 2LL * m * c->nwaves;
+      A.waves_h = c->waves_h + 2LL * m * c->stride();
+      A.waves_e = c->waves_e + 2LL * m * c->stride();
       if (c->profiling) {
         if (c->events_used + 2 > c->events.size()) {
           for (int q = 0; q < 256; q++) {
@@ -2880,11 +2952,13 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   std::vector<int> point(std::max(nwaves, 1), -1);
   for (int64_t q = 0; q < ninj; q++) {
     const fdtd_injection &x = inj[q];
+    const int slots = x.point == 2 ? c->naux : nwaves;  // a coupling reads a plane wave's slot
     if (x.field < 0 || x.field > 1 || x.component < 0 || x.component > 2 || x.r < 0 ||
-        x.r >= c->N || x.emitter < 0 || x.emitter >= nwaves || !std::isfinite(x.a_re) ||
-        !std::isfinite(x.a_im))
+        x.r >= c->N || x.emitter < 0 || x.emitter >= slots || !std::isfinite(x.a_re) ||
+        !std::isfinite(x.a_im) || x.point < 0 || x.point > 2)
       return fail(c, FDTD_E_INVALID, "injection %lld is outside the grid or not finite",
                   (long long)q);
+    if (x.point == 2) continue;
     int want = x.point ? 1 : 0;
     if (point[x.emitter] >= 0 && point[x.emitter] != want)
       return fail(c, FDTD_E_INVALID, "emitter %d is both a point source and a current", x.emitter);
@@ -2922,8 +2996,8 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
       Entry en;
       en.are = x.a_re;
       en.aim = x.a_im;
-      en.emitter = x.emitter;
-      en.pad = 0;
+      en.emitter = x.point == 2 ? nwaves + x.emitter : x.emitter;
+      en.pad = x.point == 2 ? 1 : 0;
       lists[at].push_back((int)entries.size());
       entries.push_back(en);
     }
@@ -3005,6 +3079,13 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   if (!ordered_entries.empty())
     CUDA_TRY(c, copy(c, c->entries, ordered_entries.data(), ordered_entries.size() * sizeof(Entry), cudaMemcpyHostToDevice));
   c->nwaves = nwaves;
+  c->naux_laid = c->naux;
+  if (c->stride() > 0) {
+    const int K = c->ring_k > 0 ? c->ring_k : 64;
+    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * c->stride() * 16)) return r;
+    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * c->stride() * 16)) return r;
+    c->wave_batch = K;
+  }
   if (nwaves > 0) {
     std::vector<Wave> w(nwaves);
     for (int q = 0; q < nwaves; q++) {
@@ -3012,15 +3093,110 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
       for (int p = 0; p < 5; p++) w[q].p[p] = waves[q].p[p];
       if (point[q] < 0) point[q] = 0;
     }
-    const int K = c->ring_k > 0 ? c->ring_k : 64;
     if (int r = alloc(c, (void **)&c->d_waves, nwaves * sizeof(Wave))) return r;
     if (int r = alloc(c, (void **)&c->d_point, nwaves * sizeof(int))) return r;
-    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * nwaves * 16)) return r;
-    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * nwaves * 16)) return r;
-    c->wave_batch = K;
     CUDA_TRY(c, copy(c, c->d_waves, w.data(), nwaves * sizeof(Wave), cudaMemcpyHostToDevice));
     CUDA_TRY(c, copy(c, c->d_point, point.data(), nwaves * sizeof(int), cudaMemcpyHostToDevice));
   }
+  return 0;
+}
+
+int fdtd_set_plane_waves(fdtd_ctx *c, int32_t count, const fdtd_plane_wave *w) {
+  if (!c) return FDTD_E_INVALID;
+  if (count < 0 || (count > 0 && !w)) return fail(c, FDTD_E_INVALID, "no plane waves given");
+  for (int32_t n = 0; n < count; n++) {
+    const fdtd_plane_wave &x = w[n];
+    long long reach = 0;
+    for (int a = 0; a < 3; a++) reach = std::max<long long>(reach, std::llabs(x.g[a]));
+    bool ok = x.len > 0 && x.pad >= reach && 2 * x.pad < x.len && x.ca && x.cb && x.da && x.db &&
+              x.nsheet >= 0 && x.nslots >= 0 && x.wave.kind >= 0 && x.wave.kind <= 2;
+    for (int a = 0; a < 3 && ok; a++) ok = x.g[a] == 0 || x.steps[a] > 0.0;
+    for (int q = 0; q < x.nsheet && ok; q++)
+      ok = x.sheet_comp[q] >= 0 && x.sheet_comp[q] < 3 && x.sheet_i[q] >= 0 &&
+           x.sheet_i[q] < x.len;
+    for (int q = 0; q < x.nslots && ok; q++)
+      ok = (x.slot_field[q] == 0 || x.slot_field[q] == 1) && x.slot_comp[q] >= 0 &&
+           x.slot_comp[q] < 3 && x.slot_i[q] >= 0 && x.slot_i[q] < x.len;
+    if (!ok) return fail(c, FDTD_E_INVALID, "plane wave %d's run is malformed", (int)n);
+  }
+  c->generation++;
+  c->layout++;
+  for (void *p : c->aux_memory) release(c, p);
+  c->aux_memory.clear();
+  c->aux.clear();
+  release(c, c->d_aux);
+  c->d_aux = nullptr;
+  c->naux_runs = 0;
+  c->naux = 0;
+  auto put = [&](const void *src, size_t bytes, void **dst) -> int {
+    if (int r = alloc(c, dst, bytes)) return r;
+    c->aux_memory.push_back(*dst);
+    if (src) CUDA_TRY(c, copy(c, *dst, src, bytes, cudaMemcpyHostToDevice));
+    else CUDA_TRY(c, cudaMemsetAsync(*dst, 0, bytes, c->stream));
+    return 0;
+  };
+  int slots = 0;
+  for (int32_t n = 0; n < count; n++) {
+    const fdtd_plane_wave &x = w[n];
+    AuxDev d;
+    d.len = x.len;
+    d.pad = x.pad;
+    for (int a = 0; a < 3; a++) {
+      d.g[a] = x.g[a];
+      d.steps[a] = x.steps[a];
+    }
+    const size_t L = (size_t)x.len * 8;
+    void *p = nullptr;
+    if (int r = put(x.e0, 3 * L, &p)) return r;
+    d.e = (double *)p;
+    if (int r = put(x.h0, 3 * L, &p)) return r;
+    d.h = (double *)p;
+    if (int r = put(x.ca, L, &p)) return r;
+    d.ca = (const double *)p;
+    if (int r = put(x.cb, L, &p)) return r;
+    d.cb = (const double *)p;
+    if (int r = put(x.da, L, &p)) return r;
+    d.da = (const double *)p;
+    if (int r = put(x.db, L, &p)) return r;
+    d.db = (const double *)p;
+    d.nsheet = x.nsheet;
+    std::vector<int> sc(x.sheet_comp, x.sheet_comp + x.nsheet);
+    if (int r = put(sc.data(), sc.size() * 4, &p)) return r;
+    d.sheet_comp = (const int *)p;
+    if (int r = put(x.sheet_i, (size_t)x.nsheet * 8, &p)) return r;
+    d.sheet_i = (const long long *)p;
+    if (int r = put(x.sheet_j, (size_t)x.nsheet * 8, &p)) return r;
+    d.sheet_j = (const double *)p;
+    d.wave.kind = x.wave.kind;
+    for (int q = 0; q < 5; q++) d.wave.p[q] = x.wave.p[q];
+    d.nslots = x.nslots;
+    d.slot0 = slots;
+    std::vector<int> sf(x.slot_field, x.slot_field + x.nslots),
+        sp(x.slot_comp, x.slot_comp + x.nslots);
+    if (int r = put(sf.data(), sf.size() * 4, &p)) return r;
+    d.slot_field = (const int *)p;
+    if (int r = put(sp.data(), sp.size() * 4, &p)) return r;
+    d.slot_comp = (const int *)p;
+    if (int r = put(x.slot_i, (size_t)x.nslots * 8, &p)) return r;
+    d.slot_i = (const long long *)p;
+    slots += x.nslots;
+    c->aux.push_back(d);
+  }
+  if (count > 0) {
+    if (int r = alloc(c, (void **)&c->d_aux, count * sizeof(AuxDev))) return r;
+    CUDA_TRY(c, copy(c, c->d_aux, c->aux.data(), count * sizeof(AuxDev), cudaMemcpyHostToDevice));
+  }
+  c->naux_runs = count;
+  c->naux = slots;
+  return 0;
+}
+
+int fdtd_plane_wave_state(fdtd_ctx *c, int32_t n, double *e, double *h) {
+  if (!c) return FDTD_E_INVALID;
+  if (n < 0 || n >= c->naux_runs) return fail(c, FDTD_E_INVALID, "no plane wave %d", (int)n);
+  const AuxDev &d = c->aux[n];
+  if (e) CUDA_TRY(c, copy(c, e, d.e, (size_t)d.len * 24, cudaMemcpyDeviceToHost));
+  if (h) CUDA_TRY(c, copy(c, h, d.h, (size_t)d.len * 24, cudaMemcpyDeviceToHost));
   return 0;
 }
 
@@ -3137,12 +3313,12 @@ int fdtd_set_dft(fdtd_ctx *c, int32_t nseries, const fdtd_series *series, int32_
   CUDA_TRY(c, copy(c, c->d_slot_field, slot_field.data(), slot_field.size() * 4, cudaMemcpyHostToDevice));
   CUDA_TRY(c, cudaMemsetAsync(c->sums, 0, sums * 16, c->stream));
   // the source waves' batch must match the ring's
-  if (c->nwaves > 0 && c->wave_batch < K) {
+  if (c->stride() > 0 && c->wave_batch < K) {
     release(c, c->waves_h);
     release(c, c->waves_e);
     c->waves_h = c->waves_e = nullptr;
-    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * c->nwaves * 16)) return r;
-    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * c->nwaves * 16)) return r;
+    if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * c->stride() * 16)) return r;
+    if (int r = alloc(c, (void **)&c->waves_e, (size_t)K * c->stride() * 16)) return r;
     c->wave_batch = (int)K;
   }
   return 0;
@@ -3466,6 +3642,7 @@ int fdtd_instance_view(fdtd_ctx *c, InstanceView *v) {
   v->nprobes = c->nprobes;
   v->probes = c->d_probes;
   v->media = c->media;
+  v->plane_waves = c->naux_runs > 0;
   v->stream = c->stream;
   v->generation = c->generation;
   return 0;

@@ -16,6 +16,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -213,6 +214,47 @@ bool medium_stable(double eps_inf, const std::vector<double> &co, double sigma, 
   return true;
 }
 
+// Twice a value's position along `axis` in steps from node 0 (src/fdtd/sources.rs:155-162).
+int64_t twice(int field, int comp, int axis, int64_t m) {
+  const bool half = field == 0 ? comp == axis : comp != axis;
+  return 2 * m + (half ? 1 : 0);
+}
+
+// One coupling across a total-field/scattered-field surface (src/fdtd/sources.rs:138-153).
+struct Link {
+  int target, comp;
+  int64_t r;
+  double weight;
+  int from_field, from_comp;
+  int64_t from[3];
+};
+
+// A plane wave's run (PlaneWaveRun, src/fdtd/sources.rs:740-951) as the host builds it: the
+// auxiliary 1D grid's coefficients and sheet, the box's couplings, and a copy of its state (the
+// device steps it; the copy is brought up to date when read, or when the engine is remade).
+struct PlaneRun {
+  int64_t g[3];
+  double steps[3];
+  int64_t base = 0, pad = 0, len = 0;
+  std::vector<double> ca, cb, da, db;
+  std::vector<int32_t> sheet_comp;
+  std::vector<int64_t> sheet_i;
+  std::vector<double> sheet_j;
+  fdtd_waveform wave;
+  struct Coupling { int c; int64_t r; double w; int from; int64_t i; };
+  std::vector<Coupling> on_e, on_h;
+  std::vector<double> e, h;  // 3 x len each
+
+  bool sample(int field, int comp, const int64_t at[3], int64_t *i) const {
+    int64_t l = 0;
+    for (int a = 0; a < 3; a++) l += g[a] * twice(field, comp, a, at[a]);
+    const int64_t q = l - base;
+    if (q < 0 || q >= len) return false;
+    *i = q;
+    return true;
+  }
+};
+
 }  // namespace
 
 struct pxs_sim {
@@ -243,6 +285,8 @@ struct pxs_sim {
   std::vector<std::vector<FluxFace>> fluxes;
   std::vector<MediaGroup> groups;
   std::unordered_map<int64_t, int> members;  // a dispersive value (comp * N + r): its group
+  std::vector<PlaneRun> plane_waves;
+  int aux_on_device = 0;  // the plane waves whose latest state is the engine's
   bool configured = false;  // sources, probes and transforms pushed to the engine
   bool fields_dropped = false;  // released without reading the fields back (a served job's)
   fdtd_ctx *ctx = nullptr;
@@ -398,10 +442,73 @@ struct pxs_sim {
     return 0;
   }
 
+  // The plane waves' states from the engine into the host's copies.
+  int pull_plane_waves() {
+    for (int n = 0; n < aux_on_device && ctx; n++) {
+      PlaneRun &p = plane_waves[n];
+      if (int r = fdtd_plane_wave_state(ctx, n, p.e.data(), p.h.data()))
+        return fail(r, "%s", fdtd_last_error(ctx));
+    }
+    return 0;
+  }
+
   int configure() {
     if (configured) return 0;
     std::vector<fdtd_injection> inj(points);
     inj.insert(inj.end(), currents.begin(), currents.end());
+    // the plane waves' runs, with their states so far; each coupling reads a slot of them, its
+    // coefficient folded as the reference's correct() has it: dt w for H, cb w for E
+    if (int r = pull_plane_waves()) return r;
+    std::vector<fdtd_plane_wave> pw(plane_waves.size());
+    std::vector<std::vector<int32_t>> sf(plane_waves.size()), sc(plane_waves.size());
+    std::vector<std::vector<int64_t>> si(plane_waves.size());
+    int32_t slot0 = 0;
+    for (size_t n = 0; n < plane_waves.size(); n++) {
+      const PlaneRun &p = plane_waves[n];
+      std::map<std::tuple<int, int, int64_t>, int32_t> slot;
+      auto slot_of = [&](int field, int comp, int64_t i) {
+        auto key = std::make_tuple(field, comp, i);
+        auto it = slot.find(key);
+        if (it != slot.end()) return it->second;
+        const int32_t q = (int32_t)sf[n].size();
+        sf[n].push_back(field);
+        sc[n].push_back(comp);
+        si[n].push_back(i);
+        slot[key] = q;
+        return q;
+      };
+      for (const PlaneRun::Coupling &q : p.on_h)
+        inj.push_back(fdtd_injection{1, q.c, q.r, dt * q.w, 0.0, slot0 + slot_of(0, q.from, q.i), 2});
+      for (const PlaneRun::Coupling &q : p.on_e)
+        inj.push_back(fdtd_injection{0, q.c, q.r, cb[q.c][q.r] * q.w, 0.0,
+                                     slot0 + slot_of(1, q.from, q.i), 2});
+      fdtd_plane_wave &d = pw[n];
+      d.len = p.len;
+      d.pad = p.pad;
+      for (int a = 0; a < 3; a++) {
+        d.g[a] = p.g[a];
+        d.steps[a] = p.steps[a];
+      }
+      d.ca = p.ca.data();
+      d.cb = p.cb.data();
+      d.da = p.da.data();
+      d.db = p.db.data();
+      d.nsheet = (int32_t)p.sheet_comp.size();
+      d.sheet_comp = p.sheet_comp.data();
+      d.sheet_i = p.sheet_i.data();
+      d.sheet_j = p.sheet_j.data();
+      d.wave = p.wave;
+      d.nslots = (int32_t)sf[n].size();
+      d.slot_field = sf[n].data();
+      d.slot_comp = sc[n].data();
+      d.slot_i = si[n].data();
+      d.e0 = p.e.data();
+      d.h0 = p.h.data();
+      slot0 += d.nslots;
+    }
+    if (int r = fdtd_set_plane_waves(ctx, (int32_t)pw.size(), pw.data()))
+      return fail(r, "%s", fdtd_last_error(ctx));
+    aux_on_device = (int)plane_waves.size();
     if (int r = fdtd_set_sources(ctx, (int32_t)waves.size(), waves.data(), (int64_t)inj.size(),
                                  inj.data()))
       return fail(r, "%s", fdtd_last_error(ctx));
@@ -482,6 +589,8 @@ struct pxs_sim {
       fields_dropped = true;  // the host's copies are stale: reading them or running refuses
     }
     if (int r = pull_sums()) return r;
+    if (int r = pull_plane_waves()) return r;
+    aux_on_device = 0;
     fdtd_destroy(ctx);
     ctx = nullptr;
     configured = false;
@@ -1100,6 +1209,277 @@ int pxs_add_current(pxs_sim *s, int32_t field, int64_t count, const int32_t *com
     s->currents.push_back(fdtd_injection{field, comps[q], s->index(p[0], p[1], p[2]), amps[2 * q],
                                          amps[2 * q + 1], (int32_t)s->waves.size() - 1, 0});
   }
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Simulation::links (src/fdtd/sources.rs:316-420): the couplings across a total-field /
+// scattered-field surface among the values in [lo, hi) per axis, total() saying which side each
+// value is on; values held at zero (cb = 0) neither take nor give one.
+template <typename F>
+std::vector<Link> surface_links(const pxs_sim *s, const int64_t lo[3], const int64_t hi[3],
+                                const F &total) {
+  const Grid &g = s->g;
+  auto neighbour = [&](const int64_t at[3], int axis, bool forward, int64_t out[3]) -> bool {
+    for (int q = 0; q < 3; q++) out[q] = at[q];
+    const int64_t n = g.n[axis];
+    if (forward) {
+      if (at[axis] + 1 < n) out[axis] += 1;
+      else if (s->periodic(axis)) out[axis] = 0;
+      else return false;
+    } else if (at[axis] > 0) {
+      out[axis] -= 1;
+    } else if (s->periodic(axis)) {
+      out[axis] = n - 1;
+    } else {
+      return false;
+    }
+    return true;
+  };
+  auto index = [&](const int64_t at[3]) { return (at[2] * g.n[1] + at[1]) * g.n[0] + at[0]; };
+  auto held = [&](int comp, const int64_t at[3]) { return s->cb[comp][index(at)] == 0.0; };
+  struct Term { int comp; bool ok; int64_t from[3]; double coefficient; };
+  std::vector<Link> out;
+  for (int64_t k = lo[2]; k < hi[2]; k++)
+    for (int64_t j = lo[1]; j < hi[1]; j++)
+      for (int64_t i = lo[0]; i < hi[0]; i++) {
+        const int64_t at[3] = {i, j, k};
+        const int64_t r = index(at);
+        for (int c = 0; c < 3; c++) {
+          const int a = first_of(c), b = second_of(c);
+          // E_c: curl = D_a H_b - D_b H_a, back differences
+          if (!held(c, at)) {
+            const bool inside = total(0, c, at);
+            const double fa = s->kn[a][at[a]] / g.d[a], fb = s->kn[b][at[b]] / g.d[b];
+            Term t[4];
+            t[0] = {b, true, {i, j, k}, fa};
+            t[1].comp = b;
+            t[1].ok = neighbour(at, a, false, t[1].from);
+            t[1].coefficient = -fa;
+            t[2] = {a, true, {i, j, k}, -fb};
+            t[3].comp = a;
+            t[3].ok = neighbour(at, b, false, t[3].from);
+            t[3].coefficient = fb;
+            for (const Term &q : t)
+              if (q.ok && total(1, q.comp, q.from) != inside)
+                out.push_back(Link{0, c, r, (inside ? -1.0 : 1.0) * q.coefficient, 1, q.comp,
+                                   {q.from[0], q.from[1], q.from[2]}});
+          }
+          // H_c: curl = D_a E_b - D_b E_a, forward differences
+          const bool inside = total(1, c, at);
+          const double fa = s->kh[a][at[a]] / g.d[a], fb = s->kh[b][at[b]] / g.d[b];
+          Term t[4];
+          t[0].comp = b;
+          t[0].ok = neighbour(at, a, true, t[0].from);
+          t[0].coefficient = fa;
+          t[1] = {b, true, {i, j, k}, -fa};
+          t[2].comp = a;
+          t[2].ok = neighbour(at, b, true, t[2].from);
+          t[2].coefficient = -fb;
+          t[3] = {a, true, {i, j, k}, fb};
+          for (const Term &q : t)
+            if (q.ok && !held(q.comp, q.from) && total(0, q.comp, q.from) != inside)
+              out.push_back(Link{1, c, r, (inside ? 1.0 : -1.0) * q.coefficient, 0, q.comp,
+                                 {q.from[0], q.from[1], q.from[2]}});
+        }
+      }
+  return out;
+}
+
+// Simulation::uniform (src/fdtd/sources.rs:509-522): every value of E on the surface in a
+// lossless medium of eps, not a dispersive one.
+bool surface_uniform(const pxs_sim *s, const std::vector<Link> &ls, double eps) {
+  const double expected = s->dt / eps;
+  for (const Link &l : ls) {
+    const int c = l.target == 0 ? l.comp : l.from_comp;
+    const int64_t r =
+        l.target == 0 ? l.r : (l.from[2] * s->g.n[1] + l.from[1]) * s->g.n[0] + l.from[0];
+    if (!(std::fabs(s->cb[c][r] - expected) <= 1e-12 * expected && s->ca[c][r] == 1.0 &&
+          s->members.find((int64_t)c * s->N() + r) == s->members.end()))
+      return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Simulation::add_plane_wave / PlaneWaveRun::new (src/fdtd/sources.rs:716-951).
+int pxs_add_plane_wave(pxs_sim *s, const int64_t low[3], const int64_t high[3],
+                       const int64_t direction[3], const double polarization[3], double eps,
+                       const double wave[6]) {
+  if (!s || !low || !high || !direction || !polarization || !wave) return FDTD_E_INVALID;
+  if (s->fields_dropped) return s->dropped();
+  auto gcd = [](int64_t a, int64_t b) {
+    while (b != 0) {
+      const int64_t t = a % b;
+      a = b;
+      b = t;
+    }
+    return a < 0 ? -a : a;
+  };
+  PlaneRun run;
+  const int64_t divisor = gcd(gcd(direction[0], direction[1]), direction[2]);
+  if (divisor == 0) return s->fail(FDTD_E_INVALID, "a plane wave's direction can't be zero");
+  for (int a = 0; a < 3; a++) run.g[a] = direction[a] / divisor;
+  if (!(std::isfinite(eps) && eps > 0.0))
+    return s->fail(FDTD_E_INVALID, "the background's permittivity must be positive, got %g", eps);
+  const int kind = (int)wave[0];
+  if (kind < 0 || kind > 2 || (double)kind != wave[0])
+    return s->fail(FDTD_E_INVALID, "no waveform of kind %g", wave[0]);
+  bool faces[3];
+  for (int a = 0; a < 3; a++) {
+    const int64_t n = s->g.n[a];
+    faces[a] = true;
+    if (s->periodic(a)) {
+      if (low[a] != 0 || high[a] != n || run.g[a] != 0)
+        return s->fail(FDTD_E_INVALID,
+                       "along the periodic axis %d the box must be whole (0 to %lld) and the "
+                       "direction zero, got %lld to %lld and %lld",
+                       a, (long long)n, (long long)low[a], (long long)high[a],
+                       (long long)run.g[a]);
+      faces[a] = false;
+    } else {
+      const int64_t lo = s->low[a], hi = s->high[a];
+      if (low[a] < lo + 1 || high[a] + hi + 1 > n || low[a] >= high[a])
+        return s->fail(FDTD_E_INVALID,
+                       "along axis %d the box's faces, nodes %lld and %lld, must be in order and "
+                       "a cell clear of the CPMLs (%lld and %lld cells) and the ends of %lld "
+                       "cells",
+                       a, (long long)low[a], (long long)high[a], (long long)lo, (long long)hi,
+                       (long long)n);
+    }
+  }
+  for (int a = 0; a < 3; a++) run.steps[a] = s->g.d[a];
+  double gv[3], khat[3], pt[3];
+  for (int a = 0; a < 3; a++) gv[a] = (double)run.g[a] / run.steps[a];
+  double sq = 0.0;
+  for (int a = 0; a < 3; a++) sq += gv[a] * gv[a];
+  const double norm = std::sqrt(sq);
+  for (int a = 0; a < 3; a++) khat[a] = gv[a] / norm;
+  double along = 0.0;
+  for (int a = 0; a < 3; a++) along += polarization[a] * khat[a];
+  for (int a = 0; a < 3; a++) pt[a] = polarization[a] - along * khat[a];
+  double size2 = 0.0;
+  for (int a = 0; a < 3; a++) size2 += pt[a] * pt[a];
+  const double size = std::sqrt(size2);
+  if (!(std::isfinite(size) && size > 1e-12))
+    return s->fail(FDTD_E_INVALID, "the polarization has nothing across the direction");
+  for (int a = 0; a < 3; a++) pt[a] /= size;
+  auto total = [&](int field, int comp, const int64_t at[3]) {
+    for (int a = 0; a < 3; a++) {
+      if (!faces[a]) continue;
+      const int64_t t = twice(field, comp, a, at[a]);
+      if (!(t >= 2 * low[a] && t <= 2 * high[a])) return false;
+    }
+    return true;
+  };
+  int64_t rlo[3], rhi[3];
+  for (int a = 0; a < 3; a++) {
+    rlo[a] = faces[a] ? low[a] - 1 : 0;
+    rhi[a] = faces[a] ? high[a] + 2 : s->g.n[a];
+  }
+  const std::vector<Link> ls = surface_links(s, rlo, rhi, total);
+  if (!surface_uniform(s, ls, eps))
+    return s->fail(FDTD_E_INVALID,
+                   "the medium on the box's surface must be uniform, with the permittivity %g "
+                   "and no conductivity",
+                   eps);
+  int64_t least = 0, most = 0;
+  for (int a = 0; a < 3; a++) {
+    const int64_t t0 = faces[a] ? 2 * low[a] - 2 : 0, t1 = faces[a] ? 2 * high[a] + 2 : 0;
+    least += std::min(run.g[a] * t0, run.g[a] * t1);
+    most += std::max(run.g[a] * t0, run.g[a] * t1);
+  }
+  int64_t stride = 0;
+  for (int a = 0; a < 3; a++) stride = std::max<int64_t>(stride, run.g[a] < 0 ? -run.g[a] : run.g[a]);
+  const int64_t pad = stride, absorber = 200 * stride;
+  const int64_t sheet_at = least - 4 * stride - 4;
+  int64_t base = sheet_at - (absorber + 4 * stride + pad);
+  base -= ((base % 2) + 2) % 2;
+  const int64_t top = most + (4 * stride + absorber + pad);
+  const int64_t len = top - base + 1;
+  // a matched absorber at each end: sigma for E and sigma/eps for H, cubic
+  const double sample = 1.0 / (2.0 * norm);
+  const double depth = (double)absorber * sample;
+  const double sqrt_eps = std::sqrt(eps);
+  const double sigma_max = 50.0 * sqrt_eps / depth;
+  const double dt = s->dt;
+  run.ca.assign(len, 1.0);
+  run.cb.assign(len, dt / eps);
+  run.da.assign(len, 1.0);
+  run.db.assign(len, dt);
+  for (int64_t i = 0; i < len; i++) {
+    double into;
+    if (i < pad + absorber) into = (double)(pad + absorber - i);
+    else if (i + pad + absorber >= len) into = (double)(i + pad + absorber + 1 - len);
+    else continue;
+    const double v = std::min(into / (double)absorber, 1.0);
+    const double sigma = sigma_max * (v * (v * v));  // powi(v, 3): v (v v)
+    const double half_e = sigma * dt / (2.0 * eps);
+    run.ca[i] = (1.0 - half_e) / (1.0 + half_e);
+    run.cb[i] = dt / eps / (1.0 + half_e);
+    const double half_h = sigma / eps * dt / 2.0;
+    run.da[i] = (1.0 - half_h) / (1.0 + half_h);
+    run.db[i] = dt / (1.0 + half_h);
+  }
+  // the sheet: J = -2 n |G| p w where each component lives, halved over the two neighbours
+  // where the sheet's sample is the other parity
+  for (int c = 0; c < 3; c++) {
+    if (pt[c] == 0.0) continue;
+    const double j = -2.0 * sqrt_eps * norm * pt[c];
+    if ((((sheet_at - run.g[c]) % 2) + 2) % 2 == 0) {
+      run.sheet_comp.push_back(c);
+      run.sheet_i.push_back(sheet_at - base);
+      run.sheet_j.push_back(j);
+    } else {
+      for (int64_t l : {sheet_at - 1, sheet_at + 1}) {
+        run.sheet_comp.push_back(c);
+        run.sheet_i.push_back(l - base);
+        run.sheet_j.push_back(0.5 * j);
+      }
+    }
+  }
+  run.base = base;
+  run.pad = pad;
+  run.len = len;
+  run.e.assign(3 * len, 0.0);
+  run.h.assign(3 * len, 0.0);
+  run.wave.kind = kind;
+  for (int q = 0; q < 5; q++) run.wave.p[q] = wave[q + 1];
+  for (const Link &l : ls) {
+    int64_t i;
+    if (!run.sample(l.from_field, l.from_comp, l.from, &i))
+      return s->fail(FDTD_E_INVALID, "the auxiliary grid doesn't span the box");
+    PlaneRun::Coupling q{l.comp, l.r, l.weight, l.from_comp, i};
+    (l.target == 0 ? run.on_e : run.on_h).push_back(q);
+  }
+  s->plane_waves.push_back(std::move(run));
+  s->configured = false;
+  return (int)s->plane_waves.size() - 1;
+}
+
+// Simulation::incident (src/fdtd/sources.rs:729-767): plane wave n's incident field now (E at the
+// current time, H half a step behind) at a value; 0 beyond its auxiliary grid.
+int pxs_incident(pxs_sim *s, int32_t n, int32_t field, int32_t comp, int64_t i, int64_t j,
+                 int64_t k, double *out) {
+  if (!s || !out) return FDTD_E_INVALID;
+  if (n < 0 || n >= (int32_t)s->plane_waves.size() || field < 0 || field > 1 || comp < 0 ||
+      comp > 2 || !s->inside(i, j, k))
+    return s->fail(FDTD_E_INVALID, "no plane wave %d, or the value is outside the grid", (int)n);
+  if (n < s->aux_on_device && s->ctx) {
+    PlaneRun &p = s->plane_waves[n];
+    if (int r = fdtd_plane_wave_state(s->ctx, n, p.e.data(), p.h.data()))
+      return s->fail(r, "%s", fdtd_last_error(s->ctx));
+  }
+  const PlaneRun &p = s->plane_waves[n];
+  const int64_t at[3] = {i, j, k};
+  int64_t q;
+  *out = p.sample(field, comp, at, &q) ? (field == 0 ? p.e : p.h)[comp * p.len + q] : 0.0;
   return 0;
 }
 

@@ -36,6 +36,7 @@ struct InstanceView {
   int nprobes;
   const long long *probes;
   bool media;
+  bool plane_waves;  // total-field/scattered-field boxes (stepped by the engine alone)
   cudaStream_t stream;
   unsigned long long generation;  // moves on with every change the engine's calls make
 };

@@ -22,7 +22,7 @@ from typing import Optional
 import numpy as np
 
 from .types import (Boxes, Current, Dipole, Dispersive, Field, FluxPlane, GpuError, Grid3d,
-                    Growing, InvalidValue, Source)
+                    Growing, InvalidValue, PlaneWave, Source)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libphotonoxide_fdtd.so")
@@ -87,6 +87,8 @@ def library():
         x.pxs_run_until.argtypes = [P, D]
         x.pxs_run_until_decayed.argtypes = [P, I32, I32P, D, D, D, I32P, DP]
         x.pxs_waveform_spectrum.argtypes = [DP, I32, D, I64, I32, DP, DP]
+        x.pxs_add_plane_wave.argtypes = [P, I64P, I64P, I64P, DP, D, DP]
+        x.pxs_incident.argtypes = [P, I32, I32, I32, I64, I64, I64, DP]
         x.pxs_engine.restype = P
         _lib = x
     return _lib
@@ -272,6 +274,25 @@ class Simulation:
         a = complex(d.amplitude)
         self._check(library().pxs_add_dipole(self._h, int(d.field), int(d.component), pp, a.real,
                                              a.imag, wp))
+
+    def add_plane_wave(self, wave: PlaneWave) -> int:
+        """``Simulation::add_plane_wave``: a total-field/scattered-field box whose incident
+        field an auxiliary 1D run along the direction gives (stepped on the device with the
+        grid); its number, for :meth:`incident`."""
+        lo, lp = _i64(wave.low)
+        hi, hp = _i64(wave.high)
+        dr, dp = _i64(wave.direction)
+        po, pp = _d(wave.polarization)
+        w, wp = _d(wave.waveform.as_array())
+        return self._check(library().pxs_add_plane_wave(self._h, lp, hp, dp, pp, float(wave.eps),
+                                                        wp))
+
+    def incident(self, n: int, field, component, at) -> float:
+        """``Simulation::incident``: plane wave n's incident field now at a value."""
+        out = C.c_double(0.0)
+        self._check(library().pxs_incident(self._h, int(n), int(field), int(component),
+                                           *[int(v) for v in at], C.byref(out)))
+        return out.value
 
     def add_probe(self, field, component, at) -> int:
         return self._check(library().pxs_add_probe(self._h, int(field), int(component),
