@@ -95,6 +95,17 @@ int pxs_add_flux_box(pxs_sim *s, const int64_t planes[6], int32_t nf, const doub
 int pxs_add_plane_wave(pxs_sim *s, const int64_t low[3], const int64_t high[3],
                        const int64_t direction[3], const double polarization[3], double eps,
                        const double wave[6]);
+/* Simulation::add_beam (src/fdtd/sources.rs:598-714): a Gaussian beam launched from the plane of
+ * nodes `plane` normal to `axis`, forward (direction >= 0, the total field from the plane on) or
+ * back; where its axis crosses the plane (along axis.others()), its waist and the focus's distance
+ * ahead, its tilt towards `tilt` by `angle` (radians), E across the tilt's plane (parallel 0) or
+ * in it (1), the medium's eps uniform where it enters. The plane's E, decomposed into the grid's
+ * own plane waves, becomes currents on the surface, added with the waveform (which needs a
+ * carrier). The real functions beyond exp and sin/cos are the C library's (the reference's are
+ * the libm crate's), so the currents are within a few ulps of the reference's. */
+int pxs_add_beam(pxs_sim *s, int32_t axis, int64_t plane, int32_t direction,
+                 const double centre[2], double waist, double focus, int32_t tilt, double angle,
+                 int32_t parallel, double eps, const double wave[6]);
 /* Simulation::incident (src/fdtd/sources.rs:729-767): plane wave n's incident field now at a
  * value (E at the current time, H half a step behind), into *out; 0 beyond its run. */
 int pxs_incident(pxs_sim *s, int32_t n, int32_t field, int32_t comp, int64_t i, int64_t j,

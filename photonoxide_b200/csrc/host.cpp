@@ -4,6 +4,7 @@
 // through the engine's C ABI (photonoxide_fdtd.h). Compiled without floating-point contraction,
 // so every table is the reference's bits.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -1458,9 +1459,374 @@ int pxs_add_plane_wave(pxs_sim *s, const int64_t low[3], const int64_t high[3],
     PlaneRun::Coupling q{l.comp, l.r, l.weight, l.from_comp, i};
     (l.target == 0 ? run.on_e : run.on_h).push_back(q);
   }
+  if (int r = s->reconfigure()) return r;
   s->plane_waves.push_back(std::move(run));
-  s->configured = false;
   return (int)s->plane_waves.size() - 1;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Complex numbers with num-complex's arithmetic (the schoolbook product and quotient), which the
+// reference's beam set-up uses.
+struct Cx {
+  double re = 0.0, im = 0.0;
+};
+inline Cx operator+(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+inline Cx operator-(Cx a, Cx b) { return {a.re - b.re, a.im - b.im}; }
+inline Cx operator*(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline Cx operator*(Cx a, double s) { return {a.re * s, a.im * s}; }
+inline Cx operator*(double s, Cx a) { return {s * a.re, s * a.im}; }
+inline Cx operator/(Cx a, double s) { return {a.re / s, a.im / s}; }
+inline Cx operator/(Cx a, Cx b) {
+  const double n = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / n, (a.im * b.re - a.re * b.im) / n};
+}
+inline Cx operator-(Cx a) { return {-a.re, -a.im}; }
+// e^z (src/portable/complex.rs:71-93), the reference's exp and sin/cos
+inline Cx cexp(Cx z) {
+  const double r = pxp::exp(z.re);
+  if (z.im == 0.0) return {r, z.im};
+  double sn, cs;
+  pxp::sincos(z.im, &sn, &cs);
+  return {r * cs, r * sn};
+}
+inline double cabs(Cx z) { return std::hypot(z.re, z.im); }
+// the principal square root (src/portable/complex.rs:132-180) for finite z
+inline Cx csqrt(Cx z) {
+  const double x = z.re, y = z.im;
+  if (y == 0.0) {
+    if (!std::signbit(x)) return {std::sqrt(x), y};
+    return {0.0, std::copysign(std::sqrt(-x), y)};
+  }
+  const double t = std::sqrt(0.5 * (std::fabs(x) + std::hypot(x, y)));
+  if (x >= 0.0) return {t, y / (2.0 * t)};
+  return {std::fabs(y) / (2.0 * t), std::copysign(t, y)};
+}
+// asin z for finite z of moderate size (src/portable/complex.rs:336-406: Hull, Fairgrieve and
+// Tang's algorithm, ACM TOMS 23 (1997) 299, as FreeBSD's casin)
+inline Cx casin(Cx z) {
+  const double x = std::fabs(z.re), y = std::fabs(z.im);
+  const double SMALL = 0x1p-27, TINY = 0x1p-500, LARGE = 0x1p500;
+  double re, im;
+  if (std::max(x, y) < SMALL) {
+    re = x;
+    im = y;
+  } else if (std::max(x, y) >= LARGE) {
+    re = std::atan2(x, y);
+    im = std::log(std::hypot(x, y)) + 0.6931471805599453;
+  } else if (y < TINY) {
+    if (x < 1.0) {
+      re = std::asin(x);
+      im = y / std::sqrt((1.0 - x) * (1.0 + x));
+    } else if (x == 1.0) {
+      re = 1.5707963267948966;
+      im = std::sqrt(y);
+    } else {
+      re = 1.5707963267948966;
+      im = std::acosh(x);
+    }
+  } else {
+    const double xp1 = x + 1.0, r = std::hypot(xp1, y), s = std::hypot(x - 1.0, y);
+    const double a = 0.5 * (r + s), b = x / a, yy = y * y;
+    if (b <= 0.6417) {
+      re = std::asin(b);
+    } else {
+      const double apx = a + x;
+      re = x <= 1.0 ? std::atan(x / std::sqrt(0.5 * apx * (yy / (r + xp1) + (s + (1.0 - x)))))
+                    : std::atan(x / (y * std::sqrt(0.5 * (apx / (r + xp1) + apx / (s + (x - 1.0))))));
+    }
+    if (a <= 1.5) {
+      const double am1 = x < 1.0 ? 0.5 * (yy / (r + xp1) + yy / (s + (1.0 - x)))
+                                 : 0.5 * (yy / (r + xp1) + (s + (x - 1.0)));
+      im = std::log1p(am1 + std::sqrt(am1 * (a + 1.0)));
+    } else {
+      im = std::log(a + std::sqrt(a * a - 1.0));
+    }
+  }
+  return {std::copysign(re, z.re), std::copysign(im, z.im)};
+}
+
+double psin(double x) {
+  double s, c;
+  pxp::sincos(x, &s, &c);
+  return s;
+}
+double pcos(double x) {
+  double s, c;
+  pxp::sincos(x, &s, &c);
+  return c;
+}
+
+// The wavenumbers of a discrete Fourier series over n samples `step` apart
+// (src/fdtd/sources.rs:1125-1130).
+std::vector<double> wavenumbers(int64_t n, double step) {
+  const int64_t low = -((n - 1) / 2);
+  std::vector<double> out(n);
+  for (int64_t m = 0; m < n; m++)
+    out[m] = 6.283185307179586476925286766559 * (double)(low + m) / ((double)n * step);
+  return out;
+}
+
+// The separable sum of src/fdtd/sources.rs:1278-1328: from samples to waves (sign -1) or back
+// (+1), along b then along c.
+std::vector<Cx> plane_transform(const std::vector<Cx> &values, const int64_t n[2],
+                                const std::vector<double> k[2], const std::vector<double> x[2],
+                                double sign) {
+  const bool to_waves = sign < 0.0;
+  std::vector<Cx> table[2];
+  for (int t = 0; t < 2; t++) {
+    const int64_t m = n[t];
+    table[t].resize(m * m);
+    for (int64_t p = 0; p < m; p++)
+      for (int64_t q = 0; q < m; q++) {
+        const int64_t wave = to_waves ? p : q, sample = to_waves ? q : p;
+        table[t][p * m + q] = cexp(Cx{0.0, sign * k[t][wave] * x[t][sample]});
+      }
+  }
+  std::vector<Cx> along_b(n[0] * n[1]), out(n[0] * n[1]);
+  for (int64_t v = 0; v < n[1]; v++)
+    for (int64_t p = 0; p < n[0]; p++) {
+      Cx sum;
+      for (int64_t q = 0; q < n[0]; q++) sum = sum + values[v * n[0] + q] * table[0][p * n[0] + q];
+      along_b[v * n[0] + p] = sum;
+    }
+  for (int64_t p = 0; p < n[1]; p++)
+    for (int64_t u = 0; u < n[0]; u++) {
+      Cx sum;
+      for (int64_t q = 0; q < n[1]; q++) sum = sum + along_b[q * n[0] + u] * table[1][p * n[1] + q];
+      out[p * n[0] + u] = sum;
+    }
+  return out;
+}
+
+// The positions along axis.others() of field's component over the window (sources.rs:1255-1276).
+void transverse_positions(const Grid &g, int axis, const int64_t lo[2], const int64_t n[2],
+                          int field, int comp, std::vector<double> out[2]) {
+  const int bc[2] = {first_of(axis), second_of(axis)};
+  for (int t = 0; t < 2; t++) {
+    const bool half = field == 0 ? comp == bc[t] : comp != bc[t];
+    out[t].resize(n[t]);
+    for (int64_t u = 0; u < n[t]; u++)
+      out[t][u] = g.node(bc[t], lo[t] + u) + (half ? 0.5 * g.d[bc[t]] : 0.0);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Simulation::add_beam (src/fdtd/sources.rs:598-714, beam_profile :1042-1108, PlaneSpectrum
+// :1110-1353): a Gaussian beam launched one way from the plane of nodes `plane` normal to `axis`,
+// its tangential E on the plane the paraxial beam's, decomposed into the grid's own plane waves
+// over the window clear of the CPMLs, each wave's normal wavenumber the grid's at the leapfrog's
+// frequency; the waves' E and H on the planes the surface's couplings read become currents
+// (phasor_surface), added with the waveform.
+int pxs_add_beam(pxs_sim *s, int32_t axis, int64_t plane, int32_t direction,
+                 const double centre[2], double waist, double focus, int32_t tilt, double angle,
+                 int32_t parallel, double eps, const double wave[6]) {
+  if (!s || !centre || !wave || axis < 0 || axis > 2 || tilt < 0 || tilt > 2)
+    return FDTD_E_INVALID;
+  if (s->fields_dropped) return s->dropped();
+  const Grid &g = s->g;
+  const int a = axis, b = first_of(axis), c = second_of(axis);
+  auto ok = [](double v) { return std::isfinite(v) && v > 0.0; };
+  if (!ok(waist) || !ok(eps) || !std::isfinite(focus))
+    return s->fail(FDTD_E_INVALID,
+                   "a beam needs a positive waist and permittivity and a finite focus");
+  if (tilt == axis || std::isnan(angle) || std::fabs(angle) >= 1.5707963267948966 ||
+      (angle != 0.0 && !s->varies[tilt]))
+    return s->fail(FDTD_E_INVALID,
+                   "a beam tilts towards an axis across its plane along which the field varies, "
+                   "by less than 90 degrees");
+  if (s->periodic(axis))
+    return s->fail(FDTD_E_INVALID, "a beam normal to axis %d needs ends along it, not periodic "
+                                   "ones", a);
+  const int64_t n = g.n[a];
+  const int64_t lo_a = s->low[a], hi_a = s->high[a];
+  if (plane < lo_a + 1 || plane + 2 + hi_a > n)
+    return s->fail(FDTD_E_INVALID,
+                   "the beam's plane %lld and the next must be clear of the CPMLs (%lld and %lld "
+                   "cells) and the ends of %lld cells",
+                   (long long)plane, (long long)lo_a, (long long)hi_a, (long long)n);
+  // carrier_wavenumber (src/fdtd/sources.rs:487-507): the leapfrog's (2/dt) sin(omega dt/2)
+  const int kind = (int)wave[0];
+  if (kind != 0 && kind != 2)
+    return s->fail(FDTD_E_INVALID,
+                   "a beam needs a waveform with a carrier (a Gaussian or a continuous wave)");
+  const double omega = 6.283185307179586476925286766559 * wave[1];
+  if (!(omega * s->dt < 3.141592653589793238462643383279))
+    return s->fail(FDTD_E_INVALID, "the carrier is beyond the time step's Nyquist frequency");
+  const double k0 = 2.0 / s->dt * psin(omega * s->dt / 2.0);
+  int64_t wlo[2], wn[2];
+  const int bc[2] = {b, c};
+  for (int t = 0; t < 2; t++) {
+    if (s->periodic(bc[t])) {
+      wlo[t] = 0;
+      wn[t] = g.n[bc[t]];
+    } else {
+      wlo[t] = s->low[bc[t]];
+      wn[t] = g.n[bc[t]] - s->high[bc[t]] - s->low[bc[t]];
+    }
+  }
+  // beam_profile: the paraxial beam's E at a point, at unit amplitude
+  const bool forward = direction >= 0;
+  double u[3] = {0, 0, 0}, crossing[3] = {0, 0, 0}, wpt[3], sv[3] = {0, 0, 0}, pv[3];
+  u[a] = (forward ? 1.0 : -1.0) * pcos(angle);
+  u[tilt] = psin(angle);
+  crossing[a] = g.node(a, plane);
+  crossing[b] = centre[0];
+  crossing[c] = centre[1];
+  for (int q = 0; q < 3; q++) wpt[q] = crossing[q] + focus * u[q];
+  sv[3 - a - tilt] = 1.0;
+  pv[0] = sv[1] * u[2] - sv[2] * u[1];
+  pv[1] = sv[2] * u[0] - sv[0] * u[2];
+  pv[2] = sv[0] * u[1] - sv[1] * u[0];
+  if (pv[tilt] < 0.0 || (pv[tilt] == 0.0 && pv[a] < 0.0))
+    for (double &v : pv) v = -v;
+  const double *evec = parallel ? pv : sv;
+  const double k = std::sqrt(eps) * k0;
+  const double rayleigh = k * waist * waist / 2.0;
+  const int transverse = (int)s->varies[b] + (int)s->varies[c];
+  auto profile = [&](const double r[3], Cx out[3]) {
+    double rho[3] = {0, 0, 0};
+    for (int q = 0; q < 3; q++)
+      if (s->varies[q]) rho[q] = r[q] - wpt[q];
+    double z = 0.0, r2 = 0.0;
+    for (int q = 0; q < 3; q++) z += rho[q] * u[q];
+    for (int q = 0; q < 3; q++) r2 += rho[q] * rho[q];
+    r2 -= z * z;
+    const Cx qq{z, -rayleigh};
+    const Cx ratio = Cx{0.0, -rayleigh} / qq;
+    const Cx envelope = transverse >= 2 ? ratio : csqrt(ratio);
+    const Cx phase = Cx{0.0, 1.0} * (Cx{k * r2, 0.0} / (2.0 * qq) + Cx{k * z, 0.0});
+    const Cx value = envelope * cexp(phase);
+    for (int q = 0; q < 3; q++) out[q] = value * evec[q];
+  };
+  // PlaneSpectrum::new: the tangential E's waves over the window, going one way
+  const std::vector<double> kt[2] = {wavenumbers(wn[0], g.d[b]), wavenumbers(wn[1], g.d[c])};
+  std::vector<Cx> coefficients[2];
+  for (int t = 0; t < 2; t++) {
+    const int comp = bc[t];
+    std::vector<double> pos[2];
+    transverse_positions(g, a, wlo, wn, 0, comp, pos);
+    std::vector<Cx> samples(wn[0] * wn[1]);
+    for (int64_t v = 0; v < wn[1]; v++)
+      for (int64_t w = 0; w < wn[0]; w++) {
+        int64_t at[3];
+        at[a] = plane;
+        at[b] = wlo[0] + w;
+        at[c] = wlo[1] + v;
+        double p[3] = {g.node(0, at[0]), g.node(1, at[1]), g.node(2, at[2])};
+        p[comp] += 0.5 * g.d[comp];
+        Cx e[3];
+        profile(p, e);
+        samples[v * wn[0] + w] = e[comp];
+      }
+    coefficients[t] = plane_transform(samples, wn, kt, pos, -1.0);
+    const double scale = 1.0 / (double)(wn[0] * wn[1]);
+    for (Cx &x : coefficients[t]) x = x * scale;
+  }
+  const double step_a = g.d[a];
+  const double sign = forward ? 1.0 : -1.0;
+  const int64_t W = wn[0] * wn[1];
+  std::vector<Cx> ka(W);
+  std::vector<std::array<Cx, 3>> amplitude(W), big_k(W);
+  for (int64_t mc = 0; mc < wn[1]; mc++)
+    for (int64_t mb = 0; mb < wn[0]; mb++) {
+      const double kb = 2.0 / g.d[b] * psin(kt[0][mb] * g.d[b] / 2.0);
+      const double kc = 2.0 / g.d[c] * psin(kt[1][mc] * g.d[c] / 2.0);
+      const double square = eps * k0 * k0 - kb * kb - kc * kc;
+      const Cx normal =
+          (square >= 0.0 ? Cx{std::sqrt(square), 0.0} : Cx{0.0, std::sqrt(-square)}) * sign;
+      const Cx k_normal = 2.0 / step_a * casin(normal * step_a / 2.0);
+      const int64_t w = mc * wn[0] + mb;
+      const Cx eb = coefficients[0][w], ec = coefficients[1][w];
+      std::array<Cx, 3> vec{}, kvec{};
+      kvec[a] = normal;
+      kvec[b] = Cx{kb, 0.0};
+      kvec[c] = Cx{kc, 0.0};
+      if (cabs(normal) > 1e-12 * k0) {
+        vec[b] = eb;
+        vec[c] = ec;
+        vec[a] = -(Cx{kb, 0.0} * eb + Cx{kc, 0.0} * ec) / normal;
+      }
+      ka[w] = k_normal;
+      amplitude[w] = vec;
+      big_k[w] = kvec;
+    }
+  // the couplings of the beam's surface: forward, the total field from the plane on; back, up
+  // to the plane after it
+  auto total = [&](int field, int comp, const int64_t at[3]) {
+    const int64_t t = twice(field, comp, a, at[a]);
+    return forward ? t >= 2 * plane : t <= 2 * (plane + 1);
+  };
+  int64_t rlo[3], rhi[3];
+  rlo[a] = plane - 1;
+  rhi[a] = std::min(plane + 3, n);
+  rlo[b] = wlo[0];
+  rhi[b] = wlo[0] + wn[0];
+  rlo[c] = wlo[1];
+  rhi[c] = wlo[1] + wn[1];
+  const std::vector<Link> ls = surface_links(s, rlo, rhi, total);
+  if (!surface_uniform(s, ls, eps))
+    return s->fail(FDTD_E_INVALID,
+                   "the medium where the beam enters must be uniform, with its permittivity %g "
+                   "and no conductivity",
+                   eps);
+  // the waves' E and H on each plane the couplings read (synthesize, sources.rs:1229-1252)
+  std::map<std::tuple<int, int, int64_t>, std::vector<Cx>> planes;
+  for (const Link &l : ls) {
+    const auto key = std::make_tuple(l.from_field, l.from_comp, l.from[a]);
+    if (planes.count(key)) continue;
+    const int field = l.from_field, comp = l.from_comp;
+    const double offset = (double)(twice(field, comp, a, l.from[a]) - 2 * plane) * step_a / 2.0;
+    std::vector<Cx> co(W);
+    for (int64_t w = 0; w < W; w++) {
+      Cx value;
+      if (field == 0) {
+        value = amplitude[w][comp];
+      } else {
+        const int x = first_of(comp), y = second_of(comp);
+        value = (big_k[w][x] * amplitude[w][y] - big_k[w][y] * amplitude[w][x]) / k0;
+      }
+      co[w] = value * cexp(Cx{0.0, 1.0} * ka[w] * offset);
+    }
+    std::vector<double> pos[2];
+    transverse_positions(g, a, wlo, wn, field, comp, pos);
+    planes[key] = plane_transform(co, wn, kt, pos, 1.0);
+  }
+  auto incident = [&](int field, int comp, const int64_t at[3]) -> Cx {
+    const int64_t uu = at[b], vv = at[c];
+    if (uu < wlo[0] || uu >= wlo[0] + wn[0] || vv < wlo[1] || vv >= wlo[1] + wn[1]) return Cx{};
+    auto it = planes.find(std::make_tuple(field, comp, at[a]));
+    if (it == planes.end()) return Cx{};
+    return it->second[(vv - wlo[1]) * wn[0] + (uu - wlo[0])];
+  };
+  // phasor_surface (sources.rs:420-455): the couplings' currents, J for E and M for H, by value
+  if (int r = s->reconfigure()) return r;
+  for (int field = 0; field < 2; field++) {
+    std::map<std::pair<int, int64_t>, Cx> values;
+    for (const Link &l : ls) {
+      if (l.target != field) continue;
+      Cx &v = values[std::make_pair(l.comp, l.r)];
+      v = v + l.weight * incident(l.from_field, l.from_comp, l.from);
+    }
+    bool any = false;
+    for (auto &kv : values)
+      if (kv.second.re != 0.0 || kv.second.im != 0.0) any = true;
+    if (!any) continue;
+    fdtd_waveform w;
+    w.kind = kind;
+    for (int q = 0; q < 5; q++) w.p[q] = wave[q + 1];
+    s->waves.push_back(w);
+    for (auto &kv : values)
+      if (kv.second.re != 0.0 || kv.second.im != 0.0)
+        s->currents.push_back(fdtd_injection{field, kv.first.first, kv.first.second, kv.second.re,
+                                             kv.second.im, (int32_t)s->waves.size() - 1, 0});
+  }
+  return 0;
 }
 
 // Simulation::incident (src/fdtd/sources.rs:729-767): plane wave n's incident field now (E at the

@@ -21,8 +21,8 @@ from typing import Optional
 
 import numpy as np
 
-from .types import (Boxes, Current, Dipole, Dispersive, Field, FluxPlane, GpuError, Grid3d,
-                    Growing, InvalidValue, PlaneWave, Source)
+from .types import (Boxes, Current, Dipole, Dispersive, Field, FluxPlane, GaussianBeam,
+                    GpuError, Grid3d, Growing, InvalidValue, PlaneWave, Source)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libphotonoxide_fdtd.so")
@@ -89,6 +89,7 @@ def library():
         x.pxs_waveform_spectrum.argtypes = [DP, I32, D, I64, I32, DP, DP]
         x.pxs_add_plane_wave.argtypes = [P, I64P, I64P, I64P, DP, D, DP]
         x.pxs_incident.argtypes = [P, I32, I32, I32, I64, I64, I64, DP]
+        x.pxs_add_beam.argtypes = [P, I32, I64, I32, DP, D, D, I32, D, I32, D, DP]
         x.pxs_engine.restype = P
         _lib = x
     return _lib
@@ -286,6 +287,16 @@ class Simulation:
         w, wp = _d(wave.waveform.as_array())
         return self._check(library().pxs_add_plane_wave(self._h, lp, hp, dp, pp, float(wave.eps),
                                                         wp))
+
+    def add_beam(self, beam: GaussianBeam, waveform) -> None:
+        """``Simulation::add_beam``: the beam's plane waves on its surface become currents
+        with ``waveform`` (which needs a carrier)."""
+        c, cp = _d(beam.centre)
+        w, wp = _d(waveform.as_array())
+        self._check(library().pxs_add_beam(self._h, int(beam.axis), int(beam.plane),
+                                           1 if beam.forward else -1, cp, float(beam.waist),
+                                           float(beam.focus), int(beam.tilt), float(beam.angle),
+                                           1 if beam.parallel else 0, float(beam.eps), wp))
 
     def incident(self, n: int, field, component, at) -> float:
         """``Simulation::incident``: plane wave n's incident field now at a value."""

@@ -274,6 +274,26 @@ class PlaneWave:
 
 
 @dataclass(frozen=True)
+class GaussianBeam:
+    """A Gaussian beam launched from a plane of nodes, one way (``src/fdtd/sources.rs:104-133``):
+    the plane ``plane`` normal to ``axis``, ``forward`` towards +axis; ``centre`` where its axis
+    crosses the plane (along ``axis.others()``), ``waist`` w0 and the ``focus``'s distance ahead
+    (um); tilted towards ``tilt`` by ``angle`` (radians); E across the tilt's plane
+    (``parallel`` False, s) or in it (p); ``eps`` the medium's on the plane."""
+
+    axis: Axis
+    plane: int
+    forward: bool
+    centre: Tuple[float, float]
+    waist: float
+    focus: float
+    tilt: Axis
+    angle: float
+    parallel: bool
+    eps: float
+
+
+@dataclass(frozen=True)
 class FluxPlane:
     """Halfway between node planes ``plane`` and ``plane + 1`` along ``axis``, within a window
     along ``axis.others()`` (``src/fdtd/monitors.rs:212-263``)."""
