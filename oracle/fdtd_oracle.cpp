@@ -393,6 +393,15 @@ struct Sim : Base {
   std::vector<Group<T>> groups;
   std::map<std::pair<int, long>, int> members;
   std::vector<PlaneRun> plane_waves;
+  // Bloch sides (src/fdtd/bloch.rs:45-95): the wavenumbers, and with one not zero the fields'
+  // imaginary part as a second run stepped alongside, e^(ikL) along each axis
+  double bloch_k[3] = {0.0, 0.0, 0.0};
+  bool along[3] = {false, false, false};
+  c64 phase[3];
+  Sim *twin = nullptr;
+  Sim() = default;
+  Sim(const Sim &) = default;
+  ~Sim() override { delete twin; }
 
   long stride(int a) const { return a == 0 ? 1 : (a == 1 ? g.n[0] : g.n[0] * g.n[1]); }
   bool periodic(int a) const { return kind[a] == 1; }
@@ -409,15 +418,27 @@ struct Sim : Base {
     return false;
   }
 
+  // bloch::curl_bound (src/fdtd/bloch.rs:31-43): sum of w_i / h_i^2, w_i = sin^2(k h / 2) along an
+  // axis one cell long with a Bloch phase, nothing along one without, 1 along the others
+  double curl_bound() const {
+    double sum = 0.0;
+    for (int a = 0; a < 3; a++) {
+      const double h = g.d[a], hh = h * h;
+      if (periodic(a) && g.n[a] == 1) {
+        if (bloch_k[a] == 0.0) continue;
+        const double sn = refmath::ref_sin(bloch_k[a] * h / 2.0);
+        sum += (sn * sn) * (1.0 / hh);
+        continue;
+      }
+      sum += 1.0 / hh;
+    }
+    return sum;
+  }
+
   // Simulation::with_permittivity (src/fdtd.rs:680-796) after the checks
   bool init(const double *eps, double courant, std::string &err) {
     long N = g.cells();
-    double sum = 0.0;  // bloch::curl_bound (src/fdtd/bloch.rs:31-43) with k = 0
-    for (int a = 0; a < 3; a++) {
-      if (periodic(a) && g.n[a] == 1) continue;
-      double hh = g.d[a] * g.d[a];
-      sum += 1.0 / hh;
-    }
+    const double sum = curl_bound();
     if (sum == 0.0) { err = "the field varies along no axis"; return false; }
     dt64 = courant / std::sqrt(sum);
     for (int c = 0; c < 3; c++) {
@@ -649,6 +670,47 @@ struct Sim : Base {
     }
   }
 
+  // Simulation::push_current (src/fdtd/sources.rs:190-207): a current, and in a complex run the
+  // imaginary part of its values a w(t), Im(a w) = Re(-i a w), on the imaginary part.
+  void push_current(int field, const std::vector<std::pair<int, long>> &where,
+                    const std::vector<c64> &a, const Wave &w) {
+    emitters.push_back(w);
+    for (size_t q = 0; q < where.size(); q++)
+      injections.push_back(Injection{field, where[q].first, where[q].second, a[q],
+                                     (int)emitters.size() - 1, false});
+    if (twin) {
+      twin->emitters.push_back(w);
+      for (size_t q = 0; q < where.size(); q++)
+        twin->injections.push_back(Injection{field, where[q].first, where[q].second,
+                                             cmul(c64(0.0, -1.0), a[q]),
+                                             (int)twin->emitters.size() - 1, false});
+    }
+  }
+
+  // Bloch::image (src/fdtd/bloch.rs:85-95): e^(-ikL turns), num-complex's powi of the phase.
+  c64 image(int axis, long turns) const {
+    if (turns == 0 || !along[axis]) return c64(1.0, 0.0);
+    auto power = [](c64 base, unsigned long e) {  // num_traits::pow, by squaring
+      while ((e & 1) == 0) {
+        base = cmul(base, base);
+        e >>= 1;
+      }
+      if (e == 1) return base;
+      c64 acc = base;
+      while (e > 1) {
+        e >>= 1;
+        base = cmul(base, base);
+        if (e & 1) acc = cmul(acc, base);
+      }
+      return acc;
+    };
+    const long n = -turns;
+    if (n >= 0) return power(phase[axis], (unsigned long)n);
+    const c64 p = power(phase[axis], (unsigned long)(-n));
+    const double ns = p.real() * p.real() + p.imag() * p.imag();
+    return c64(p.real() / ns, 0.0 - p.imag() / ns);
+  }
+
   // PlaneWaveRun::correct (src/fdtd/sources.rs:971-991): the box's corrections from the incident
   // field now, in f64 as the reference; the f32 run rounds each correction to T.
   void correct(const PlaneRun &p, int field) {
@@ -806,12 +868,23 @@ struct Sim : Base {
         ph[f] = c64(p.real() * dt64, p.imag() * dt64);
       }
       const T *src = s.field == 0 ? e[s.comp].data() : h[s.comp].data();
+      // a complex run's values are transformed whole (src/fdtd/monitors.rs:127-154)
+      const T *isrc = !twin ? nullptr : (s.field == 0 ? twin->e[s.comp].data() : twin->h[s.comp].data());
       long vol = s.volume();
 #pragma omp parallel for schedule(static)
       for (long o = 0; o < vol; o++) {
         long i = s.lo[0] + o % s.len[0], j = s.lo[1] + (o / s.len[0]) % s.len[1],
              k = s.lo[2] + o / (s.len[0] * s.len[1]);
         double v = (double)src[k * plane + j * nx + i];
+        if (isrc) {
+          const double w = (double)isrc[k * plane + j * nx + i];
+          for (size_t f = 0; f < ph.size(); f++) {
+            c64 &acc = s.values[f * vol + o];
+            const c64 x = cmul(c64(v, w), ph[f]);
+            acc = c64(acc.real() + x.real(), acc.imag() + x.imag());
+          }
+          continue;
+        }
         for (size_t f = 0; f < ph.size(); f++) {
           c64 &acc = s.values[f * vol + o];
           acc = c64(acc.real() + v * ph[f].real(), acc.imag() + v * ph[f].imag());
@@ -821,8 +894,8 @@ struct Sim : Base {
   }
 
   // Simulation::step (src/fdtd.rs:1319-1419)
-  void step() {
-    double t = (double)steps * dt64, half = t + 0.5 * dt64;
+  // Simulation::step_h / step_e / finish_step (src/fdtd.rs:1344-1419)
+  void step_h(double t) {
     curl_update(1);
     update_slabs(1);
     inject(1, t);
@@ -830,6 +903,8 @@ struct Sim : Base {
       correct(p, 1);
       p.step_h();
     }
+  }
+  void step_e(double half) {
     media_save();
     curl_update(0);
     update_slabs(0);
@@ -838,6 +913,8 @@ struct Sim : Base {
       correct(p, 0);
       p.step_e(half);
     }
+  }
+  void finish_step() {
     media_update();
     steps += 1;
     for (Probe &p : probes)
@@ -846,6 +923,71 @@ struct Sim : Base {
     for (Dft &d : dfts) record_dft(d, te, th);
     for (Flux &f : fluxes)
       for (Dft &d : f.dfts) record_dft(d, te, th);
+  }
+
+  // Bloch::wrap (src/fdtd/bloch.rs:97-152): after `field`'s update in both parts, each value
+  // whose difference along a Bloch axis reached across the side read the other end's value of
+  // its own part; it gets the difference e^(+-ikL) makes, (e^(+-ikL) - 1) F, in both parts.
+  void wrap(int field) {
+    const bool forward = field == 1;
+    for (int w = 0; w < 3; w++) {
+      if (!along[w]) continue;
+      const long n = g.n[w];
+      const long m = forward ? n - 1 : 0;
+      long o = 0;
+      offset(w, m, forward, &o);
+      const c64 ph = forward ? phase[w] : std::conj(phase[w]);
+      const double kappa = forward ? kh64[w][m] : kn64[w][m];
+      const double factor = kappa / g.d[w];
+      long lo[3] = {0, 0, 0}, hi[3] = {g.n[0], g.n[1], g.n[2]};
+      lo[w] = m;
+      hi[w] = m + 1;
+      for (int c = 0; c < 3; c++) {
+        if (c == w) continue;
+        const int a = first_of(c), b = second_of(c);
+        double sign = w == a ? 1.0 : -1.0;
+        const int d = w == a ? b : a;
+        if (!forward) sign = -sign;
+        const std::vector<T> &src_re = forward ? e[d] : h[d];
+        const std::vector<T> &src_im = forward ? twin->e[d] : twin->h[d];
+        std::vector<T> &dst_re = forward ? h[c] : e[c];
+        std::vector<T> &dst_im = forward ? twin->h[c] : twin->e[c];
+        for (long k = lo[2]; k < hi[2]; k++)
+          for (long j = lo[1]; j < hi[1]; j++)
+            for (long i = lo[0]; i < hi[0]; i++) {
+              const long r = (k * g.n[1] + j) * g.n[0] + i, q = r + o;
+              const c64 f((double)src_re[q], (double)src_im[q]);
+              const c64 x = cmul(c64(ph.real() - 1.0, ph.imag()), f);
+              const c64 curl(x.real() * (sign * factor), x.imag() * (sign * factor));
+              if (forward) {
+                dst_re[r] = dst_re[r] - (T)(dt64 * curl.real());
+                dst_im[r] = dst_im[r] - (T)(dt64 * curl.imag());
+              } else {
+                dst_re[r] = dst_re[r] + (T)(cb64[c][r] * curl.real());
+                dst_im[r] = dst_im[r] + (T)(cb64[c][r] * curl.imag());
+              }
+            }
+      }
+    }
+  }
+
+  // Simulation::step (src/fdtd.rs:1319-1343): with a Bloch phase the imaginary part steps
+  // alongside, each half step followed by the two parts' coupling; its media, probes and
+  // monitors go first, then the real part's (whose monitors take both parts).
+  void step() {
+    double t = (double)steps * dt64, half = t + 0.5 * dt64;
+    step_h(t);
+    if (twin) {
+      twin->step_h(t);
+      wrap(1);
+    }
+    step_e(half);
+    if (twin) {
+      twin->step_e(half);
+      wrap(0);
+      twin->finish_step();
+    }
+    finish_step();
   }
 };
 
@@ -995,9 +1137,30 @@ int orc_sample_boxes(const long n[3], const double d[3], const double o[3], cons
   return 0;
 }
 
+orc_sim *orc_create_bloch(int precision, const long n[3], const double d[3], const double o[3],
+                          const int kind[3], const long low[3], const long high[3],
+                          const double cpml[5], const double bloch[3], double courant,
+                          const double *eps, char *err, int errlen);
+
 orc_sim *orc_create(int precision, const long n[3], const double d[3], const double o[3],
                     const int kind[3], const long low[3], const long high[3], const double cpml[5],
                     double courant, const double *eps, char *err, int errlen) {
+  const double none[3] = {0.0, 0.0, 0.0};
+  return orc_create_bloch(precision, n, d, o, kind, low, high, cpml, none, courant, eps, err,
+                          errlen);
+}
+
+// Simulation::with_permittivity with Bloch sides (src/fdtd.rs:680-796, src/fdtd/bloch.rs:59-83):
+// a side periodic along an axis with bloch[axis] != 0 makes the fields complex.
+orc_sim *orc_create_bloch(int precision, const long n[3], const double d[3], const double o[3],
+                          const int kind[3], const long low[3], const long high[3],
+                          const double cpml[5], const double bloch[3], double courant,
+                          const double *eps, char *err, int errlen) {
+  for (int a = 0; a < 3; a++)
+    if (!std::isfinite(bloch[a]) || (bloch[a] != 0.0 && kind[a] != 1)) {
+      fill(err, errlen, "a Bloch wavenumber must be finite, on a periodic axis");
+      return nullptr;
+    }
   // the checks of with_permittivity (src/fdtd.rs:686-724)
   auto ok = [](double v) { return std::isfinite(v) && v > 0.0; };
   if (n[0] * n[1] * n[2] <= 0 || !ok(d[0]) || !ok(d[1]) || !ok(d[2])) {
@@ -1027,6 +1190,7 @@ orc_sim *orc_create(int precision, const long n[3], const double d[3], const dou
       s->high[a] = kind[a] == 0 ? high[a] : 0;
     }
     for (int i = 0; i < 5; i++) s->cpml[i] = cpml[i];
+    for (int a = 0; a < 3; a++) s->bloch_k[a] = bloch[a];
     std::string m;
     if (!s->init(eps, courant, m)) {
       fill(err, errlen, m);
@@ -1034,6 +1198,15 @@ orc_sim *orc_create(int precision, const long n[3], const double d[3], const dou
       return nullptr;
     }
     s->materialize();
+    if (bloch[0] != 0.0 || bloch[1] != 0.0 || bloch[2] != 0.0) {
+      for (int a = 0; a < 3; a++) {
+        s->along[a] = bloch[a] != 0.0;
+        double sn, cs;  // from_polar(1, k L)
+        refmath::ref_sincos(bloch[a] * ((double)n[a] * d[a]), &sn, &cs);
+        s->phase[a] = c64(1.0 * cs, 1.0 * sn);
+      }
+      s->twin = new typename std::remove_reference<decltype(*s)>::type(*s);
+    }
     return reinterpret_cast<orc_sim *>(static_cast<Base *>(s));
   };
   if (precision == 32) return build(new Sim<float>());
@@ -1044,7 +1217,7 @@ void orc_destroy(orc_sim *s) { delete reinterpret_cast<Base *>(s); }
 
 int orc_conductivity(orc_sim *s, const double *sigma, char *err, int errlen) {
   // Simulation::conductivity (src/fdtd.rs:949-992)
-  return with(s, [&](auto &x) -> int {
+  auto body = [&](auto &x) -> int {
     if (!x.groups.empty()) {
       fill(err, errlen, "the conductivity comes before the dispersive media");
       return -1;
@@ -1064,11 +1237,18 @@ int orc_conductivity(orc_sim *s, const double *sigma, char *err, int errlen) {
       }
     x.refresh_coefficients();
     return 0;
+  };
+  // a Bloch run's imaginary part takes it too (src/fdtd.rs:962-964, 1005-1007;
+  // src/fdtd/media.rs:756-759)
+  return with(s, [&](auto &x) -> int {
+    if (x.twin)
+      if (int r = body(*x.twin)) return r;
+    return body(x);
   });
 }
 
 int orc_conductor(orc_sim *s, int comp, long i, long j, long k) {
-  return with(s, [&](auto &x) -> int {  // src/fdtd.rs:995-1008
+  auto body = [&](auto &x) -> int {  // src/fdtd.rs:995-1008
     long r = (k * x.g.n[1] + j) * x.g.n[0] + i;
     x.ca64[comp][r] = x.cb64[comp][r] = 0.0;
     x.ca[comp][r] = x.cb[comp][r] = 0;
@@ -1089,6 +1269,13 @@ int orc_conductor(orc_sim *s, int comp, long i, long j, long k) {
       x.members.erase(it);
     }
     return 0;
+  };
+  // a Bloch run's imaginary part takes it too (src/fdtd.rs:962-964, 1005-1007;
+  // src/fdtd/media.rs:756-759)
+  return with(s, [&](auto &x) -> int {
+    if (x.twin)
+      if (int r = body(*x.twin)) return r;
+    return body(x);
   });
 }
 
@@ -1116,13 +1303,14 @@ int orc_add_current(orc_sim *s, int field, long count, const int *comps, const l
         return -1;
       if (!std::isfinite(amps[2 * q]) || !std::isfinite(amps[2 * q + 1])) return -1;
     }
-    x.emitters.push_back(Wave::from(wave));
+    std::vector<std::pair<int, long>> where;
+    std::vector<c64> a;
     for (long q = 0; q < count; q++) {
       const long *p = at + 3 * q;
-      x.injections.push_back(Injection{field, comps[q], (p[2] * x.g.n[1] + p[1]) * x.g.n[0] + p[0],
-                                       c64(amps[2 * q], amps[2 * q + 1]),
-                                       (int)x.emitters.size() - 1, false});
+      where.push_back({comps[q], (p[2] * x.g.n[1] + p[1]) * x.g.n[0] + p[0]});
+      a.push_back(c64(amps[2 * q], amps[2 * q + 1]));
     }
+    x.push_current(field, where, a, Wave::from(wave));
     return 0;
   });
 }
@@ -1162,6 +1350,33 @@ int orc_add_dipole(orc_sim *s, int field, int comp, const double pos[3], double 
       wt[axis][1] = f;
     }
     std::map<long, c64> values;
+    if (x.twin) {  // a Bloch run: each value beyond a periodic end takes its image's phase
+      c64 cw[3][2];
+      for (int axis = 0; axis < 3; axis++)
+        for (int q = 0; q < 2; q++) {
+          c64 image(1.0, 0.0);
+          if (x.varies[axis] && x.periodic(axis)) {
+            const double sp = (pos[axis] - (x.g.node(axis, 0) +
+                                            ((field == 0 ? comp == axis : comp != axis)
+                                                 ? 0.5 * x.g.d[axis] : 0.0))) / x.g.d[axis];
+            const long m = (long)std::floor(sp) + q, n = x.g.n[axis];
+            const long turns = m >= 0 ? m / n : -((-m + n - 1) / n);
+            image = x.image(axis, turns);
+          }
+          cw[axis][q] = c64(image.real() * wt[axis][q], image.imag() * wt[axis][q]);
+        }
+      for (int p = 0; p < 2; p++)
+        for (int q = 0; q < 2; q++)
+          for (int r = 0; r < 2; r++) {
+            const c64 w = cmul(cmul(cw[0][p], cw[1][q]), cw[2][r]);
+            if (w.real() != 0.0 || w.imag() != 0.0) {
+              long at = (idx[2][r] * x.g.n[1] + idx[1][q]) * x.g.n[0] + idx[0][p];
+              c64 add = cmul(a, c64(w.real() / volume, w.imag() / volume));
+              c64 &acc = values[at];
+              acc = c64(acc.real() + add.real(), acc.imag() + add.imag());
+            }
+          }
+    } else
     for (int p = 0; p < 2; p++)
       for (int q = 0; q < 2; q++)
         for (int r = 0; r < 2; r++) {
@@ -1174,10 +1389,13 @@ int orc_add_dipole(orc_sim *s, int field, int comp, const double pos[3], double 
             acc = c64(acc.real() + add.real(), acc.imag() + add.imag());
           }
         }
-    x.emitters.push_back(Wave::from(wave));
-    for (auto &kv : values)
-      x.injections.push_back(
-          Injection{field, comp, kv.first, kv.second, (int)x.emitters.size() - 1, false});
+    std::vector<std::pair<int, long>> where;
+    std::vector<c64> amounts;
+    for (auto &kv : values) {
+      where.push_back({comp, kv.first});
+      amounts.push_back(kv.second);
+    }
+    x.push_current(field, where, amounts, Wave::from(wave));
     return 0;
   });
 }
@@ -1188,6 +1406,7 @@ int orc_add_probe(orc_sim *s, int field, int comp, long i, long j, long k) {
     typename std::remove_reference<decltype(x)>::type::Probe p{
         field, comp, (k * x.g.n[1] + j) * x.g.n[0] + i, {}};
     x.probes.push_back(p);
+    if (x.twin) x.twin->probes.push_back(p);
     return (int)x.probes.size() - 1;
   });
 }
@@ -1266,7 +1485,7 @@ int orc_add_flux_box(orc_sim *s, const long planes[6], int nf, const double *fre
 
 int orc_add_medium(orc_sim *s, double eps_inf, int npoles, const double *poles,
                    const unsigned char *inside, int check_stability, char *err, int errlen) {
-  return with(s, [&](auto &x) -> int {  // Simulation::medium (src/fdtd/media.rs:741-825)
+  auto body = [&](auto &x) -> int {  // Simulation::medium (src/fdtd/media.rs:741-825)
     using T = typename std::remove_reference<decltype(x.dt)>::type;
     if (x.steps > 0) {
       fill(err, errlen, "a dispersive medium goes in before the run starts");
@@ -1299,12 +1518,7 @@ int orc_add_medium(orc_sim *s, double eps_inf, int npoles, const double *poles,
         sigmas.push_back(std::max(sg, 0.0));
       }
     if (check_stability) {
-      double top = 0.0;
-      for (int a = 0; a < 3; a++) {
-        if (x.periodic(a) && x.g.n[a] == 1) continue;
-        top += 1.0 / (x.g.d[a] * x.g.d[a]);
-      }
-      top *= 4.0;
+      const double top = 4.0 * x.curl_bound();
       double largest = 0.0;
       for (double sg : sigmas) largest = std::max(largest, sg);
       for (double sg : {0.0, largest})
@@ -1361,6 +1575,13 @@ int orc_add_medium(orc_sim *s, double eps_inf, int npoles, const double *poles,
       x.groups.push_back(gr);
     }
     return 0;
+  };
+  // a Bloch run's imaginary part takes it too (src/fdtd.rs:962-964, 1005-1007;
+  // src/fdtd/media.rs:756-759)
+  return with(s, [&](auto &x) -> int {
+    if (x.twin)
+      if (int r = body(*x.twin)) return r;
+    return body(x);
   });
 }
 
@@ -1575,6 +1796,9 @@ int orc_add_plane_wave(orc_sim *s, const long low[3], const long high[3], const 
                        const double pol[3], double eps, const double *wave, char *err,
                        int errlen) {
   return with(s, [&](auto &x) -> int {
+    if (x.twin)  // Simulation::real_run (src/fdtd/sources.rs:209-221)
+      return fill(err, errlen, "a plane wave needs real fields: with a Bloch phase, launch a "
+                               "Current with it instead"), -1;
     auto gcd = [](long a, long b) {
       while (b != 0) {
         const long t = a % b;
@@ -1711,6 +1935,34 @@ double orc_incident(const orc_sim *s, int n, int field, int comp, long i, long j
     if (n < 0 || n >= (int)x.plane_waves.size()) return 0.0;
     const long at[3] = {i, j, k};
     return x.plane_waves[n].value(field, comp, at);
+  });
+}
+
+// The host threads the oracle's loops use (a column of a few hundred cells runs fastest on one).
+int orc_threads(int n) {
+  const int before = omp_get_max_threads();
+  if (n > 0) omp_set_num_threads(n);
+  return before;
+}
+
+// A complex run's imaginary part (src/fdtd.rs:911-935, 1094-1110): 1 if the run is complex.
+int orc_is_complex(const orc_sim *s) {
+  return with(s, [&](auto &x) -> int { return x.twin ? 1 : 0; });
+}
+int orc_get_field_imag(const orc_sim *s, int field, int comp, double *out) {
+  return with(s, [&](auto &x) -> int {
+    if (!x.twin) return -1;
+    const auto &v = field == 0 ? x.twin->e[comp] : x.twin->h[comp];
+    for (size_t r = 0; r < v.size(); r++) out[r] = (double)v[r];
+    return 0;
+  });
+}
+long orc_probe_imag(const orc_sim *s, int p, double *out) {
+  return with(s, [&](auto &x) -> long {
+    if (!x.twin) return -1;
+    const auto &v = x.twin->probes[p].values;
+    if (out) std::copy(v.begin(), v.end(), out);
+    return (long)v.size();
   });
 }
 

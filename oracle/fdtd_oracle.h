@@ -44,6 +44,17 @@ int orc_sample_boxes(const long n[3], const double d[3], const double o[3], cons
 orc_sim *orc_create(int precision, const long n[3], const double d[3], const double o[3],
                     const int kind[3], const long low[3], const long high[3], const double cpml[5],
                     double courant, const double *eps, char *err, int errlen);
+/* The same with Bloch sides: bloch[a] != 0 on a periodic axis makes the fields complex, the
+ * imaginary part a second run stepped alongside (src/fdtd/bloch.rs). */
+orc_sim *orc_create_bloch(int precision, const long n[3], const double d[3], const double o[3],
+                          const int kind[3], const long low[3], const long high[3],
+                          const double cpml[5], const double bloch[3], double courant,
+                          const double *eps, char *err, int errlen);
+int orc_is_complex(const orc_sim *s);
+/* Sets the host threads of the oracle's loops (n > 0); returns the number before. */
+int orc_threads(int n);
+int orc_get_field_imag(const orc_sim *s, int field, int comp, double *out);
+long orc_probe_imag(const orc_sim *s, int p, double *out);
 void orc_destroy(orc_sim *s);
 
 int orc_conductivity(orc_sim *s, const double *sigma, char *err, int errlen);

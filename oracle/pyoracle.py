@@ -76,6 +76,14 @@ def lib():
         x.orc_triad.restype = D
         x.orc_waveform_spectrum.argtypes = [DP, C.c_int, D, L, C.c_int, DP, DP]
         x.orc_add_plane_wave.argtypes = [P, LP, LP, LP, DP, D, DP, C.c_char_p, C.c_int]
+        x.orc_create_bloch.restype = P
+        x.orc_create_bloch.argtypes = [C.c_int, LP, DP, DP, IP, LP, LP, DP, DP, D, DP,
+                                       C.c_char_p, C.c_int]
+        x.orc_is_complex.argtypes = [P]
+        x.orc_threads.argtypes = [C.c_int]
+        x.orc_get_field_imag.argtypes = [P, C.c_int, C.c_int, DP]
+        x.orc_probe_imag.argtypes = [P, C.c_int, DP]
+        x.orc_probe_imag.restype = L
         x.orc_incident.argtypes = [P, C.c_int, C.c_int, C.c_int, L, L, L]
         x.orc_incident.restype = D
         _lib = x
@@ -136,9 +144,10 @@ class OracleSimulation:
         err = C.create_string_buffer(512)
         keep = [_l(n), _d(d), _d(o), _i(kind), _l(low), _l(high), _d(boundaries.cpml.as_array()),
                 _d(eps)]
-        h = lib().orc_create(precision, keep[0][1], keep[1][1], keep[2][1], keep[3][1],
-                             keep[4][1], keep[5][1], keep[6][1], float(courant), keep[7][1], err,
-                             512)
+        bloch = _d(boundaries.bloch() if hasattr(boundaries, "bloch") else [0.0, 0.0, 0.0])
+        h = lib().orc_create_bloch(precision, keep[0][1], keep[1][1], keep[2][1], keep[3][1],
+                                   keep[4][1], keep[5][1], keep[6][1], bloch[1], float(courant),
+                                   keep[7][1], err, 512)
         if not h:
             raise InvalidValue(err.value.decode())
         self._h = h
@@ -212,6 +221,32 @@ class OracleSimulation:
     def incident(self, n: int, field, component, at) -> float:
         return float(lib().orc_incident(self._h, int(n), int(field), int(component),
                                         *[int(v) for v in at]))
+
+    @property
+    def is_complex(self) -> bool:
+        return bool(lib().orc_is_complex(self._h))
+
+    def _imag(self, field, component):
+        out = np.empty(self.grid.cells())
+        if lib().orc_get_field_imag(self._h, int(field), int(component),
+                                    out.ctypes.data_as(DP)):
+            raise InvalidValue("the fields are real: no Bloch phase")
+        return out
+
+    def e_imaginary(self, component) -> np.ndarray:
+        return self._imag(0, component)
+
+    def h_imaginary(self, component) -> np.ndarray:
+        return self._imag(1, component)
+
+    def probe_complex(self, n: int) -> np.ndarray:
+        re = self.probe(n)
+        if not self.is_complex:
+            return re + 0j
+        count = lib().orc_probe_imag(self._h, int(n), None)
+        im = np.empty(count)
+        lib().orc_probe_imag(self._h, int(n), im.ctypes.data_as(DP))
+        return re + 1j * im
 
     def add_probe(self, field, component, at) -> int:
         r = lib().orc_add_probe(self._h, int(field), int(component), *[int(v) for v in at])
@@ -317,3 +352,8 @@ def waveform_spectrum(waveform, field, dt: float, steps: int, frequencies) -> np
                                    out.ctypes.data_as(DP)) != 0:
         raise InvalidValue("a waveform's spectrum needs dt > 0 and steps >= 0")
     return out[0::2] + 1j * out[1::2]
+
+
+def threads(n: int) -> int:
+    """Sets the host threads the oracle's loops use; returns the number before."""
+    return int(lib().orc_threads(int(n)))

@@ -130,6 +130,15 @@ class Periodic:
 
 
 @dataclass(frozen=True)
+class Bloch:
+    """A Bloch-periodic axis (the reference's ``Edges::Bloch { k }``, ``src/fdtd.rs:206-256``):
+    one period on, the field is e^(ikL) times itself; k (rad/um) not zero makes the fields
+    complex (``src/fdtd/bloch.rs``)."""
+
+    k: float
+
+
+@dataclass(frozen=True)
 class Cpml:
     """The convolutional PML's parameters (``src/fdtd.rs:83-118``)."""
 
@@ -171,13 +180,18 @@ class Boundaries:
         return (self.x, self.y, self.z)[axis]
 
     def periodic(self, axis: int) -> bool:
-        return isinstance(self.edges(axis), Periodic)
+        return isinstance(self.edges(axis), (Periodic, Bloch))
+
+    def bloch(self) -> List[float]:
+        """Each axis' Bloch wavenumber (0 for a plain periodic side or a CPML)."""
+        return [float(self.edges(a).k) if isinstance(self.edges(a), Bloch) else 0.0
+                for a in range(3)]
 
     def as_arrays(self):
         kind, low, high = [], [], []
         for a in range(3):
             e = self.edges(a)
-            if isinstance(e, Periodic):
+            if isinstance(e, (Periodic, Bloch)):
                 kind.append(1), low.append(0), high.append(0)
             else:
                 kind.append(0), low.append(int(e.low)), high.append(int(e.high))
