@@ -169,6 +169,27 @@ typedef struct {
 int fdtd_set_plane_waves(fdtd_ctx *ctx, int32_t count, const fdtd_plane_wave *waves);
 /* Plane wave n's auxiliary state now: E and H, 3 x len each (either may be NULL). */
 int fdtd_plane_wave_state(fdtd_ctx *ctx, int32_t n, double *e, double *h);
+/* A coupling across a Bloch side (Bloch::wrap, src/fdtd/bloch.rs:97-152) of a complex run: after
+ * `field`'s update, value r of component `comp` gets (e^(+-ikL) - 1) F s, F = (real, imaginary)
+ * of component `from_comp` at q across the side (both parts' E before the step for H, field 1;
+ * their new H for E, field 0); phase = e^(ikL) - 1 for H and e^(-ikL) - 1 for E; s = its sign
+ * times kappa / step. H's: dt times it subtracted in the step as the point-2 injection of Bloch
+ * slot `slot` (after the plane waves' slots); E's: cb times it added. */
+typedef struct {
+  int32_t field, comp, from_comp, slot;
+  int64_t r, q;
+  double phase_re, phase_im, s, cb;
+} fdtd_wrap;
+/* The Bloch slots a context's point-2 injections may name after its plane waves'; call before
+ * fdtd_set_sources. */
+int fdtd_set_bloch_slots(fdtd_ctx *ctx, int32_t nslots);
+/* A complex run's steps (src/fdtd.rs:1319-1343): `re` and `im` hold the fields' real and
+ * imaginary parts (the same grid, coefficients and media; im with the currents' imaginary
+ * amplitudes and the same probes); both step together with the couplings, re's transforms
+ * taking both parts. No counterpart in the reference's GPU path, which refuses Bloch phases
+ * (gpu.rs:427). */
+int fdtd_bloch_run(fdtd_ctx *re, fdtd_ctx *im, int32_t nwraps, const fdtd_wrap *wraps,
+                   int64_t steps, int64_t first_step);
 /* The probes: field, component and index of each value recorded after every step. */
 int fdtd_set_probes(fdtd_ctx *ctx, int32_t n, const int32_t *field, const int32_t *component,
                     const int64_t *r);

@@ -59,6 +59,22 @@ pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], co
                     const int64_t low[3], const int64_t high[3], const double cpml[5],
                     double courant, const double *eps, const pxs_geometry *geometry,
                     int32_t precision, size_t hbm_budget, char *err, int32_t errlen);
+/* The same with Bloch sides (src/fdtd.rs:206-256, src/fdtd/bloch.rs): bloch[a] (rad/um) on a
+ * periodic axis (kind 1); one not zero makes the fields complex, the imaginary part a second
+ * simulation stepped alongside and coupled across the sides (pxs_is_complex). Its time step
+ * counts sin^2(k d / 2) along an axis one cell long. Plane waves and beams are refused in a
+ * complex run; batches, the adjoint and the serving loop refuse one. */
+pxs_sim *pxs_create_bloch(const int64_t n[3], const double d[3], const double o[3],
+                          const int32_t kind[3], const int64_t low[3], const int64_t high[3],
+                          const double cpml[5], const double bloch[3], double courant,
+                          const double *eps, const pxs_geometry *geometry, int32_t precision,
+                          size_t hbm_budget, char *err, int32_t errlen);
+/* Whether the fields are complex; their imaginary part (src/fdtd.rs:911-935) and a probe's
+ * (probe_complex, src/fdtd.rs:1094-1110). */
+int pxs_is_complex(const pxs_sim *s);
+int pxs_get_field_imag(pxs_sim *s, int32_t field, int32_t comp, double *out);
+int pxs_set_field_imag(pxs_sim *s, int32_t field, int32_t comp, const double *in);
+int64_t pxs_probe_imag(pxs_sim *s, int32_t n, double *out);
 void pxs_destroy(pxs_sim *s);
 const char *pxs_last_error(const pxs_sim *s);
 

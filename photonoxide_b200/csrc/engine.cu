@@ -1973,6 +1973,50 @@ __global__ void __launch_bounds__(1024) aux_kernel(const AuxDev *runs, int nw, i
   }
 }
 
+// One coupling across a Bloch side (Bloch::wrap, src/fdtd/bloch.rs:97-152): value r of
+// component c reads component d at q across the side; (pr, pi) = e^(+-ikL) - 1, s = its sign
+// times kappa / step; for E's, cb the value's; for H's, its slot among the step's values.
+struct WrapDev {
+  long long r, q;
+  int c, d;
+  double pr, pi, s, cb;
+  int slot, pad;
+};
+
+// H's couplings: this step's amounts dt Re and dt Im of (e^(ikL) - 1) F s, F both parts' E now,
+// into each part's step values (the step kernels subtract them after H's sources).
+template <typename T>
+__global__ void bloch_h_kernel(const WrapDev *w, int n, const T *e_re, const T *e_im,
+                               long long N, double dt, double *vals_re, double *vals_im) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const WrapDev x = w[k];
+  const double fr = (double)e_re[x.d * N + x.q], fi = (double)e_im[x.d * N + x.q];
+  const double cr = x.pr * fr - x.pi * fi, ci = x.pr * fi + x.pi * fr;
+  vals_re[2 * x.slot] = dt * (cr * x.s);
+  vals_re[2 * x.slot + 1] = 0.0;
+  vals_im[2 * x.slot] = dt * (ci * x.s);
+  vals_im[2 * x.slot + 1] = 0.0;
+}
+
+// E's couplings after both parts' E updates: E += cb Re and Im of (e^(-ikL) - 1) F s, F both
+// parts' new H; one thread a value, its couplings (one per Bloch axis) in the reference's order.
+template <typename T>
+__global__ void bloch_e_kernel(const WrapDev *w, const int *start, int nvalues, const T *h_re,
+                               const T *h_im, long long N, T *e_re, T *e_im) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nvalues) return;
+  for (int k = start[v]; k < start[v + 1]; k++) {
+    const WrapDev x = w[k];
+    const double fr = (double)h_re[x.d * N + x.q], fi = (double)h_im[x.d * N + x.q];
+    const double cr = x.pr * fr - x.pi * fi, ci = x.pr * fi + x.pi * fr;
+    T &a = e_re[x.c * N + x.r];
+    a = a + (T)(x.cb * (cr * x.s));
+    T &b = e_im[x.c * N + x.r];
+    b = b + (T)(x.cb * (ci * x.s));
+  }
+}
+
 // After a step: the probes' values into the record, the transformed values into the ring.
 template <typename T>
 __global__ void gather_kernel(const T *e, const T *h, const long long *where, int count,
@@ -2026,6 +2070,33 @@ __global__ void dft_kernel(const SeriesDev *series, int nseries, const long long
       double x = (double)ring[(long long)m * nvalues + v];
       re = re + x * ph[2 * (long long)m * nslots];
       im = im + x * ph[2 * (long long)m * nslots + 1];
+    }
+    acc[0] = re;
+    acc[1] = im;
+  }
+}
+
+// The transform of a complex run's values (src/fdtd/monitors.rs:127-154): each step's
+// (re + i im) times its phase added to the sums in time order, the real parts from `ring`, the
+// imaginary from `ring_im`.
+template <typename T>
+__global__ void dft_complex_kernel(const SeriesDev *series, const long long *value_series,
+                                   long long nvalues, const T *ring, const T *ring_im, int batch,
+                                   const double *phase, int nslots, double *sums) {
+  long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nvalues) return;
+  SeriesDev s = series[value_series[v]];
+  long long o = v - s.value0;
+  for (int f = 0; f < s.nf; f++) {
+    double *acc = sums + 2 * (s.sum0 + (long long)f * s.volume + o);
+    double re = acc[0], im = acc[1];
+    const double *ph = phase + 2 * (long long)(s.slot0 + f);
+    for (int m = 0; m < batch; m++) {
+      const double x = (double)ring[(long long)m * nvalues + v];
+      const double y = (double)ring_im[(long long)m * nvalues + v];
+      const double pr = ph[2 * (long long)m * nslots], pi = ph[2 * (long long)m * nslots + 1];
+      re = re + (x * pr - y * pi);
+      im = im + (x * pi + y * pr);
     }
     acc[0] = re;
     acc[1] = im;
@@ -2131,11 +2202,12 @@ struct fdtd_ctx {
   // plane waves' auxiliary runs (fdtd_set_plane_waves): their descriptors (pointing into device
   // memory), and the slots their couplings read, recorded each step after the emitters' values
   int naux_runs = 0, naux = 0;
-  int naux_laid = 0;  // the slot count fdtd_set_sources laid the step's values out for
+  int nbloch = 0;     // slots of H's couplings across Bloch sides (fdtd_set_bloch_slots), after
+  int naux_laid = 0;  // the plane waves'; the slot count fdtd_set_sources laid the values out for
   std::vector<AuxDev> aux;
   std::vector<void *> aux_memory;
   AuxDev *d_aux = nullptr;
-  int stride() const { return nwaves + naux; }
+  int stride() const { return nwaves + naux + nbloch; }
   // probes and transforms
   int nprobes = 0;
   long long *d_probes = nullptr;
@@ -2387,7 +2459,7 @@ void launch_staged(fdtd_ctx *c, const StepArgs<T> &A) {
 }
 
 template <typename T>
-void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
+void launch_step(fdtd_ctx *c, const StepArgs<T> &A, bool ade = true) {
   if (c->quad) {
     dim3 grid(c->tiles_x * c->tiles_y * c->zchunks);
     const size_t smem = quad::Smem<T>::BYTES;
@@ -2399,7 +2471,7 @@ void launch_step(fdtd_ctx *c, const StepArgs<T> &A) {
     // media: the step (its E update without them), then their pass over the members
     if (c->lossless) go(quad_kernel<T, false>);
     else go(quad_kernel<T, true>);
-    if (c->media)
+    if (c->media && ade)
       ade_kernel<T><<<(unsigned)((A.media.members + 255) / 256), 256, 0, c->stream>>>(A);
     return;
   }
@@ -2564,8 +2636,10 @@ template <typename T>
 int run_impl(fdtd_ctx *c, long long steps, long long first) {
   if (!c->coeffs_set || !c->fields_set)
     return fail(c, FDTD_E_STATE, "upload the coefficients and the fields before a run");
-  if (c->naux_laid != c->naux)
+  if (c->naux_laid != c->naux + c->nbloch)
     return fail(c, FDTD_E_STATE, "set the sources again after the plane waves");
+  if (c->nbloch > 0)
+    return fail(c, FDTD_E_STATE, "a context with Bloch couplings steps with fdtd_bloch_run");
   const int K = c->ring_k > 0 ? c->ring_k : 64;
   // the probes' record: grow to the run's steps
   if (c->nprobes > 0 && c->recorded + steps > c->record_cap) {
@@ -2681,9 +2755,198 @@ int run_impl(fdtd_ctx *c, long long steps, long long first) {
   return 0;
 }
 
+// The probes' record grown to hold `steps` more steps.
+int grow_record(fdtd_ctx *c, long long steps) {
+  if (c->nprobes == 0 || c->recorded + steps <= c->record_cap) return 0;
+  long long cap = std::max<long long>(c->recorded + steps, 2 * c->record_cap);
+  double *nr = nullptr;
+  if (int r = alloc(c, (void **)&nr, (size_t)cap * c->nprobes * 8)) return r;
+  if (c->record && c->recorded)
+    CUDA_TRY(c, cudaMemcpyAsync(nr, c->record, (size_t)c->recorded * c->nprobes * 8,
+                                cudaMemcpyDeviceToDevice, c->stream));
+  release(c, c->record);
+  c->record = nr;
+  c->record_cap = cap;
+  return 0;
+}
+
+// A complex run (src/fdtd.rs:1319-1343, src/fdtd/bloch.rs): the real part `a` and the imaginary
+// part `b`, two contexts of one grid, stepped together on a's stream: each step, H's couplings
+// across the Bloch sides from both parts' E (subtracted in the step kernels after H's sources),
+// a's step and b's, E's couplings from both parts' new H, the media (b's, then a's), then each
+// part's probes and the transforms of a's monitors taken whole (real and imaginary parts).
+template <typename T>
+int bloch_impl(fdtd_ctx *a, fdtd_ctx *b, const std::vector<WrapDev> &hw,
+               const std::vector<WrapDev> &ew, const std::vector<int> &estart, long long steps,
+               long long first) {
+  for (fdtd_ctx *c : {a, b}) {
+    if (!c->coeffs_set || !c->fields_set)
+      return fail(a, FDTD_E_STATE, "upload both parts' coefficients and fields before a run");
+    if (c->naux_laid != c->naux + c->nbloch)
+      return fail(a, FDTD_E_STATE, "set the sources again after the Bloch slots");
+    if (c->media && !c->quad)
+      return fail(a, FDTD_E_INVALID,
+                  "Bloch sides with dispersive media step on grids whose nx is a multiple of 4");
+  }
+  if (a->N != b->N || a->precision != b->precision || a->nbloch != b->nbloch)
+    return fail(a, FDTD_E_INVALID, "the two parts of a complex run differ");
+  CUDA_TRY(a, cudaStreamSynchronize(b->stream));
+  const cudaStream_t st = a->stream;
+  const int K = a->ring_k > 0 ? a->ring_k : 64;
+  if (int r = grow_record(a, steps)) return r;
+  if (int r = grow_record(b, steps)) return fail(a, r, "%s", b->error.c_str());
+  // the couplings and the imaginary part's ring, for this run
+  WrapDev *dh = nullptr, *de = nullptr;
+  int *dstart = nullptr;
+  T *ring_im = nullptr;
+  auto freed = [&]() {
+    release(a, dh);
+    release(a, de);
+    release(a, dstart);
+    release(a, ring_im);
+  };
+  if (int r = alloc(a, (void **)&dh, std::max<size_t>(hw.size(), 1) * sizeof(WrapDev))) return r;
+  if (int r = alloc(a, (void **)&de, std::max<size_t>(ew.size(), 1) * sizeof(WrapDev))) {
+    freed();
+    return r;
+  }
+  if (int r = alloc(a, (void **)&dstart, estart.size() * 4)) {
+    freed();
+    return r;
+  }
+  if (a->nvalues > 0)
+    if (int r = alloc(a, (void **)&ring_im, (size_t)K * a->nvalues * a->elem)) {
+      freed();
+      return r;
+    }
+  cudaError_t e = cudaSuccess;
+  if (!hw.empty()) e = copy(a, dh, hw.data(), hw.size() * sizeof(WrapDev), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !ew.empty())
+    e = copy(a, de, ew.data(), ew.size() * sizeof(WrapDev), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = copy(a, dstart, estart.data(), estart.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    freed();
+    return fail(a, FDTD_E_GPU, "the Bloch couplings: %s", cudaGetErrorString(e));
+  }
+  const int nvals_e = (int)estart.size() - 1;
+  // b's step launches on a's stream for the run (its kernels and a's must be ordered)
+  const cudaStream_t b_stream = b->stream;
+  b->stream = st;
+  long long done = 0;
+  while (done < steps) {
+    const int batch = (int)std::min<long long>(K, steps - done);
+    for (fdtd_ctx *c : {a, b})
+      if (c->nwaves > 0) {
+        const int total = c->nwaves * batch;
+        waves_kernel<<<(total + 127) / 128, 128, 0, st>>>(c->d_waves, c->d_point, c->nwaves,
+                                                          c->stride(), first + done, nullptr,
+                                                          batch, c->dt, c->waves_h, c->waves_e);
+      }
+    for (int m = 0; m < batch; m++) {
+      const long long row_a = 2LL * m * a->stride(), row_b = 2LL * m * b->stride();
+      if (!hw.empty())
+        bloch_h_kernel<T><<<(unsigned)((hw.size() + 127) / 128), 128, 0, st>>>(
+            dh, (int)hw.size(), (const T *)a->e[a->parity], (const T *)b->e[b->parity], a->N,
+            a->dt, a->waves_h + row_a + 2LL * (a->nwaves + a->naux),
+            b->waves_h + row_b + 2LL * (b->nwaves + b->naux));
+      StepArgs<T> A = step_args<T>(a), B = step_args<T>(b);
+      A.waves_h = a->waves_h + row_a;
+      A.waves_e = a->waves_e + row_a;
+      B.waves_h = b->waves_h + row_b;
+      B.waves_e = b->waves_e + row_b;
+      launch_step<T>(a, A, false);
+      launch_step<T>(b, B, false);
+      a->parity = 1 - a->parity;
+      b->parity = 1 - b->parity;
+      if (nvals_e > 0)
+        bloch_e_kernel<T><<<(unsigned)((nvals_e + 127) / 128), 128, 0, st>>>(
+            de, dstart, nvals_e, (const T *)a->h[a->parity], (const T *)b->h[b->parity], a->N,
+            (T *)a->e[a->parity], (T *)b->e[b->parity]);
+      if (b->media && b->quad)
+        ade_kernel<T><<<(unsigned)((B.media.members + 255) / 256), 256, 0, st>>>(B);
+      if (a->media && a->quad)
+        ade_kernel<T><<<(unsigned)((A.media.members + 255) / 256), 256, 0, st>>>(A);
+      // b's probes, and a's monitored values of b into the imaginary ring; then a's own
+      const long long count = a->nvalues;
+      if (count + b->nprobes > 0)
+        gather_kernel<T><<<(unsigned)((count + b->nprobes + 255) / 256), 256, 0, st>>>(
+            (const T *)b->e[b->parity], (const T *)b->h[b->parity], a->d_where, (int)count,
+            count ? ring_im + (long long)m * count : nullptr, b->d_probes, b->nprobes,
+            b->nprobes ? b->record + (b->recorded + done + m) * b->nprobes : nullptr);
+      if (count + a->nprobes > 0)
+        gather_kernel<T><<<(unsigned)((count + a->nprobes + 255) / 256), 256, 0, st>>>(
+            (const T *)a->e[a->parity], (const T *)a->h[a->parity], a->d_where, (int)count,
+            count ? (T *)a->ring + (long long)m * count : nullptr, a->d_probes, a->nprobes,
+            a->nprobes ? a->record + (a->recorded + done + m) * a->nprobes : nullptr);
+    }
+    if (a->nvalues > 0) {
+      const int total = a->nslots * batch;
+      phase_kernel<<<(total + 127) / 128, 128, 0, st>>>(a->d_omega, a->d_slot_field, a->nslots,
+                                                        first + done, nullptr, batch, a->dt,
+                                                        a->phase);
+      dft_complex_kernel<T><<<(unsigned)((a->nvalues + 127) / 128), 128, 0, st>>>(
+          a->d_series, a->d_value_series, a->nvalues, (const T *)a->ring, ring_im, batch,
+          a->phase, a->nslots, a->sums);
+    }
+    done += batch;
+  }
+  b->stream = b_stream;
+  e = cudaStreamSynchronize(st);
+  freed();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(a, FDTD_E_GPU, "a complex run: %s", cudaGetErrorString(e));
+  a->recorded += steps;
+  b->recorded += steps;
+  a->generation++;
+  b->generation++;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+int fdtd_set_bloch_slots(fdtd_ctx *c, int32_t nslots) {
+  if (!c || nslots < 0) return FDTD_E_INVALID;
+  c->generation++;
+  c->layout++;
+  c->nbloch = nslots;
+  return 0;
+}
+
+int fdtd_bloch_run(fdtd_ctx *re, fdtd_ctx *im, int32_t nwraps, const fdtd_wrap *wraps,
+                   int64_t steps, int64_t first_step) {
+  if (!re || !im || re == im || nwraps < 0 || (nwraps > 0 && !wraps)) return FDTD_E_INVALID;
+  if (steps < 0) return fail(re, FDTD_E_INVALID, "a negative number of steps");
+  if (steps == 0) return 0;
+  // H's couplings each in their own slot; E's grouped by value, each value's in the given order
+  std::vector<WrapDev> hw, ew;
+  std::map<std::pair<int, long long>, std::vector<WrapDev>> byvalue;
+  std::vector<std::pair<int, long long>> order;
+  for (int32_t k = 0; k < nwraps; k++) {
+    const fdtd_wrap &x = wraps[k];
+    if (x.comp < 0 || x.comp > 2 || x.from_comp < 0 || x.from_comp > 2 || x.r < 0 ||
+        x.r >= re->N || x.q < 0 || x.q >= re->N || (x.field == 1 && (x.slot < 0 ||
+        x.slot >= re->nbloch)))
+      return fail(re, FDTD_E_INVALID, "Bloch coupling %d is outside the grid", (int)k);
+    WrapDev d{x.r, x.q, x.comp, x.from_comp, x.phase_re, x.phase_im, x.s, x.cb, x.slot, 0};
+    if (x.field == 1) {
+      hw.push_back(d);
+    } else {
+      auto key = std::make_pair((int)x.comp, (long long)x.r);
+      if (!byvalue.count(key)) order.push_back(key);
+      byvalue[key].push_back(d);
+    }
+  }
+  std::vector<int> start{0};
+  for (auto &key : order) {
+    for (auto &d : byvalue[key]) ew.push_back(d);
+    start.push_back((int)ew.size());
+  }
+  re->launches = 0;
+  return re->precision == 64 ? bloch_impl<double>(re, im, hw, ew, start, steps, first_step)
+                             : bloch_impl<float>(re, im, hw, ew, start, steps, first_step);
+}
 
 const char *fdtd_last_error(const fdtd_ctx *ctx) { return ctx ? ctx->error.c_str() : "no context"; }
 
@@ -2952,7 +3215,7 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   std::vector<int> point(std::max(nwaves, 1), -1);
   for (int64_t q = 0; q < ninj; q++) {
     const fdtd_injection &x = inj[q];
-    const int slots = x.point == 2 ? c->naux : nwaves;  // a coupling reads a plane wave's slot
+    const int slots = x.point == 2 ? c->naux + c->nbloch : nwaves;  // a coupling's slot
     if (x.field < 0 || x.field > 1 || x.component < 0 || x.component > 2 || x.r < 0 ||
         x.r >= c->N || x.emitter < 0 || x.emitter >= slots || !std::isfinite(x.a_re) ||
         !std::isfinite(x.a_im) || x.point < 0 || x.point > 2)
@@ -3079,7 +3342,7 @@ int fdtd_set_sources(fdtd_ctx *c, int32_t nwaves, const fdtd_waveform *waves, in
   if (!ordered_entries.empty())
     CUDA_TRY(c, copy(c, c->entries, ordered_entries.data(), ordered_entries.size() * sizeof(Entry), cudaMemcpyHostToDevice));
   c->nwaves = nwaves;
-  c->naux_laid = c->naux;
+  c->naux_laid = c->naux + c->nbloch;
   if (c->stride() > 0) {
     const int K = c->ring_k > 0 ? c->ring_k : 64;
     if (int r = alloc(c, (void **)&c->waves_h, (size_t)K * c->stride() * 16)) return r;

@@ -288,12 +288,67 @@ struct pxs_sim {
   std::unordered_map<int64_t, int> members;  // a dispersive value (comp * N + r): its group
   std::vector<PlaneRun> plane_waves;
   int aux_on_device = 0;  // the plane waves whose latest state is the engine's
+  // Bloch sides (src/fdtd/bloch.rs): the wavenumbers, e^(ikL) along each axis, and with one not
+  // zero the fields' imaginary part, a second simulation stepped alongside
+  double bloch_k[3] = {0.0, 0.0, 0.0};
+  bool along[3] = {false, false, false};
+  double phase_re[3] = {1.0, 1.0, 1.0}, phase_im[3] = {0.0, 0.0, 0.0};
+  pxs_sim *twin = nullptr;
   bool configured = false;  // sources, probes and transforms pushed to the engine
   bool fields_dropped = false;  // released without reading the fields back (a served job's)
   fdtd_ctx *ctx = nullptr;
 
   int64_t N() const { return g.cells(); }
   bool periodic(int a) const { return kind[a] == 1; }
+  // Bloch::image (src/fdtd/bloch.rs:85-95): e^(-ikL turns) along `axis`, num-complex's powi of
+  // the phase (squaring; a negative power the inverse, (re, 0 - im) / |z|^2)
+  void image(int axis, int64_t turns, double *re, double *im) const {
+    *re = 1.0;
+    *im = 0.0;
+    if (turns == 0 || !along[axis]) return;
+    auto mul = [](double ar, double ai, double br, double bi, double *cr, double *ci) {
+      *cr = ar * br - ai * bi;
+      *ci = ar * bi + ai * br;
+    };
+    const int64_t n = -turns;
+    uint64_t e = (uint64_t)(n >= 0 ? n : -n);
+    double br = phase_re[axis], bi = phase_im[axis];
+    while ((e & 1) == 0) {
+      mul(br, bi, br, bi, &br, &bi);
+      e >>= 1;
+    }
+    double ar = br, ai = bi;
+    while (e > 1) {
+      e >>= 1;
+      mul(br, bi, br, bi, &br, &bi);
+      if (e & 1) mul(ar, ai, br, bi, &ar, &ai);
+    }
+    if (n >= 0) {
+      *re = ar;
+      *im = ai;
+    } else {
+      const double ns = ar * ar + ai * ai;
+      *re = ar / ns;
+      *im = 0.0 - ai / ns;
+    }
+  }
+
+  // bloch::curl_bound (src/fdtd/bloch.rs:31-43): sum of w/d^2 over the axes
+  double curl_bound() const {
+    double sum = 0.0;
+    for (int a = 0; a < 3; a++) {
+      const double h = g.d[a], hh = h * h;
+      if (g.n[a] == 1 && periodic(a)) {
+        if (bloch_k[a] == 0.0) continue;
+        double sn, cs;
+        pxp::sincos(bloch_k[a] * h / 2.0, &sn, &cs);
+        sum += (sn * sn) * (1.0 / hh);
+        continue;
+      }
+      sum += 1.0 / hh;
+    }
+    return sum;
+  }
   int fail(int code, const char *fmt, ...) {
     char buf[1024];
     va_list ap;
@@ -443,6 +498,53 @@ struct pxs_sim {
     return 0;
   }
 
+  // The couplings across the Bloch sides (Bloch::wrap, src/fdtd/bloch.rs:97-152): H's on the
+  // last plane along each Bloch axis (reading E at the first, e^(ikL) - 1), then E's on the
+  // first (reading H at the last, e^(-ikL) - 1), by axis, component and value.
+  void bloch_wraps(std::vector<fdtd_wrap> &out) const {
+    for (int field : {1, 0}) {
+      const bool forward = field == 1;
+      int32_t slot = 0;
+      for (int w = 0; w < 3; w++) {
+        if (!along[w]) continue;
+        const int64_t n = g.n[w];
+        const int64_t m = forward ? n - 1 : 0;
+        const int64_t stride = w == 0 ? 1 : (w == 1 ? g.n[0] : g.n[0] * g.n[1]);
+        const int64_t o = forward ? -(n - 1) * stride : (n - 1) * stride;
+        const double pr = phase_re[w] - 1.0, pi = forward ? phase_im[w] : -phase_im[w];
+        const double kappa = forward ? kh[w][m] : kn[w][m];
+        const double factor = kappa / g.d[w];
+        int64_t lo[3] = {0, 0, 0}, hi[3] = {g.n[0], g.n[1], g.n[2]};
+        lo[w] = m;
+        hi[w] = m + 1;
+        for (int c = 0; c < 3; c++) {
+          if (c == w) continue;
+          const int a = first_of(c), b = second_of(c);
+          double sign = w == a ? 1.0 : -1.0;
+          const int d = w == a ? b : a;
+          if (!forward) sign = -sign;
+          for (int64_t k = lo[2]; k < hi[2]; k++)
+            for (int64_t j = lo[1]; j < hi[1]; j++)
+              for (int64_t i = lo[0]; i < hi[0]; i++) {
+                const int64_t r = (k * g.n[1] + j) * g.n[0] + i;
+                fdtd_wrap x;
+                x.field = field;
+                x.comp = c;
+                x.from_comp = d;
+                x.slot = forward ? slot++ : 0;
+                x.r = r;
+                x.q = r + o;
+                x.phase_re = pr;
+                x.phase_im = pi;
+                x.s = sign * factor;
+                x.cb = forward ? 0.0 : cb[c][r];
+                out.push_back(x);
+              }
+        }
+      }
+    }
+  }
+
   // The plane waves' states from the engine into the host's copies.
   int pull_plane_waves() {
     for (int n = 0; n < aux_on_device && ctx; n++) {
@@ -510,6 +612,17 @@ struct pxs_sim {
     if (int r = fdtd_set_plane_waves(ctx, (int32_t)pw.size(), pw.data()))
       return fail(r, "%s", fdtd_last_error(ctx));
     aux_on_device = (int)plane_waves.size();
+    // a complex run's H couplings across the Bloch sides, each in a slot of its own after the
+    // plane waves', subtracted last (Bloch::wrap after step_h, src/fdtd.rs:1330-1333)
+    std::vector<fdtd_wrap> wraps;
+    bloch_wraps(wraps);
+    int32_t nh = 0;
+    for (const fdtd_wrap &w : wraps)
+      if (w.field == 1) {
+        inj.push_back(fdtd_injection{1, w.comp, w.r, 1.0, 0.0, slot0 + w.slot, 2});
+        nh++;
+      }
+    if (int r = fdtd_set_bloch_slots(ctx, nh)) return fail(r, "%s", fdtd_last_error(ctx));
     if (int r = fdtd_set_sources(ctx, (int32_t)waves.size(), waves.data(), (int64_t)inj.size(),
                                  inj.data()))
       return fail(r, "%s", fdtd_last_error(ctx));
@@ -575,6 +688,16 @@ struct pxs_sim {
     if (count <= 0) return 0;
     if (fields_dropped) return dropped();
     if (int r = prepare()) return r;
+    if (twin) {  // a complex run: both parts together, coupled across the Bloch sides
+      if (int r = twin->prepare()) return fail(r, "%s", twin->error.c_str());
+      std::vector<fdtd_wrap> wraps;
+      bloch_wraps(wraps);
+      if (int r = fdtd_bloch_run(ctx, twin->ctx, (int32_t)wraps.size(), wraps.data(), count,
+                                 steps))
+        return fail(r, "%s", fdtd_last_error(ctx));
+      if (int r = twin->finish(count)) return fail(r, "%s", twin->error.c_str());
+      return finish(count);
+    }
     if (int r = fdtd_run(ctx, count, steps)) return fail(r, "%s", fdtd_last_error(ctx));
     return finish(count);
   }
@@ -583,6 +706,8 @@ struct pxs_sim {
   // read after each run), then the engine and its device memory released. A later run makes a
   // new engine from the host's copies.
   int release(bool keep_fields = true) {
+    if (twin)
+      if (int r = twin->release(keep_fields)) return fail(r, "%s", twin->error.c_str());
     if (!ctx) return 0;
     if (keep_fields) {
       if (int r = pull()) return r;
@@ -922,6 +1047,16 @@ pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], co
                     const int64_t low[3], const int64_t high[3], const double cpml[5],
                     double courant, const double *eps, const pxs_geometry *geometry,
                     int32_t precision, size_t hbm_budget, char *err, int32_t errlen) {
+  const double none[3] = {0.0, 0.0, 0.0};
+  return pxs_create_bloch(n, d, o, kind, low, high, cpml, none, courant, eps, geometry, precision,
+                          hbm_budget, err, errlen);
+}
+
+pxs_sim *pxs_create_bloch(const int64_t n[3], const double d[3], const double o[3],
+                          const int32_t kind[3], const int64_t low[3], const int64_t high[3],
+                          const double cpml[5], const double bloch[3], double courant,
+                          const double *eps, const pxs_geometry *geometry, int32_t precision,
+                          size_t hbm_budget, char *err, int32_t errlen) {
   std::string msg;
   auto refuse = [&](const char *fmt, auto... args) -> pxs_sim * {
     set_error(&msg, FDTD_E_INVALID, fmt, args...);
@@ -942,6 +1077,9 @@ pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], co
                     (long long)high[a], (long long)n[a]);
   if (!(courant > 0.0 && courant <= 1.0))
     return refuse("the Courant number must be in (0, 1], got %g", courant);
+  for (int a = 0; a < 3; a++)
+    if (!std::isfinite(bloch[a]) || (bloch[a] != 0.0 && kind[a] != 1))
+      return refuse("the Bloch wavenumber along axis %d must be finite, on a periodic axis", a);
   pxs_sim *s = new pxs_sim();
   s->g = Grid{{n[0], n[1], n[2]}, {d[0], d[1], d[2]}, {o[0], o[1], o[2]}};
   for (int a = 0; a < 3; a++) {
@@ -953,11 +1091,10 @@ pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], co
   for (int q = 0; q < 5; q++) s->cpml[q] = cpml[q];
   s->precision = precision == 64 ? 64 : 32;
   s->budget = hbm_budget;
-  // Delta t = C / sqrt(sum 1/d^2) over the axes the field varies along (bloch::curl_bound,
-  // src/fdtd/bloch.rs:31-43, with k = 0)
-  double sum = 0.0;
-  for (int a = 0; a < 3; a++)
-    if (s->varies[a]) sum += 1.0 / (d[a] * d[a]);
+  // Delta t = C / sqrt(sum w/d^2) (bloch::curl_bound, src/fdtd/bloch.rs:31-43): w = 1 along an
+  // axis the field varies along, sin^2(k d / 2) along one a cell long with a Bloch phase
+  for (int a = 0; a < 3; a++) s->bloch_k[a] = bloch[a];
+  const double sum = s->curl_bound();
   if (sum == 0.0) {
     delete s;
     return refuse("the field varies along no axis");
@@ -992,11 +1129,22 @@ pxs_sim *pxs_create(const int64_t n[3], const double d[3], const double o[3], co
     }
   s->build_cpml();
   s->psi.resize(s->slabs.size());
+  if (bloch[0] != 0.0 || bloch[1] != 0.0 || bloch[2] != 0.0) {
+    for (int a = 0; a < 3; a++) {
+      s->along[a] = bloch[a] != 0.0;
+      double sn, cs;  // from_polar(1, k L)
+      pxp::sincos(bloch[a] * ((double)n[a] * d[a]), &sn, &cs);
+      s->phase_re[a] = 1.0 * cs;
+      s->phase_im[a] = 1.0 * sn;
+    }
+    s->twin = new pxs_sim(*s);
+  }
   return s;
 }
 
 void pxs_destroy(pxs_sim *s) {
   if (!s) return;
+  pxs_destroy(s->twin);
   fdtd_destroy(s->ctx);
   delete s;
 }
@@ -1004,6 +1152,9 @@ void pxs_destroy(pxs_sim *s) {
 const char *pxs_last_error(const pxs_sim *s) { return s ? s->error.c_str() : "no simulation"; }
 
 int pxs_conductivity(pxs_sim *s, const double *sigma, const pxs_geometry *geometry) {
+  if (s && s->twin)  // a complex run's imaginary part takes it too (src/fdtd.rs:962-964)
+    if (int r = pxs_conductivity(s->twin, sigma, geometry))
+      return s->fail(r, "%s", s->twin->error.c_str());
   if (!s->groups.empty())
     return s->fail(FDTD_E_INVALID,
                    "the conductivity comes before the dispersive media: with_conductivity, then "
@@ -1031,6 +1182,9 @@ int pxs_conductivity(pxs_sim *s, const double *sigma, const pxs_geometry *geomet
 }
 
 int pxs_conductor(pxs_sim *s, int32_t comp, int64_t i, int64_t j, int64_t k) {
+  if (s && s->twin)  // src/fdtd.rs:1005-1007
+    if (int r = pxs_conductor(s->twin, comp, i, j, k))
+      return s->fail(r, "%s", s->twin->error.c_str());
   if (comp < 0 || comp > 2 || !s->inside(i, j, k))
     return s->fail(FDTD_E_INVALID, "(%lld, %lld, %lld) is outside the grid", (long long)i,
                    (long long)j, (long long)k);
@@ -1059,6 +1213,9 @@ int pxs_conductor(pxs_sim *s, int32_t comp, int64_t i, int64_t j, int64_t k) {
 
 int pxs_medium(pxs_sim *s, double eps_inf, int32_t npoles, const double *poles,
                const uint8_t *inside, const pxs_geometry *geometry) {
+  if (s && s->twin)  // src/fdtd/media.rs:756-759
+    if (int r = pxs_medium(s->twin, eps_inf, npoles, poles, inside, geometry))
+      return s->fail(r, "%s", s->twin->error.c_str());
   // Simulation::medium (src/fdtd/media.rs:749-825), with its stability check
   if (!(std::isfinite(eps_inf) && eps_inf > 0.0))
     return s->fail(FDTD_E_INVALID, "a dispersive medium's eps_inf must be positive and finite");
@@ -1110,10 +1267,7 @@ int pxs_medium(pxs_sim *s, double eps_inf, int32_t npoles, const double *poles,
     return it != s->members.end() ? s->groups[it->second].chi : 0.0;
   };
   {
-    double top = 0.0, largest = 0.0;
-    for (int a = 0; a < 3; a++)
-      if (s->varies[a]) top += 1.0 / (s->g.d[a] * s->g.d[a]);
-    top *= 4.0;
+    double top = 4.0 * s->curl_bound(), largest = 0.0;
     for (int64_t q = 0; q < 3 * N; q++) {
       if (!in[q]) continue;
       const int c = (int)(q / N);
@@ -1193,6 +1347,15 @@ int pxs_add_source(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j
 
 int pxs_add_current(pxs_sim *s, int32_t field, int64_t count, const int32_t *comps,
                     const int64_t *at, const double *amps, const double wave[6]) {
+  if (s && s->twin && count > 0) {  // Im(a w) = Re(-i a w) on the imaginary part (sources.rs:190-207)
+    std::vector<double> im(2 * count);
+    for (int64_t q = 0; q < count; q++) {
+      im[2 * q] = 0.0 * amps[2 * q] - (-1.0) * amps[2 * q + 1];
+      im[2 * q + 1] = 0.0 * amps[2 * q + 1] + (-1.0) * amps[2 * q];
+    }
+    if (int r = pxs_add_current(s->twin, field, count, comps, at, im.data(), wave))
+      return s->fail(r, "%s", s->twin->error.c_str());
+  }
   for (int64_t q = 0; q < count; q++) {  // src/fdtd/sources.rs:223-242
     const int64_t *p = at + 3 * q;
     if (!s->inside(p[0], p[1], p[2]) || comps[q] < 0 || comps[q] > 2)
@@ -1315,6 +1478,9 @@ int pxs_add_plane_wave(pxs_sim *s, const int64_t low[3], const int64_t high[3],
                        const double wave[6]) {
   if (!s || !low || !high || !direction || !polarization || !wave) return FDTD_E_INVALID;
   if (s->fields_dropped) return s->dropped();
+  if (s->twin)  // Simulation::real_run (src/fdtd/sources.rs:209-221)
+    return s->fail(FDTD_E_INVALID, "a total-field/scattered-field source needs real fields: with "
+                                   "a Bloch phase, launch a current with it instead");
   auto gcd = [](int64_t a, int64_t b) {
     while (b != 0) {
       const int64_t t = a % b;
@@ -1629,6 +1795,9 @@ int pxs_add_beam(pxs_sim *s, int32_t axis, int64_t plane, int32_t direction,
   if (!s || !centre || !wave || axis < 0 || axis > 2 || tilt < 0 || tilt > 2)
     return FDTD_E_INVALID;
   if (s->fields_dropped) return s->dropped();
+  if (s->twin)  // Simulation::real_run (src/fdtd/sources.rs:209-221)
+    return s->fail(FDTD_E_INVALID, "a total-field/scattered-field source needs real fields: with "
+                                   "a Bloch phase, launch a current with it instead");
   const Grid &g = s->g;
   const int a = axis, b = first_of(axis), c = second_of(axis);
   auto ok = [](double v) { return std::isfinite(v) && v > 0.0; };
@@ -1885,6 +2054,38 @@ int pxs_add_dipole(pxs_sim *s, int32_t field, int32_t comp, const double pos[3],
     wt[axis][1] = f;
   }
   std::map<int64_t, std::pair<double, double>> values;
+  if (s->twin) {
+    // a complex run: a value beyond a periodic end is its image's, e^(-ikL turns) times it
+    // (Bloch::image, src/fdtd/bloch.rs:85-95); the weights complex, multiplied as num-complex
+    double cw[3][2][2];
+    for (int axis = 0; axis < 3; axis++)
+      for (int q = 0; q < 2; q++) {
+        double ir = 1.0, ii = 0.0;
+        if (s->varies[axis] && s->periodic(axis)) {
+          const bool half = field == 0 ? comp == axis : comp != axis;
+          const double first = s->g.node(axis, 0) + (half ? 0.5 * s->g.d[axis] : 0.0);
+          const int64_t n = s->g.n[axis];
+          const int64_t m = (int64_t)std::floor((pos[axis] - first) / s->g.d[axis]) + q;
+          const int64_t turns = m >= 0 ? m / n : -((-m + n - 1) / n);
+          s->image(axis, turns, &ir, &ii);
+        }
+        cw[axis][q][0] = ir * wt[axis][q];
+        cw[axis][q][1] = ii * wt[axis][q];
+      }
+    for (int p = 0; p < 2; p++)
+      for (int q = 0; q < 2; q++)
+        for (int r = 0; r < 2; r++) {
+          const double xr = cw[0][p][0] * cw[1][q][0] - cw[0][p][1] * cw[1][q][1];
+          const double xi = cw[0][p][0] * cw[1][q][1] + cw[0][p][1] * cw[1][q][0];
+          const double wr = xr * cw[2][r][0] - xi * cw[2][r][1];
+          const double wi = xr * cw[2][r][1] + xi * cw[2][r][0];
+          if (wr == 0.0 && wi == 0.0) continue;
+          const double sr = wr / volume, si = wi / volume;
+          auto &acc = values[s->index(idx[0][p], idx[1][q], idx[2][r])];
+          acc.first = acc.first + (are * sr - aim * si);
+          acc.second = acc.second + (are * si + aim * sr);
+        }
+  } else
   for (int p = 0; p < 2; p++)
     for (int q = 0; q < 2; q++)
       for (int r = 0; r < 2; r++) {
@@ -1895,6 +2096,22 @@ int pxs_add_dipole(pxs_sim *s, int32_t field, int32_t comp, const double pos[3],
         acc.first = acc.first + (are * sc - aim * 0.0);
         acc.second = acc.second + (are * 0.0 + aim * sc);
       }
+  if (s->twin) {  // the values' imaginary part, -i times them, on the imaginary part
+    std::vector<int32_t> comps;
+    std::vector<int64_t> at;
+    std::vector<double> im;
+    for (auto &kv : values) {
+      comps.push_back(comp);
+      at.push_back(kv.first % s->g.n[0]);
+      at.push_back((kv.first / s->g.n[0]) % s->g.n[1]);
+      at.push_back(kv.first / (s->g.n[0] * s->g.n[1]));
+      im.push_back(0.0 * kv.second.first - (-1.0) * kv.second.second);
+      im.push_back(0.0 * kv.second.second + (-1.0) * kv.second.first);
+    }
+    if (int r = pxs_add_current(s->twin, field, (int64_t)comps.size(), comps.data(), at.data(),
+                                im.data(), wave))
+      return s->fail(r, "%s", s->twin->error.c_str());
+  }
   if (int r = s->reconfigure()) return r;
   fdtd_waveform wv;
   wv.kind = (int32_t)wave[0];
@@ -1907,6 +2124,9 @@ int pxs_add_dipole(pxs_sim *s, int32_t field, int32_t comp, const double pos[3],
 }
 
 int pxs_add_probe(pxs_sim *s, int32_t field, int32_t comp, int64_t i, int64_t j, int64_t k) {
+  if (s && s->twin)  // src/fdtd.rs:1079-1081
+    if (int r = pxs_add_probe(s->twin, field, comp, i, j, k); r < 0)
+      return s->fail(r, "%s", s->twin->error.c_str());
   if (!s->inside(i, j, k) || comp < 0 || comp > 2)
     return s->fail(FDTD_E_INVALID, "(%lld, %lld, %lld) is outside the grid", (long long)i,
                    (long long)j, (long long)k);
@@ -2121,6 +2341,25 @@ int pxs_set_field(pxs_sim *s, int32_t field, int32_t comp, const double *in) {
   return 0;
 }
 
+int pxs_is_complex(const pxs_sim *s) { return s && s->twin ? 1 : 0; }
+
+int pxs_get_field_imag(pxs_sim *s, int32_t field, int32_t comp, double *out) {
+  if (!s->twin) return s->fail(FDTD_E_INVALID, "the fields are real: no Bloch phase");
+  if (int r = pxs_get_field(s->twin, field, comp, out)) return s->fail(r, "%s", s->twin->error.c_str());
+  return 0;
+}
+
+int pxs_set_field_imag(pxs_sim *s, int32_t field, int32_t comp, const double *in) {
+  if (!s->twin) return s->fail(FDTD_E_INVALID, "the fields are real: no Bloch phase");
+  if (int r = pxs_set_field(s->twin, field, comp, in)) return s->fail(r, "%s", s->twin->error.c_str());
+  return 0;
+}
+
+int64_t pxs_probe_imag(pxs_sim *s, int32_t n, double *out) {
+  if (!s->twin) return s->fail(FDTD_E_INVALID, "the fields are real: no Bloch phase");
+  return pxs_probe(s->twin, n, out);
+}
+
 int64_t pxs_probe(pxs_sim *s, int32_t n, double *out) {
   if (n < 0 || n >= (int32_t)s->probes.size()) return s->fail(FDTD_E_INVALID, "no probe %d", n);
   const auto &v = s->probes[n].values;
@@ -2228,6 +2467,11 @@ int pxs_batch_create(int32_t count, pxs_sim *const *sims, pxs_batch **out) {
       b->error = "a batch's simulation is missing";
       return FDTD_E_INVALID;
     }
+    if (sims[i]->twin) {
+      b->error = "simulation " + std::to_string(i) + " is a complex run (a Bloch phase), which "
+                 "the batch does not step";
+      return FDTD_E_INVALID;
+    }
     if (int r = sims[i]->prepare()) {
       b->error = "simulation " + std::to_string(i) + ": " + sims[i]->error;
       return r;
@@ -2326,6 +2570,10 @@ int pxs_adjoint_create(pxs_sim *s, int64_t steps, int32_t segment, int64_t count
   *out = a;
   if (!s) {
     a->error = "no simulation";
+    return FDTD_E_INVALID;
+  }
+  if (s->twin) {
+    a->error = "the adjoint does not step a complex run (a Bloch phase)";
     return FDTD_E_INVALID;
   }
   a->sim = s;
@@ -2638,6 +2886,10 @@ const char *pxs_server_last_error(const pxs_server *sv) { return sv ? sv->error.
 
 int64_t pxs_server_submit(pxs_server *sv, pxs_sim *s, int64_t steps, int32_t keep_fields) {
   if (!sv || !s || steps <= 0) return FDTD_E_INVALID;
+  if (s->twin) {
+    sv->error = "a complex run (a Bloch phase) steps on its own, with pxs_run";
+    return FDTD_E_INVALID;
+  }
   if (s->fields_dropped) {
     sv->error = s->dropped() ? s->error : std::string();
     return FDTD_E_STATE;

@@ -90,6 +90,14 @@ def library():
         x.pxs_add_plane_wave.argtypes = [P, I64P, I64P, I64P, DP, D, DP]
         x.pxs_incident.argtypes = [P, I32, I32, I32, I64, I64, I64, DP]
         x.pxs_add_beam.argtypes = [P, I32, I64, I32, DP, D, D, I32, D, I32, D, DP]
+        x.pxs_create_bloch.restype = P
+        x.pxs_create_bloch.argtypes = [I64P, DP, DP, I32P, I64P, I64P, DP, DP, D, DP,
+                                       C.POINTER(Geometry), I32, C.c_size_t, C.c_char_p, I32]
+        x.pxs_is_complex.argtypes = [P]
+        x.pxs_get_field_imag.argtypes = [P, I32, I32, DP]
+        x.pxs_set_field_imag.argtypes = [P, I32, I32, DP]
+        x.pxs_probe_imag.argtypes = [P, I32, DP]
+        x.pxs_probe_imag.restype = I64
         x.pxs_engine.restype = P
         _lib = x
     return _lib
@@ -202,9 +210,10 @@ class Simulation:
             keep.append(e)
             eps_p = e.ctypes.data_as(DP)
         err = C.create_string_buffer(1024)
-        h = lib.pxs_create(keep[0][1], keep[1][1], keep[2][1], keep[3][1], keep[4][1],
-                           keep[5][1], keep[6][1], float(courant), eps_p, geo_p, int(precision),
-                           int(hbm_budget), err, 1024)
+        bloch = _d(boundaries.bloch() if hasattr(boundaries, "bloch") else [0.0, 0.0, 0.0])
+        h = lib.pxs_create_bloch(keep[0][1], keep[1][1], keep[2][1], keep[3][1], keep[4][1],
+                                 keep[5][1], keep[6][1], bloch[1], float(courant), eps_p, geo_p,
+                                 int(precision), int(hbm_budget), err, 1024)
         if not h:
             raise InvalidValue(err.value.decode())
         self._h = h
@@ -383,6 +392,39 @@ class Simulation:
     def set_field(self, field, component, values):
         a, p = _d(np.asarray(values).reshape(-1))
         self._check(library().pxs_set_field(self._h, int(field), int(component), p))
+
+    @property
+    def is_complex(self) -> bool:
+        """``Simulation::is_complex``: a Bloch phase on a side makes the fields complex."""
+        return bool(library().pxs_is_complex(self._h))
+
+    def _imag(self, field, component) -> np.ndarray:
+        out = np.empty(self.grid.cells())
+        self._check(library().pxs_get_field_imag(self._h, int(field), int(component),
+                                                 out.ctypes.data_as(DP)))
+        return out
+
+    def e_imaginary(self, component) -> np.ndarray:
+        """``Simulation::e_imaginary``: E's imaginary part in a complex run."""
+        return self._imag(0, component)
+
+    def h_imaginary(self, component) -> np.ndarray:
+        return self._imag(1, component)
+
+    def set_field_imaginary(self, field, component, values):
+        a, p = _d(np.asarray(values).reshape(-1))
+        self._check(library().pxs_set_field_imag(self._h, int(field), int(component), p))
+
+    def probe_complex(self, n: int) -> np.ndarray:
+        """``Simulation::probe_complex``: the probe's values with their imaginary part."""
+        re = self.probe(n)
+        if not self.is_complex:
+            return re + 0j
+        lib = library()
+        count = self._check(lib.pxs_probe_imag(self._h, int(n), None))
+        im = np.empty(count)
+        self._check(lib.pxs_probe_imag(self._h, int(n), im.ctypes.data_as(DP)))
+        return re + 1j * im
 
     def probe(self, n: int) -> np.ndarray:
         count = self._check(library().pxs_probe(self._h, int(n), None))
