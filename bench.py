@@ -609,7 +609,9 @@ def workload_serving(args):
     1e5-5e7, or PHOTONOXIDE_SERVING_CELLS="lo,hi"; PHOTONOXIDE_SERVING_JOBS of them, 60 by default;
     steps 2000-20000; 1-4 Si boxes in SiO2; 1-51 DFT wavelengths) served
     by the resident loop (150 GB budget, continuous admission) against the same jobs run one at a
-    time in arrival order: p50/p99 latency and aggregate Gcell-updates/s. The offered load exceeds
+    time in arrival order, the 2D ones on the 3D engine (``one_at_a_time``) and as batches of one
+    on the TE kernel the loop batches them on (``one_at_a_time_te_kernel``): p50/p99 latency and
+    aggregate Gcell-updates/s. The offered load exceeds
     the GPU's capacity (a backlog builds), as at full scale. A job's results are its transforms
     (read back when it ends; its fields are not kept, in both arms). Each job's host set-up
     (permittivity averaging, tables) is made before the stream starts, for both arms: the
@@ -634,6 +636,28 @@ def workload_serving(args):
         t = max(t, sp.arrival) + d
         lat1.append(t - sp.arrival)
     span1 = t - specs[0].arrival
+    # one at a time with each 2D job on the TE kernel the served loop batches them on (a batch
+    # of one, on the loop's tiles): the baseline that leaves the loop's own gain
+    from photonoxide_b200.batch import Batch
+    sims = [make_job(sp) for sp in specs]
+    durations = []
+    for sp, s in zip(specs, sims):
+        if sp.two_d:
+            def one():
+                Batch([s], tile=(124, 7) if s.grid.nx % 4 == 0 else (32, 16)).run(sp.steps)
+                s.transforms()
+        else:
+            def one():
+                s.run(sp.steps)
+                s.transforms()
+        _, d = _timed(one)
+        durations.append(d)
+    del sims
+    t, lat2 = 0.0, []
+    for sp, d in zip(specs, durations):
+        t = max(t, sp.arrival) + d
+        lat2.append(t - sp.arrival)
+    span2 = t - specs[0].arrival
     # served: submitted at their arrival times
     sims = [make_job(sp) for sp in specs]
     torch.cuda.synchronize()
@@ -658,6 +682,10 @@ def workload_serving(args):
                               "latency_s": {"p50": float(np.percentile(lat1, 50)),
                                             "p99": float(np.percentile(lat1, 99))}},
             "speedup": span1 / span,
+            "one_at_a_time_te_kernel": {"value": work / span2 / 1e9,
+                                        "latency_s": {"p50": float(np.percentile(lat2, 50)),
+                                                      "p99": float(np.percentile(lat2, 99))}},
+            "speedup_vs_te_kernel_one_at_a_time": span2 / span,
             "loop_seconds": {k: loop[k] for k in ("launch_s", "host_s", "wait_s")},
             "config": {"workload": f"Poisson stream, 20 jobs/s, 70% 2D / 30% 3D, cells "
                                    f"log-uniform {lo:g}-{hi:g}, steps 2000-20000, 150 GB budget; "
