@@ -387,6 +387,14 @@ __device__ inline void cp_async16(void *smem, const void *gmem, bool valid) {
                : "memory");
 }
 __device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// One value (4 or 8 bytes) copied from global to shared memory without waiting.
+template <typename T>
+__device__ inline void cp_async_value(T *smem, const T *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem),
+               "n"((int)sizeof(T))
+               : "memory");
+}
 // Brings `bytes` (a multiple of 16, from a 16-byte aligned address) of global memory into L2
 // ahead of use, without waiting and without registers.
 __device__ inline void prefetch_l2(const void *gmem, unsigned bytes) {
@@ -1155,7 +1163,11 @@ constexpr int ER = RW + 2;     // staged E rows: y0-1 .. y0+RW
 template <typename T>
 struct Smem {
   static constexpr int E_SLOT = 3 * ER * EW;             // E of one plane
-  static constexpr int HB_SLOT = 3 * WARPS * ROW + 3 * RW * ROW;  // H(k) rows, cb(k) rows
+  // H(k) rows, cb(k) rows, then each warp's x-slab psi of its row at plane k: [field][component
+  // y, z][16 places] (XP_OFF on), staged with the rows rather than read when the slab needs it
+  static constexpr int XP_OFF = 3 * WARPS * ROW + 3 * RW * ROW;
+  static constexpr int XP = 64;
+  static constexpr int HB_SLOT = XP_OFF + WARPS * XP;
   static constexpr int X = 2 * WARPS * ROW;              // H_x, H_z exchange
   // the x CPML's b and a at the row's places: [field][component y, z][b, a][ROW] (0 outside)
   static constexpr int XC = 2 * 2 * 2 * ROW;
@@ -1331,7 +1343,8 @@ __device__ __forceinline__ int xslab_places(const StepArgs<T> &A, int x0, int &p
 template <typename T, int FIELD>
 __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x0, int lane,
                                       int ownmin, bool write, T v[3][4], const T d1[4],
-                                      const T d2[4], const T cbv[3][4], const T *xc) {
+                                      const T d2[4], const T cbv[3][4], const T *xc,
+                                      const T *xp) {
   using quad::ROW;
   using quad::VEC;
   int p0 = 0, P = 0;
@@ -1355,7 +1368,7 @@ __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x
       const long long at = s.psi + ((long long)k * A.n[1] + my) * s.pw + (x0 - VEC + pos - s.pf);
       const T *t = xc + ((FIELD * 2 + (c - 1)) * 2) * ROW;
       const T b = t[pos], a = t[ROW + pos];
-      const T old = (FIELD == 1 ? A.psi_h_in : A.psi_e)[at];
+      const T old = xp[(FIELD * 2 + (c - 1)) * 16 + (lane - (c - 1) * P)];  // staged
       const T q = div_by_step(d, A.step[0], A.inv_step[0], A.inv_step64[0], A.fast_div[0]);
       const T nw = b * old + a * q;
       u = (c == 1 ? T(-1) : T(1)) * nw;
@@ -1504,10 +1517,9 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   // the row's x-slab places (the same for every warp): one side's, at most 16, are shared out
   // over the warp's lanes (xcoop), and cpml4 takes no x slab; otherwise each lane takes its own
   bool xco;
-  {
-    int p0, P;
-    xco = xslab_places(A, x0, p0, P) >= 0;
-  }
+  int xside, xp0 = 0, xP = 0;
+  xside = xslab_places(A, x0, xp0, xP);
+  xco = xside >= 0;
   if (xco) sxl = -1;
   const T fhy = my >= 0 ? A.fh[nx + my] : T(0), fey = my >= 0 ? A.fe[nx + my] : T(0);
   int sy = -1;
@@ -1543,6 +1555,9 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     for (int q = 0; q < VEC / CH; q++) cp_async16(dst + q * CH, src + q * CH, ok);
   };
   // E(ke) rows into E slot E (ke < 0: zeros); H(kh), cb(kh) rows into HB slot H (H null: none)
+  // a lane of the x slab's (xcoop): component y (lanes below P) or z, its place xp0 + xq
+  const bool xstage = xco && rowh && lane < 2 * xP;
+  const int xcomp = lane < xP ? 1 : 2, xq = lane < xP ? lane : lane - xP;
   auto issue = [&](T *E, int ke, T *H, int kh) {
     const long long pe = ke >= 0 ? (long long)ke * plane : -1;
 #pragma unroll
@@ -1559,6 +1574,18 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       const long long ph = kh >= 0 ? (long long)kh * plane : -1;
 #pragma unroll
       for (int c = 0; c < 3; c++) chunk(H + c * WARPS * ROW + hrow, A.h_in + c * N, off_h, ph);
+      // the row's x-slab psi at plane kh, one value a lane of the slab's (xcoop reads them)
+      if (xstage && kh >= 0) {
+        T *xp = H + S::XP_OFF + w * S::XP;
+#pragma unroll
+        for (int f = 0; f < 2; f++) {
+          const SlabEntry &sl = A.slab[f][xcomp][0][xside];
+          if (sl.count)
+            cp_async_value(xp + (f * 2 + (xcomp - 1)) * 16 + xq,
+                           (f == 1 ? A.psi_h_in : A.psi_e) + sl.psi +
+                               ((long long)kh * ny + my) * sl.pw + (x0 - VEC + xp0 + xq - sl.pf));
+        }
+      }
       if (w >= 1) {
         T *B = H + 3 * WARPS * ROW;
 #pragma unroll
@@ -1619,7 +1646,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
     if (xco && rowh) {
       const T nocb[3][4] = {};
-      xcoop<T, 1>(A, k, my, x0, lane, 0, write && w >= 1, hn, dxEz, dxEy, nocb, sXC);
+      xcoop<T, 1>(A, k, my, x0, lane, 0, write && w >= 1, hn, dxEz, dxEy, nocb, sXC,
+                  sh + S::XP_OFF + w * S::XP);
     }
     if (rowh && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
       const bool ow = write && w >= 1 && lane >= 1;
@@ -1715,17 +1743,6 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
                         row);
         }
       }
-      if (xco) {
-        int p0, P;
-        const int side = xslab_places(A, x0, p0, P);
-#pragma unroll
-        for (int c = 1; c < 3; c++) {  // y and z along x
-          const SlabEntry &sl = A.slab[f][c][0][side];
-          if (sl.count)
-            prefetch_l2(base + sl.psi + ((long long)kp * ny + my) * sl.pw,
-                        (unsigned)(sl.pw * (int)sizeof(T)));
-        }
-      }
     }
   };
   for (int k = kbeg; k < kend; k++) {
@@ -1808,7 +1825,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
                              {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
                              {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
-        xcoop<T, 0>(A, k, my, x0, lane, 1, true, en, dxHz, dxHy, cbs, sXC);
+        xcoop<T, 0>(A, k, my, x0, lane, 1, true, en, dxHz, dxHy, cbs, sXC,
+                    hb_cur + S::XP_OFF + w * S::XP);
       }
       if (any_own && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
         const T diff[3][3][4] = {
