@@ -143,8 +143,9 @@ __host__ __device__ __forceinline__ float div_by_step(float x, float h, float r,
     const float e = fmaf(-q0, h, sx);
     const float q = fmaf(e, r, q0) * (tiny ? 0x1p-64f : 1.0f);
     const float aq = fabsf(q);
-    if (aq >= 0x1p-126f && aq <= 3.40282347e38f) return q;  // a normal quotient
-    if (x == 0.0f) return x * r;
+    // a normal quotient, or zero: x r with x's sign (q0, the product of the unscaled zero)
+    const bool zero = x == 0.0f;
+    if (zero || (aq >= 0x1p-126f && aq <= 3.40282347e38f)) return zero ? q0 : q;
     // a subnormal quotient: the product with 1/h in double, rounded once to float, carries
     // 53 bits for the at most 23 the result keeps
     if (aq < 0x1p-126f) return (float)((double)x * rd);
@@ -156,8 +157,9 @@ __host__ __device__ __forceinline__ double div_by_step(double x, double h, doubl
 }
 
 // Four quotients x[j] / h at once, each div_by_step's: where all four take its common path (x
-// not tiny, a normal quotient) that path's three operations each and one test for the four;
-// otherwise div_by_step value by value. The same bits either way.
+// zero, or not tiny with a normal quotient) that path's three operations each and one test for
+// the four; otherwise div_by_step value by value. The same bits either way. (Zero differences
+// are the rule where the fields are still at rest, as in most of a CPML early in a run.)
 __host__ __device__ __forceinline__ void div4_by_step(const float x[4], float q[4], float h, float r,
                                                       double rd, int fast) {
   if (fast) {
@@ -166,9 +168,12 @@ __host__ __device__ __forceinline__ void div4_by_step(const float x[4], float q[
     for (int j = 0; j < 4; j++) {
       const float q0 = x[j] * r;
       const float e = fmaf(-q0, h, x[j]);
-      q[j] = fmaf(e, r, q0);
-      const float aq = fabsf(q[j]);
-      common = common && fabsf(x[j]) >= 0x1p-90f && aq >= 0x1p-126f && aq <= 3.40282347e38f;
+      const float qj = fmaf(e, r, q0);
+      const float aq = fabsf(qj);
+      const bool zero = x[j] == 0.0f;  // x r, its sign kept: q0
+      q[j] = zero ? q0 : qj;
+      common = common &&
+               (zero || (fabsf(x[j]) >= 0x1p-90f && aq >= 0x1p-126f && aq <= 3.40282347e38f));
     }
     if (common) return;
   }

@@ -404,6 +404,15 @@ template <int N>
 __device__ inline void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
+// A named barrier (id 1..15; 0 is __syncthreads') of `threads` threads, whole warps: arrive
+// without waiting (the shared-memory writes before it are seen by the threads that sync on it),
+// or wait for the count.
+__device__ inline void named_arrive(int id, int threads) {
+  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(threads) : "memory");
+}
+__device__ inline void named_sync(int id, int threads) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(threads) : "memory");
+}
 
 template <typename T>
 struct Stage {
@@ -1782,7 +1791,11 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       st4(sX + (size_t)w * ROW + VEC * lane, a);
       st4(sX + (size_t)(WARPS + w) * ROW + VEC * lane, b);
     }
-    __syncthreads();
+    // the exchange row w goes to warp w+1 alone: a named barrier a pair of warps (id w+1, 64
+    // threads; warp w arrives, warp w+1 waits) rather than the whole tile. The row is written
+    // again only after the next plane's barrier, which every warp passes after its E.
+    if (w + 1 < WARPS) named_arrive(w + 1, 64);
+    if (w >= 1) named_sync(w, 64);
     // E's plane k at the owned places: back differences, then the slabs
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
     T en[3][4];
