@@ -1177,7 +1177,8 @@ struct Smem {
   static constexpr int XP_OFF = 3 * WARPS * ROW + 3 * RW * ROW;
   static constexpr int XP = 64;
   static constexpr int HB_SLOT = XP_OFF + WARPS * XP;
-  static constexpr int X = 2 * WARPS * ROW;              // H_x, H_z exchange
+  // the new H's rows: H_x and H_z for the row after, H_z and H_y for the row's own x CPML
+  static constexpr int X = 3 * WARPS * ROW;
   // the x CPML's b and a at the row's places: [field][component y, z][b, a][ROW] (0 outside)
   static constexpr int XC = 2 * 2 * 2 * ROW;
   static constexpr size_t BYTES =
@@ -1343,33 +1344,25 @@ __device__ __forceinline__ int xslab_places(const StepArgs<T> &A, int x0, int &p
 }
 
 // The x CPML of one field over a warp's row, its values shared out over the lanes: the row holds
-// the slab's places p0 .. p0+P-1 (xslab_places), and lane L < 2P updates component 1 + L / P at
-// place p0 + L % P with the owning lane's x difference (shuffled in); the owner applies the
-// result (shuffled back). Each value's arithmetic and each component's order of slabs are
-// slab4x's (x before the others); only the lane that computes it differs, so that a tile whose
-// rows meet an x CPML pays for its few places once per warp, not once per place of each lane.
-// Lanes below `ownmin` own no values (E: the halo lane). Every lane of the warp calls it.
+// the slab's places p0 .. p0+P-1 (side, p0 and P from xslab_places), and lane L < 2P updates
+// component 1 + L / P at place p0 + L % P; the owner applies the result (shuffled back). The x
+// difference is taken from the staged rows the owner's came from, the same two values: for H
+// forward, r[pos+1] - r[pos], over E's rows (r1 E_z for H_y, r2 E_y for H_z, positions from
+// x0-4); for E backward, r[pos] - r[pos-1], over the new H's exchange rows (r1 H_z for E_y, r2
+// H_y for E_z). Each value's arithmetic and each component's order of slabs are slab4x's (x
+// before the others); only the lane that computes it differs, so that a tile whose rows meet an
+// x CPML pays for its few places once per warp, not once per place of each lane. Lanes below
+// `ownmin` own no values (E: the halo lane). Every lane of the warp calls it.
 template <typename T, int FIELD>
 __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x0, int lane,
-                                      int ownmin, bool write, T v[3][4], const T d1[4],
-                                      const T d2[4], const T cbv[3][4], const T *xc,
+                                      int side, int p0, int P, int ownmin, bool write, T v[3][4],
+                                      const T *r1, const T *r2, const T cbv[3][4], const T *xc,
                                       const T *xp) {
   using quad::ROW;
   using quad::VEC;
-  int p0 = 0, P = 0;
-  const int side = xslab_places(A, x0, p0, P);
   const int c = lane < P ? 1 : 2;
   const int pos = p0 + lane - (c - 1) * P;
   const bool work = lane < 2 * P && (pos >> 2) >= ownmin;
-  const int src = work ? (pos >> 2) : lane;
-  const int jj = pos & 3;
-  T d = T(0);
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const T t1 = __shfl_sync(0xffffffffu, d1[r], src);
-    const T t2 = __shfl_sync(0xffffffffu, d2[r], src);
-    if (jj == r) d = c == 1 ? t1 : t2;
-  }
   T u = T(0);
   if (work) {
     const SlabEntry &s = A.slab[FIELD][c][0][side];
@@ -1378,6 +1371,8 @@ __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x
       const T *t = xc + ((FIELD * 2 + (c - 1)) * 2) * ROW;
       const T b = t[pos], a = t[ROW + pos];
       const T old = xp[(FIELD * 2 + (c - 1)) * 16 + (lane - (c - 1) * P)];  // staged
+      const T *r = c == 1 ? r1 : r2;
+      const T d = FIELD == 1 ? r[pos + 1] - r[pos] : r[pos] - r[pos - 1];
       const T q = div_by_step(d, A.step[0], A.inv_step[0], A.inv_step64[0], A.fast_div[0]);
       const T nw = b * old + a * q;
       u = (c == 1 ? T(-1) : T(1)) * nw;
@@ -1450,7 +1445,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   extern __shared__ __align__(16) unsigned char quad_raw[];
   T *sEs = reinterpret_cast<T *>(quad_raw);          // [3 slots][3][ER][EW]
   T *sHB = sEs + 3 * (size_t)S::E_SLOT;              // [2 slots][H 3][WARPS][ROW] + [cb 3][RW][ROW]
-  T *sX = sHB + 2 * (size_t)S::HB_SLOT;              // [2][WARPS][ROW]
+  T *sX = sHB + 2 * (size_t)S::HB_SLOT;              // [3][WARPS][ROW]
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nx = A.n[0], ny = A.n[1], nz = A.n[2];
   const long long N = A.N;
@@ -1655,8 +1650,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
     if (xco && rowh) {
       const T nocb[3][4] = {};
-      xcoop<T, 1>(A, k, my, x0, lane, 0, write && w >= 1, hn, dxEz, dxEy, nocb, sXC,
-                  sh + S::XP_OFF + w * S::XP);
+      xcoop<T, 1>(A, k, my, x0, lane, xside, xp0, xP, 0, write && w >= 1, hn, Erow(se, 2, w),
+                  Erow(se, 1, w), nocb, sXC, sh + S::XP_OFF + w * S::XP);
     }
     if (rowh && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
       const bool ow = write && w >= 1 && lane >= 1;
@@ -1790,10 +1785,16 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       }
       st4(sX + (size_t)w * ROW + VEC * lane, a);
       st4(sX + (size_t)(WARPS + w) * ROW + VEC * lane, b);
+      if (xco) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) a.v[j] = hn[1][j];
+        st4(sX + (size_t)(2 * WARPS + w) * ROW + VEC * lane, a);
+      }
     }
     // the exchange row w goes to warp w+1 alone: a named barrier a pair of warps (id w+1, 64
-    // threads; warp w arrives, warp w+1 waits) rather than the whole tile. The row is written
-    // again only after the next plane's barrier, which every warp passes after its E.
+    // threads; warp w arrives, warp w+1 waits) rather than the whole tile; warp w's own rows (its
+    // x CPML's) are its own writes, ordered for it by its sync. The rows are written again only
+    // after the next plane's barrier, which every warp passes after its E.
     if (w + 1 < WARPS) named_arrive(w + 1, 64);
     if (w >= 1) named_sync(w, 64);
     // E's plane k at the owned places: back differences, then the slabs
@@ -1838,7 +1839,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
                              {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
                              {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
-        xcoop<T, 0>(A, k, my, x0, lane, 1, true, en, dxHz, dxHy, cbs, sXC,
+        xcoop<T, 0>(A, k, my, x0, lane, xside, xp0, xP, 1, true, en,
+                    sX + (size_t)(WARPS + w) * ROW, sX + (size_t)(2 * WARPS + w) * ROW, cbs, sXC,
                     hb_cur + S::XP_OFF + w * S::XP);
       }
       if (any_own && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
