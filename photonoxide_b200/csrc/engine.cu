@@ -1181,8 +1181,10 @@ struct Smem {
   static constexpr int X = 3 * WARPS * ROW;
   // the x CPML's b and a at the row's places: [field][component y, z][b, a][ROW] (0 outside)
   static constexpr int XC = 2 * 2 * 2 * ROW;
+  // kappa/h along x at the row's places: [fh, fe][ROW]
+  static constexpr int FX = 2 * ROW;
   static constexpr size_t BYTES =
-      sizeof(T) * (3 * (size_t)E_SLOT + 2 * (size_t)HB_SLOT + X + XC);
+      sizeof(T) * (3 * (size_t)E_SLOT + 2 * (size_t)HB_SLOT + X + XC + FX);
 };
 }  // namespace quad
 
@@ -1472,6 +1474,11 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     }
     sXC[q] = val;
   }
+  T *sFX = sXC + S::XC;  // quad::Smem::FX
+  for (int q = threadIdx.x; q < S::FX; q += THREADS) {
+    const int mx = wrap_index(x0 - VEC + q % ROW, nx, A.periodic[0]);
+    sFX[q] = mx >= 0 ? (q < ROW ? A.fh : A.fe)[mx] : T(0);
+  }
 
   // -- this lane's four places along x, this warp's row
   const int xb = x0 - VEC + VEC * lane;  // the first of the four
@@ -1488,7 +1495,6 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const int myp = wrap_index(gy + 1, ny, A.periodic[1]);
   const bool rowh = my >= 0 && gy < ny;
   bool hv[4], ownv[4];
-  T fhx[4], fex[4];
   int sxs[4];  // the x CPML side of each place (-1 none)
 #pragma unroll
   for (int j = 0; j < 4; j++) {
@@ -1496,8 +1502,6 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     int mxj = wrap_index(x, nx, A.periodic[0]);
     hv[j] = rowh && mxj >= 0 && x < nx;
     ownv[j] = hv[j] && w >= 1 && lane >= 1;
-    fhx[j] = mxj >= 0 ? A.fh[mxj] : T(0);
-    fex[j] = mxj >= 0 ? A.fe[mxj] : T(0);
     sxs[j] = -1;
     if (mxj >= 0 && !A.periodic[0]) {
       if (mxj < A.low[0]) sxs[j] = 0;
@@ -1531,7 +1535,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     if (my < A.low[1]) sy = 0;
     else if (my >= ny - A.high[1]) sy = 1;
   }
-  const long long rowoff = my >= 0 ? (long long)my * nx : 0;
+  const int rowoff = my >= 0 ? my * nx : 0;  // in-plane offsets fit an int (quad_ok)
   // whether the tile has currents in any plane (most have none: then no plane looks them up)
   const bool hcur = A.hbucket[(long long)tile * nz] != A.hbucket[(long long)tile * nz + nz];
   const bool ecur = A.ebucket[(long long)tile * nz] != A.ebucket[(long long)tile * nz + nz];
@@ -1543,16 +1547,16 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   // Each chunk's offset within a plane is fixed for the run: -1 where it lies beyond a wall.
   const int myp_last = wrap_index(y0 + RW, ny, A.periodic[1]);
   const bool last_warp = w == WARPS - 1;
-  const long long off_e0 = (my >= 0 && mxb >= 0) ? (long long)my * nx + mxb : -1;
-  const long long off_ea0 = (my >= 0 && mxa >= 0) ? (long long)my * nx + mxa : -1;
-  const long long off_e1 = (myp_last >= 0 && mxb >= 0) ? (long long)myp_last * nx + mxb : -1;
-  const long long off_ea1 = (myp_last >= 0 && mxa >= 0) ? (long long)myp_last * nx + mxa : -1;
-  const long long off_h = off_e0;
-  const long long off_b = (w >= 1 && gy < ny) ? off_e0 : -1;
+  const int off_e0 = (my >= 0 && mxb >= 0) ? my * nx + mxb : -1;
+  const int off_ea0 = (my >= 0 && mxa >= 0) ? my * nx + mxa : -1;
+  const int off_e1 = (myp_last >= 0 && mxb >= 0) ? myp_last * nx + mxb : -1;
+  const int off_ea1 = (myp_last >= 0 && mxa >= 0) ? myp_last * nx + mxa : -1;
+  const int off_h = off_e0;
+  const int off_b = (w >= 1 && gy < ny) ? off_e0 : -1;
   // this thread's places in a staged E row, H row and cb row
   const int erow = w * EW + VEC * lane, hrow = w * ROW + VEC * lane;
   const int brow = (w >= 1 ? w - 1 : 0) * ROW + VEC * lane;
-  auto chunk = [&](T *dst, const T *field, long long off, long long pbase) {
+  auto chunk = [&](T *dst, const T *field, int off, long long pbase) {
     const bool ok = off >= 0 && pbase >= 0;
     const T *src = ok ? field + pbase + off : A.e_in;
 #pragma unroll
@@ -1622,6 +1626,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     eyp[1] = ld4(Erow(se, 2, w + 1) + VEC * lane);
     ez1[0] = ld4(Erow(se1, 0, w) + VEC * lane);     // E_x, E_y of the plane after
     ez1[1] = ld4(Erow(se1, 1, w) + VEC * lane);
+    const Vec4<T> fx = ld4(sFX + VEC * lane);  // kappa/h along x at the lane's places
     // +x of the fourth place: the next lane's first, lane 31 the chunk after the row
     T ey_n = __shfl_down_sync(0xffffffffu, e[1].v[0], 1);
     T ez_n = __shfl_down_sync(0xffffffffu, e[2].v[0], 1);
@@ -1642,9 +1647,10 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       dxEz[j] = ezn - e[2].v[j];
       dxEy[j] = eyn - e[1].v[j];
       dyEx[j] = exy - e[0].v[j];
+      const T fhx = fx.v[j];
       hn[0][j] = ho[0].v[j] - A.dt * (dyEz[j] * fhy - dzEy[j] * fhz);
-      hn[1][j] = ho[1].v[j] - A.dt * (dzEx[j] * fhz - dxEz[j] * fhx[j]);
-      hn[2][j] = ho[2].v[j] - A.dt * (dxEy[j] * fhx[j] - dyEx[j] * fhy);
+      hn[1][j] = ho[1].v[j] - A.dt * (dzEx[j] * fhz - dxEz[j] * fhx);
+      hn[2][j] = ho[2].v[j] - A.dt * (dxEy[j] * fhx - dyEx[j] * fhy);
     }
     // the CPML: H_x along y then z, H_y along x then z, H_z along x then y
     const bool zs = !A.periodic[2] && (k < A.low[2] || k >= nz - A.high[2]);
@@ -1809,6 +1815,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
       }
       hxm = ld4(sX + (size_t)(w - 1) * ROW + VEC * lane);  // the row before
       hzm = ld4(sX + (size_t)(WARPS + w - 1) * ROW + VEC * lane);
+      const Vec4<T> fex = ld4(sFX + ROW + VEC * lane);
       // -x of the first place: the previous lane's fourth
       T hz_p = __shfl_up_sync(0xffffffffu, hn[2][3], 1);
       T hy_p = __shfl_up_sync(0xffffffffu, hn[1][3], 1);
@@ -1825,8 +1832,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         dxHy[j] = hn[1][j] - hyx;
         dyHx[j] = hn[0][j] - hxm.v[j];
         T curl0 = dyHz[j] * fey - dzHy[j] * fez;
-        T curl1 = dzHx[j] * fez - dxHz[j] * fex[j];
-        T curl2 = dxHy[j] * fex[j] - dyHx[j] * fey;
+        T curl1 = dzHx[j] * fez - dxHz[j] * fex.v[j];
+        T curl2 = dxHy[j] * fex.v[j] - dyHx[j] * fey;
         T cav[3];
 #pragma unroll
         for (int c = 0; c < 3; c++) cav[c] = LOSSY ? ca[c].v[j] : (cb[c].v[j] == T(0) ? T(0) : T(1));
@@ -3102,9 +3109,11 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   {
     const char *force = getenv("PHOTONOXIDE_FDTD_KERNEL");
     // the quad kernel takes four places along x at once: nx a multiple of 4, and no group of
-    // four holding places of both x CPMLs (an interior narrower than the group)
+    // four holding places of both x CPMLs (an interior narrower than the group); its offsets
+    // within a plane are ints
     const bool quad_ok = c->n[0] % 4 == 0 &&
-        !(c->low[0] > 0 && c->high[0] > 0 && (c->low[0] - 1) / 4 == (c->n[0] - c->high[0]) / 4);
+        !(c->low[0] > 0 && c->high[0] > 0 && (c->low[0] - 1) / 4 == (c->n[0] - c->high[0]) / 4) &&
+        (long long)c->n[0] * c->n[1] < (1LL << 31);
     std::string kind = force ? force : (quad_ok ? "quad" : "row");
     if (kind == "quad" && !quad_ok) kind = "row";
     c->quad = kind == "quad";

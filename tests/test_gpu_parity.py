@@ -93,6 +93,37 @@ def test_closed_box_f32_bit_for_bit_over_300_steps():
         assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("precision", [32, 64])
+@pytest.mark.parametrize("periodic_x", [False, True])
+def test_lossless_conductors_bit_for_bit(precision, periodic_x):
+    """A lossless grid (ca 1, and 0 where cb is 0) with conductors inside tiles, on a tile's
+    first row and column and in its last row, walls, and random fields, so that E at a zero cb
+    starts non-zero: the engine keeps a table of the warps whose values hold a zero cb and takes
+    the plain E + cb curl elsewhere, the x wall's E_y and E_z at x = 0 in their own lane."""
+    from photonoxide_b200.types import Pml, Cpml
+    n = (132, 30, 12)
+
+    def make(cls):
+        g = Grid3d.centred(n, 0.05)
+        b = Boundaries(Periodic() if periodic_x else Pml(0, 0), Pml(4, 0), Pml(0, 0), Cpml())
+        eps = Boxes(1.0).add((-0.5, -0.3, -INF), (0.5, 0.3, INF), 6.0)
+        s = cls(g, eps, b, 0.9, precision=precision)
+        r = np.arange(g.cells())
+        for c in range(3):
+            s.set_field(Field.E, c, 0.01 * noise(r + 3 * c))
+            s.set_field(Field.H, c, 0.01 * noise(r + 7 * c + 50_000))
+        for comp, at in [(Axis.X, (5, 9, 4)), (Axis.Y, (124, 14, 6)), (Axis.Z, (60, 7, 8)),
+                         (Axis.Z, (131, 29, 11)), (Axis.Y, (0, 20, 3)), (Axis.X, (70, 13, 0))]:
+            s.conductor(comp, at)
+        return s
+
+    p, o = make(Simulation), make(OracleSimulation)
+    p.run(61)
+    o.run(61)
+    for c, (x, y) in enumerate(zip(fields(p), fields(o))):
+        assert np.array_equal(x, y), (c, relative(x, y))
+
+
 @pytest.mark.parametrize("precision", [64, 32])
 @pytest.mark.parametrize("two_d,n", [(False, None), (True, None), (False, (40, 21, 19)),
                                      (True, (72, 45, 1)), (False, (96, 37, 14)),
