@@ -2588,7 +2588,9 @@ int division_checked(fdtd_ctx *c, float h, float r, int *ok) {
 
 // The quad kernel's runs of z-planes: `count` runs (at most quad_max_runs) that never straddle the
 // edge of a z CPML, the CPMLs' planes (heavier) in runs of their own, the rest of about equal
-// length. Returns the number of runs; starts in c->runs.
+// length but for two short ones (a quarter of the others, from four interior runs on): taken
+// last (quad_order), they fill the step's end, where the SMs would otherwise wait on the longest
+// CTAs. Returns the number of runs; starts in c->runs.
 int quad_runs(fdtd_ctx *c, int count) {
   const int nz = c->n[2];
   const int lo = c->periodic[2] ? 0 : std::min(c->low[2], nz);
@@ -2616,16 +2618,24 @@ int quad_runs(fdtd_ctx *c, int count) {
     for (int q = 1; q <= parts; q++) c->runs[++n] = from + (int)((long long)planes * q / parts);
   };
   cut(0, lo, plo);
-  cut(lo, mid, inner);
+  const int longs = inner - 2;
+  const int shorts = inner >= 4 ? std::max(2, (int)std::lround(mid / (longs + 0.5) / 4.0)) : 0;
+  if (inner >= 4 && mid - 2 * shorts >= longs) {
+    cut(lo, mid - 2 * shorts, longs);
+    cut(lo + mid - 2 * shorts, 2 * shorts, 2);
+  } else {
+    cut(lo, mid, inner);
+  }
   cut(lo + mid, hi, phi);
   return n;
 }
 
 // The quad kernel's CTAs (run r, tile t as r * tiles + t) in launch order: by an estimate of
 // their time, heaviest first, so that the CTAs that start last are short and the step, which
-// ends with its last CTA, leaves few SMs idle at its end. A plane costs 1, 1.8 in a z CPML; a
-// tile whose rows reach an x CPML 1.4 times that, and up to 1.8 times with all its rows in a y
-// CPML; a run's first, recomputed plane of H 0.6 of a plane.
+// ends with its last CTA, leaves few SMs idle at its end. A plane of a tile costs 1, and more
+// where the tile meets a CPML: 0.4 where its rows reach an x CPML, 1.15 times the share of its
+// rows (of 8) in a y CPML, 0.95 in a z CPML's plane; a run's first, recomputed plane of H 0.6 of
+// a plane. (Fitted to the CTAs' times on the 3D MMI, 600 x 200 x 100 with CPMLs of 10.)
 std::vector<int> quad_order(const fdtd_ctx *c) {
   const int nx = c->n[0], ny = c->n[1], nz = c->n[2];
   const int tiles = c->tiles_x * c->tiles_y;
@@ -2642,12 +2652,12 @@ std::vector<int> quad_order(const fdtd_ctx *c) {
       for (int gy = y0 - 1; gy < y0 + quad::RW; gy++)
         if (!c->periodic[1] && gy >= 0 && gy < ny && (gy < c->low[1] || gy >= ny - c->high[1]))
           yrows++;
-      const double f = (1.0 + 0.4 * xe) * (1.0 + 0.8 * yrows / quad::WARPS);
+      const double base = 1.0 + 0.4 * xe + 1.15 * yrows / quad::WARPS;
       const int kbeg = c->runs[r], kend = c->runs[r + 1];
       double w = 0.0;
-      for (int k = kbeg; k < kend; k++) w += zslab(k) ? 1.8 : 1.0;
-      if (kbeg > 0) w += 0.6 * (zslab(kbeg - 1) ? 1.8 : 1.0);
-      cost.push_back({-w * f, r * tiles + t});
+      for (int k = kbeg; k < kend; k++) w += base + (zslab(k) ? 0.95 : 0.0);
+      if (kbeg > 0) w += 0.6 * (base + (zslab(kbeg - 1) ? 0.95 : 0.0));
+      cost.push_back({-w, r * tiles + t});
     }
   std::stable_sort(cost.begin(), cost.end(),
                    [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
@@ -3136,11 +3146,11 @@ int fdtd_create(const fdtd_grid *grid, double dt, const double step[3], const do
   c->tiles_x = (c->n[0] + c->tile_w - 1) / c->tile_w;
   c->tiles_y = (c->n[1] + c->tile_h - 1) / c->tile_h;
   long long tiles = (long long)c->tiles_x * c->tiles_y;
-  // z cut into runs so that the CTAs fill the device about six times over: runs that meet a
-  // CPML take longer than the rest, and shorter runs let the scheduler balance them, while each
-  // run recomputes one plane of H (a run is at least 4 planes long). On the 3D MMI 13 runs of 8
-  // planes timed best (4 % faster than 25 of 4, 9 % than 8 of 13).
-  long long want = 12LL * sms;
+  // z cut into runs so that the CTAs fill the device about three times over: fewer, longer runs
+  // recompute fewer planes of H, and the two short interior runs (quad_runs), taken last, keep
+  // the step's end short. On the 3D MMI (145 tiles) 7 runs timed best: 0.225 ms a step against
+  // 0.228 with 9 or 10, 0.231 with 8, 0.239 with 6 and 0.243 with 13.
+  long long want = 6LL * sms;
   int chunks = (int)std::max<long long>(1, (want + tiles - 1) / tiles);
   chunks = std::min(chunks, std::max(1, c->n[2] / 4));
   const char *zc = getenv("PHOTONOXIDE_FDTD_ZCHUNKS");

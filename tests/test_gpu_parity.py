@@ -93,6 +93,20 @@ def test_closed_box_f32_bit_for_bit_over_300_steps():
         assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("runs", [5, 9, 13])
+def test_runs_of_planes_give_the_oracles_bits(runs, monkeypatch):
+    """The quad kernel's z cut into runs of planes (each recomputing its first plane of H): the
+    z CPMLs' runs, equal interior runs and, from four interior runs on, two short ones; every
+    cut the oracle's bits."""
+    monkeypatch.setenv("PHOTONOXIDE_FDTD_ZCHUNKS", str(runs))
+    p = stirred(lambda *a: Simulation(*a, precision=32), (), 4, (132, 20, 40))
+    o = stirred(lambda *a: OracleSimulation(*a, precision=32), (), 4, (132, 20, 40))
+    p.run(29)
+    o.run(29)
+    for c, (x, y) in enumerate(zip(fields(p), fields(o))):
+        assert np.array_equal(x, y), (c, relative(x, y))
+
+
 @pytest.mark.parametrize("precision", [32, 64])
 @pytest.mark.parametrize("periodic_x", [False, True])
 def test_lossless_conductors_bit_for_bit(precision, periodic_x):
