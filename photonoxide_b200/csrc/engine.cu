@@ -1540,17 +1540,20 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const bool hcur = A.hbucket[(long long)tile * nz] != A.hbucket[(long long)tile * nz + nz];
   const bool ecur = A.ebucket[(long long)tile * nz] != A.ebucket[(long long)tile * nz + nz];
 
-  // -- copies: warp w copies E's row w (and the last warp also row RW+1), H's row w and cb's row
-  // w-1 of a plane; lane l the chunks of its four places (lane 0 also the chunk after the row).
+  // -- copies: warp w copies E's row w, H's row w and cb's row w-1 of a plane, lane l the chunks
+  // of its four places; warp 0 (the halo row, which has no E to update) also E's row RW+1 and
+  // the chunk after each of E's rows (lane q < 3 ER: component q / ER, row q % ER).
   // Where a chunk lies beyond a wall (a row, a group of four or a plane the grid doesn't have)
   // it is zero-filled, so the staged neighbours there are the zeros the differences need.
   // Each chunk's offset within a plane is fixed for the run: -1 where it lies beyond a wall.
   const int myp_last = wrap_index(y0 + RW, ny, A.periodic[1]);
-  const bool last_warp = w == WARPS - 1;
+  const bool w0 = w == 0;
   const int off_e0 = (my >= 0 && mxb >= 0) ? my * nx + mxb : -1;
-  const int off_ea0 = (my >= 0 && mxa >= 0) ? my * nx + mxa : -1;
   const int off_e1 = (myp_last >= 0 && mxb >= 0) ? myp_last * nx + mxb : -1;
-  const int off_ea1 = (myp_last >= 0 && mxa >= 0) ? myp_last * nx + mxa : -1;
+  // warp 0's lane q < 3 ER: the chunk after E's row q % ER of component q / ER
+  const int after_c = lane / ER, after_r = lane % ER;
+  const int my_after = wrap_index(y0 - 1 + after_r, ny, A.periodic[1]);
+  const int off_after = (w0 && lane < 3 * ER && my_after >= 0 && mxa >= 0) ? my_after * nx + mxa : -1;
   const int off_h = off_e0;
   const int off_b = (w >= 1 && gy < ny) ? off_e0 : -1;
   // this thread's places in a staged E row, H row and cb row
@@ -1569,14 +1572,13 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   auto issue = [&](T *E, int ke, T *H, int kh) {
     const long long pe = ke >= 0 ? (long long)ke * plane : -1;
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const T *f = A.e_in + c * N;
-      chunk(E + c * ER * EW + erow, f, off_e0, pe);
-      if (lane == 0) chunk(E + (c * ER + w) * EW + ROW, f, off_ea0, pe);
-      if (last_warp) {
-        chunk(E + (c * ER + RW + 1) * EW + VEC * lane, f, off_e1, pe);
-        if (lane == 0) chunk(E + (c * ER + RW + 1) * EW + ROW, f, off_ea1, pe);
-      }
+    for (int c = 0; c < 3; c++) chunk(E + c * ER * EW + erow, A.e_in + c * N, off_e0, pe);
+    if (w0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        chunk(E + (c * ER + RW + 1) * EW + VEC * lane, A.e_in + c * N, off_e1, pe);
+      if (lane < 3 * ER)
+        chunk(E + (after_c * ER + after_r) * EW + ROW, A.e_in + after_c * N, off_after, pe);
     }
     if (H) {
       const long long ph = kh >= 0 ? (long long)kh * plane : -1;
