@@ -1629,13 +1629,13 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     ez1[0] = ld4(Erow(se1, 0, w) + VEC * lane);     // E_x, E_y of the plane after
     ez1[1] = ld4(Erow(se1, 1, w) + VEC * lane);
     const Vec4<T> fx = ld4(sFX + VEC * lane);  // kappa/h along x at the lane's places
-    // +x of the fourth place: the next lane's first, lane 31 the chunk after the row
+    // +x of the fourth place: the next lane's first, lane 31 the chunk after the row (read by
+    // every lane, one address: a broadcast, and no branch)
+    const T ey_a = Erow(se, 1, w)[ROW], ez_a = Erow(se, 2, w)[ROW];
     T ey_n = __shfl_down_sync(0xffffffffu, e[1].v[0], 1);
     T ez_n = __shfl_down_sync(0xffffffffu, e[2].v[0], 1);
-    if (lane == 31) {
-      ey_n = Erow(se, 1, w)[ROW];
-      ez_n = Erow(se, 2, w)[ROW];
-    }
+    ey_n = lane == 31 ? ey_a : ey_n;
+    ez_n = lane == 31 ? ez_a : ez_n;
     // a row or plane after beyond a wall was staged as zeros: no test needed here
     T dyEz[4], dzEy[4], dzEx[4], dxEz[4], dxEy[4], dyEx[4];
 #pragma unroll
