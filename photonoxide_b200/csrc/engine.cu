@@ -1542,7 +1542,8 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 
   // -- copies: warp w copies E's row w, H's row w and cb's row w-1 of a plane, lane l the chunks
   // of its four places; warp 0 (the halo row, which has no E to update) also E's row RW+1 and
-  // the chunk after each of E's rows (lane q < 3 ER: component q / ER, row q % ER).
+  // the chunk after each of E's rows (lane q takes (component, row) = (q / ER, q % ER), and
+  // q + 32 … where 3 ER is over 32).
   // Where a chunk lies beyond a wall (a row, a group of four or a plane the grid doesn't have)
   // it is zero-filled, so the staged neighbours there are the zeros the differences need.
   // Each chunk's offset within a plane is fixed for the run: -1 where it lies beyond a wall.
@@ -1550,10 +1551,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   const bool w0 = w == 0;
   const int off_e0 = (my >= 0 && mxb >= 0) ? my * nx + mxb : -1;
   const int off_e1 = (myp_last >= 0 && mxb >= 0) ? myp_last * nx + mxb : -1;
-  // warp 0's lane q < 3 ER: the chunk after E's row q % ER of component q / ER
-  const int after_c = lane / ER, after_r = lane % ER;
-  const int my_after = wrap_index(y0 - 1 + after_r, ny, A.periodic[1]);
-  const int off_after = (w0 && lane < 3 * ER && my_after >= 0 && mxa >= 0) ? my_after * nx + mxa : -1;
+
   const int off_h = off_e0;
   const int off_b = (w >= 1 && gy < ny) ? off_e0 : -1;
   // this thread's places in a staged E row, H row and cb row
@@ -1577,8 +1575,12 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
 #pragma unroll
       for (int c = 0; c < 3; c++)
         chunk(E + (c * ER + RW + 1) * EW + VEC * lane, A.e_in + c * N, off_e1, pe);
-      if (lane < 3 * ER)
-        chunk(E + (after_c * ER + after_r) * EW + ROW, A.e_in + after_c * N, off_after, pe);
+      for (int q = lane; q < 3 * ER; q += 32) {
+        const int qc = q / ER, qr = q % ER;
+        const int qy = wrap_index(y0 - 1 + qr, ny, A.periodic[1]);
+        chunk(E + (qc * ER + qr) * EW + ROW, A.e_in + qc * N,
+              (qy >= 0 && mxa >= 0) ? qy * nx + mxa : -1, pe);
+      }
     }
     if (H) {
       const long long ph = kh >= 0 ? (long long)kh * plane : -1;
