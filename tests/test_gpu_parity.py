@@ -112,8 +112,7 @@ def test_runs_of_planes_give_the_oracles_bits(runs, monkeypatch):
 def test_lossless_conductors_bit_for_bit(precision, periodic_x):
     """A lossless grid (ca 1, and 0 where cb is 0) with conductors inside tiles, on a tile's
     first row and column and in its last row, walls, and random fields, so that E at a zero cb
-    starts non-zero: the engine keeps a table of the warps whose values hold a zero cb and takes
-    the plain E + cb curl elsewhere, the x wall's E_y and E_z at x = 0 in their own lane."""
+    starts non-zero and must come out as the oracle's zero of the right sign."""
     from photonoxide_b200.types import Pml, Cpml
     n = (132, 30, 12)
 
