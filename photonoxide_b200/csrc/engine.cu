@@ -1459,26 +1459,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   if (kbeg >= nz) return;
   const long long plane = (long long)nx * ny;
   T *sXC = sX + S::X;                                // quad::Smem::XC
-  // the x CPML's coefficients at the row's places, once (read after the prologue's barrier)
-  for (int q = threadIdx.x; q < S::XC; q += THREADS) {
-    const int at = q % ROW, ba = (q / ROW) % 2, c = 1 + (q / (2 * ROW)) % 2, f = q / (4 * ROW);
-    const int gx = x0 - VEC + at;
-    T val = T(0);
-    if (!A.periodic[0] && gx >= 0 && gx < nx) {
-      const int side = gx < A.low[0] ? 0 : (gx >= nx - A.high[0] ? 1 : -1);
-      if (side >= 0) {
-        const SlabEntry &e = A.slab[f][c][0][side];
-        if (e.count && gx >= e.from && gx < e.from + e.count)
-          val = A.coefs[e.coef + ba * e.count + (gx - e.from)];
-      }
-    }
-    sXC[q] = val;
-  }
-  T *sFX = sXC + S::XC;  // quad::Smem::FX
-  for (int q = threadIdx.x; q < S::FX; q += THREADS) {
-    const int mx = wrap_index(x0 - VEC + q % ROW, nx, A.periodic[0]);
-    sFX[q] = mx >= 0 ? (q < ROW ? A.fh : A.fe)[mx] : T(0);
-  }
+  T *sFX = sXC + S::XC;                              // quad::Smem::FX
 
   // -- this lane's four places along x, this warp's row
   const int xb = x0 - VEC + VEC * lane;  // the first of the four
@@ -1703,6 +1684,36 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   // positions: E slots by position p = plane - kbeg + 1 (km at 0), HB slots alike
   issue(e_cur, km, hb_cur, km);                          // E(km), H(km), cb(km)
   issue(e_next, kbeg, nullptr, -1);                      // E(kbeg)
+  // while those copies are in flight: kappa/h along x at the row's places, and (where the
+  // row's places reach an x CPML, else it is never read) the x CPML's b and a there; read after
+  // the barrier below or the loop's first
+  for (int q = threadIdx.x; q < S::FX; q += THREADS) {
+    const int mx = wrap_index(x0 - VEC + q % ROW, nx, A.periodic[0]);
+    sFX[q] = mx >= 0 ? (q < ROW ? A.fh : A.fe)[mx] : T(0);
+  }
+  const bool xtile = !A.periodic[0] && ((A.low[0] > 0 && x0 - VEC < A.low[0]) ||
+                                        (A.high[0] > 0 && x0 - VEC + ROW > nx - A.high[0]));
+  if (xtile) {
+    static_assert(S::XC % THREADS == 0, "the table is whole rounds of the CTA's threads");
+    T val[S::XC / THREADS];  // the loads first, then the stores: all in flight together
+#pragma unroll
+    for (int i = 0; i < S::XC / THREADS; i++) {
+      const int q = threadIdx.x + i * THREADS;
+      const int at = q % ROW, ba = (q / ROW) % 2, c = 1 + (q / (2 * ROW)) % 2, f = q / (4 * ROW);
+      const int gx = x0 - VEC + at;
+      val[i] = T(0);
+      if (gx >= 0 && gx < nx) {
+        const int side = gx < A.low[0] ? 0 : (gx >= nx - A.high[0] ? 1 : -1);
+        if (side >= 0) {
+          const SlabEntry &e = A.slab[f][c][0][side];
+          if (e.count && gx >= e.from && gx < e.from + e.count)
+            val[i] = A.coefs[e.coef + ba * e.count + (gx - e.from)];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < S::XC / THREADS; i++) sXC[threadIdx.x + i * THREADS] = val[i];
+  }
   if (km >= 0) {
     cp_async_wait<0>();
     __syncthreads();
