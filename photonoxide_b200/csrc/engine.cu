@@ -1684,6 +1684,9 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
   // positions: E slots by position p = plane - kbeg + 1 (km at 0), HB slots alike
   issue(e_cur, km, hb_cur, km);                          // E(km), H(km), cb(km)
   issue(e_next, kbeg, nullptr, -1);                      // E(kbeg)
+  // plane kbeg's H and cb, and E(kbeg+1), into the slots the prologue leaves alone: in flight
+  // while it computes (it waits for the two groups before this one only)
+  issue(e_fill, wrap_index(kbeg + 1, nz, A.periodic[2]), hb_fill, kbeg);
   // while those copies are in flight: kappa/h along x at the row's places, and (where the
   // row's places reach an x CPML, else it is never read) the x CPML's b and a there; read after
   // the barrier below or the loop's first
@@ -1715,7 +1718,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     for (int i = 0; i < S::XC / THREADS; i++) sXC[threadIdx.x + i * THREADS] = val[i];
   }
   if (km >= 0) {
-    cp_async_wait<0>();
+    cp_async_wait<1>();
     __syncthreads();
     compute_h(e_cur, e_next, hb_cur, km, A.fh[nx + ny + km], false, hn);
 #pragma unroll
@@ -1728,8 +1731,7 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     for (int j = 0; j < 4; j++) hprev[0][j] = hprev[1][j] = T(0);
   }
   __syncthreads();
-  // plane kbeg's H and cb, and E(kbeg+1); then the slots move on one plane: E(kbeg) current
-  issue(e_fill, wrap_index(kbeg + 1, nz, A.periodic[2]), hb_fill, kbeg);
+  // the slots move on one plane: E(kbeg) current
   {
     T *t = e_cur;
     e_cur = e_next;
