@@ -1349,7 +1349,8 @@ __device__ __forceinline__ int xslab_places(const StepArgs<T> &A, int x0, int &p
 // the slab's places p0 .. p0+P-1 (side, p0 and P from xslab_places), and lane L < 2P updates
 // component 1 + L / P at place p0 + L % P; the owner applies the result, which it reads back from
 // the row's positions in u1 (component 1) or u2 (component 2): scratch rows of the warp's own,
-// whose earlier values it has done with (the warp's staged rows of the old H). The x
+// whose earlier values it has done with (the warp's staged rows of the old H); or, with SHARED
+// false, which it is shuffled (the lossy form, where the shared rows' loads spill). The x
 // difference is taken from the staged rows the owner's came from, the same two values: for H
 // forward, r[pos+1] - r[pos], over E's rows (r1 E_z for H_y, r2 E_y for H_z, positions from
 // x0-4); for E backward, r[pos] - r[pos-1], over the new H's exchange rows (r1 H_z for E_y, r2
@@ -1357,14 +1358,14 @@ __device__ __forceinline__ int xslab_places(const StepArgs<T> &A, int x0, int &p
 // before the others); only the lane that computes it differs, so that a tile whose rows meet an
 // x CPML pays for its few places once per warp, not once per place of each lane. Lanes below
 // `ownmin` own no values (E: the halo lane). Every lane of the warp calls it.
-template <typename T, int FIELD>
+template <typename T, int FIELD, bool SHARED>
 __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x0, int lane,
                                       int side, int p0, int P, int ownmin, bool write, T v[3][4],
                                       const T *r1, const T *r2, const T cbv[3][4], const T *xc,
                                       const T *xp, T *u1, T *u2) {
   using quad::ROW;
   using quad::VEC;
-  __syncwarp();  // the lanes are done with the scratch rows' earlier values
+  if (SHARED) __syncwarp();  // the lanes are done with the scratch rows' earlier values
   const int c = lane < P ? 1 : 2;
   const int pos = p0 + lane - (c - 1) * P;
   const bool work = lane < 2 * P && (pos >> 2) >= ownmin;
@@ -1382,12 +1383,31 @@ __device__ __forceinline__ void xcoop(const StepArgs<T> &A, int k, int my, int x
       const T nw = b * old + a * q;
       u = (c == 1 ? T(-1) : T(1)) * nw;
       if (write && (pos >> 2) >= 1) (FIELD == 1 ? A.psi_h_out : A.psi_e)[at] = nw;
-      (c == 1 ? u1 : u2)[pos] = u;
+      if (SHARED) (c == 1 ? u1 : u2)[pos] = u;
     }
   }
-  __syncwarp();
   const bool has1 = A.slab[FIELD][1][0][side].count != 0;
   const bool has2 = A.slab[FIELD][2][0][side].count != 0;
+  if (!SHARED) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int q = 4 * lane + r - p0;  // this lane's place r as a worker of component 1
+      const bool mine = q >= 0 && q < P && lane >= ownmin;
+      const T g1 = __shfl_sync(0xffffffffu, u, mine ? q : lane);
+      const T g2 = __shfl_sync(0xffffffffu, u, mine ? P + q : lane);
+      if (mine) {
+        if (FIELD == 1) {
+          if (has1) v[1][r] = v[1][r] - A.dt * g1;
+          if (has2) v[2][r] = v[2][r] - A.dt * g2;
+        } else {
+          if (has1) v[1][r] = v[1][r] + cbv[1][r] * g1;
+          if (has2) v[2][r] = v[2][r] + cbv[2][r] * g2;
+        }
+      }
+    }
+    return;
+  }
+  __syncwarp();
   // the owners: lanes with a place in the slab (the halo lane aside), one component at a time
   if (lane >= ownmin && 4 * lane + 3 >= p0 && 4 * lane < p0 + P) {
 #pragma unroll
@@ -1647,9 +1667,9 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
     if (xco && rowh) {
       const T nocb[3][4] = {};
       // scratch: the warp's rows of the old H, in registers since the top (ho)
-      xcoop<T, 1>(A, k, my, x0, lane, xside, xp0, xP, 0, write && w >= 1, hn, Erow(se, 2, w),
-                  Erow(se, 1, w), nocb, sXC, sh + S::XP_OFF + w * S::XP,
-                  const_cast<T *>(Hrow(sh, 0)), const_cast<T *>(Hrow(sh, 1)));
+      xcoop<T, 1, !LOSSY>(A, k, my, x0, lane, xside, xp0, xP, 0, write && w >= 1, hn,
+                          Erow(se, 2, w), Erow(se, 1, w), nocb, sXC, sh + S::XP_OFF + w * S::XP,
+                          const_cast<T *>(Hrow(sh, 0)), const_cast<T *>(Hrow(sh, 1)));
     }
     if (rowh && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
       const bool ow = write && w >= 1 && lane >= 1;
@@ -1870,10 +1890,10 @@ __global__ void __launch_bounds__(quad::THREADS, 2) quad_kernel(StepArgs<T> A) {
         const T cbs[3][4] = {{cb[0].v[0], cb[0].v[1], cb[0].v[2], cb[0].v[3]},
                              {cb[1].v[0], cb[1].v[1], cb[1].v[2], cb[1].v[3]},
                              {cb[2].v[0], cb[2].v[1], cb[2].v[2], cb[2].v[3]}};
-        xcoop<T, 0>(A, k, my, x0, lane, xside, xp0, xP, 1, true, en,
-                    sX + (size_t)(WARPS + w) * ROW, sX + (size_t)(2 * WARPS + w) * ROW, cbs, sXC,
-                    hb_cur + S::XP_OFF + w * S::XP, const_cast<T *>(Hrow(hb_cur, 0)),
-                    const_cast<T *>(Hrow(hb_cur, 1)));
+        xcoop<T, 0, !LOSSY>(A, k, my, x0, lane, xside, xp0, xP, 1, true, en,
+                            sX + (size_t)(WARPS + w) * ROW, sX + (size_t)(2 * WARPS + w) * ROW,
+                            cbs, sXC, hb_cur + S::XP_OFF + w * S::XP,
+                            const_cast<T *>(Hrow(hb_cur, 0)), const_cast<T *>(Hrow(hb_cur, 1)));
       }
       if (any_own && mxb >= 0 && (zs | (sy >= 0) | (any_x && !xco))) {
         const T diff[3][3][4] = {
